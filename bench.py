@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LES time step (one JSON line on rank 0).
+
+Workload: the 600x600x120 plain FP32 step (synthetic terrain at 35% plan
+area, heights to 120 m, log-law inflow with frozen noise, dt = 0.05 s, red-
+black SOR with 50 sweeps per step).  One "step" is one full time step of
+velnw, bondv1, velfg, feedbf, les, adam and press (main_ocl.f95:264-299).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank advances its own replica of the domain
+(the single domain does not shard; replicas only) and `value` is the sum of
+the ranks' throughput, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "time-step Mpts/s: plain vs FP64-refined press at ≤1e-5 err; adjoint/fwd cost"
+WORKLOAD = dict(ip=600, jp=600, kp=120, plan_area=0.35, h_max=120.0, dt=0.05, nmaxp=50, seed=1)
+SOR_BYTES_PER_CELL_PER_COLOUR = 6.0   # 12 B/cell per SOR iteration (p read, rhs read, p write) over 2 colour sweeps
+STEP_BYTES_PER_CELL = 204.0 + 12.0 * 50  # algorithmic bytes per cell per step at 50 SOR iterations
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_case(on_device_setup=True):
+    import les_halo_b200 as lh
+    W = WORKLOAD
+    kw = dict(plan_area=W["plan_area"], h_max=W["h_max"])
+    if on_device_setup:
+        return lh.synthetic_case(W["ip"], W["jp"], W["kp"], seed=W["seed"], dt=W["dt"],
+                                 nmaxp=W["nmaxp"], **kw)
+    import oracle
+    return lh.synthetic_case(W["ip"], W["jp"], W["kp"], seed=W["seed"], dt=W["dt"],
+                             nmaxp=W["nmaxp"], masks_and_poisson=oracle.masks_and_poisson, **kw)
+
+
+def cpu_baseline(threads: int, ip=150, jp=150, kp=120, steps=1):
+    """The oracle (CPU restatement of the reference's Fortran step) on a
+    bounded sample: `steps` full time steps of an ip x jp x kp sub-domain of
+    the workload (same kp, SOR sweeps and per-cell work)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import les_halo_b200 as lh
+    import oracle
+    W = WORKLOAD
+    case = lh.synthetic_case(ip, jp, kp, seed=W["seed"], dt=W["dt"], nmaxp=W["nmaxp"],
+                             plan_area=W["plan_area"], h_max=W["h_max"],
+                             masks_and_poisson=oracle.masks_and_poisson)
+    oracle.ifdata(case, 1)
+    oracle.run_steps(case, 1, 1)  # untimed first step (n==1 broadcast)
+    t0 = time.perf_counter()
+    oracle.run_steps(case, 2, steps)
+    dt = time.perf_counter() - t0
+    return {"value": round(ip * jp * kp * steps / dt / 1e6, 3), "unit": "Mpts/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{steps} full step(s) (n>=2) of a {ip}x{jp}x{kp} sub-domain of the workload, "
+                      f"oracle C++ restatement of the Fortran CPU path, OpenMP {threads} threads, "
+                      f"{dt:.2f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import les_halo_b200 as lh
+    import oracle
+    W = WORKLOAD
+    ip, jp, kp = 120, 120, W["kp"]
+    case = lh.synthetic_case(ip, jp, kp, seed=W["seed"], dt=W["dt"], nmaxp=W["nmaxp"],
+                             plan_area=W["plan_area"], h_max=W["h_max"],
+                             masks_and_poisson=oracle.masks_and_poisson)
+    oracle.ifdata(case, 1)
+    n = 1
+    for _ in range(args.warmup):
+        oracle.run_steps(case, n, 1)
+        n += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.run_steps(case, n, 1)
+        n += 1
+    dt = time.perf_counter() - t0
+    val = ip * jp * kp * args.steps / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "Mpts/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "LES plain FP32 step 600x600x120 (35% plan area, SOR 50), per-step "
+                               f"sample {ip}x{jp}x{kp}", "sor_iters": W["nmaxp"],
+                   "l2": "CPU run"},
+        "cpu_baseline": {"value": round(val, 3), "unit": "Mpts/s", "cores": threads, "kind": "port",
+                         "sample": f"each step: one full time step of a {ip}x{jp}x{kp} sub-domain, "
+                                   "oracle restatement of the reference Fortran (no Fortran "
+                                   "compiler here to build the reference itself)"},
+        "e2e": {"value": round(val, 3), "unit": "Mpts/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import les_halo_b200 as lh
+    from les_halo_b200 import abi
+
+    case = make_case(on_device_setup=True)
+    cells = case.ip * case.jp * case.kp
+    gpu = lh.GpuLes(case)
+    gpu.warmup(1)
+    n = 1
+    gpu.step(n, args.warmup)
+    n += args.warmup
+    gpu.sync()
+    L = abi.lib()
+    # capture the timed step graph (with its event nodes) before timing, then
+    # reset the slots so the K timed steps use slots 0..K-1
+    abi.check(L.les_ctx_set_timing(gpu.ctx, args.steps))
+    gpu.step(n, 1)
+    n += 1
+    gpu.sync()
+    abi.check(L.les_ctx_set_timing(gpu.ctx, args.steps))
+
+    stream = torch.cuda.ExternalStream(gpu.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    launches0 = gpu.launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    ev0.record(stream)
+    gpu.step(n, args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    n += args.steps
+    if dist:
+        dist.barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    launches = gpu.launches() - launches0
+    phases = np.zeros((args.steps, 9), np.float32)
+    buf = (C.c_float * 9)()
+    for s in range(args.steps):
+        abi.check(L.les_ctx_phase_times(gpu.ctx, s, buf, 9))
+        phases[s] = np.frombuffer(buf, np.float32)
+    m = gpu.metrics()
+
+    # e2e through the C ABI with pinned host buffers: per step the inflow
+    # profile goes up, then the step, then the halo round trip of the state
+    # arrays (ST_HALO_READ/WRITE of run_LES_kernel) and the step record.
+    wp = torch.from_numpy(case.a("wind_profile").ravel(order="F").copy()).pin_memory()
+    halos = []
+    for h in range(len(abi.HALO_IDS)):
+        nf = int(L.les_ctx_halo_floats(gpu.ctx, h))
+        halos.append(torch.empty(nf, dtype=torch.float32).pin_memory())
+    mrec = abi.LesMetrics()
+    e2e_steps = max(3, min(args.steps, 10))
+    h2d = wp.numel() * 4 + sum(t.numel() * 4 for t in halos)
+    d2h = sum(t.numel() * 4 for t in halos) + C.sizeof(mrec)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        abi.check(L.les_set_wind_profile(gpu.ctx, wp.data_ptr()))
+        abi.check(L.les_step(gpu.ctx, n, 1))
+        n += 1
+        for h, t in enumerate(halos):
+            abi.check(L.les_ctx_halo_read(gpu.ctx, h, t.data_ptr()))
+        for h, t in enumerate(halos):
+            abi.check(L.les_ctx_halo_write(gpu.ctx, h, t.data_ptr()))
+        abi.check(L.les_last_metrics(gpu.ctx, C.byref(mrec)))
+    e2e_s = time.perf_counter() - t0
+
+    times = torch.tensor([ms_total, e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms_total, e2e_s = float(times[0]), float(times[1])
+    ms_step = ms_total / args.steps
+    value = ws * cells * args.steps / (ms_total / 1e3) / 1e6
+    e2e_val = ws * cells * e2e_steps / e2e_s / 1e6
+
+    sor_launch_ms = float(np.mean(phases[:, 5]))
+    peak, peak_kind = _peaks()
+    achieved = SOR_BYTES_PER_CELL_PER_COLOUR * cells / (sor_launch_ms / 1e3) / 1e9
+    step_gbs = STEP_BYTES_PER_CELL * cells / (ms_step / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "sor_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mpts/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded terrain + log-law inflow)",
+            "config": {"workload": "LES plain FP32 step 600x600x120 (35% plan area, heights <=120 m, "
+                                   "dt=0.05, SOR 50 sweeps/step)",
+                       "grid": [case.ip, case.jp, case.kp], "sor_iters": int(m["sor_iters"]),
+                       "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2 (19 state fields, 3.5 GB)"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_sor_colour",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic": f"{SOR_BYTES_PER_CELL_PER_COLOUR} B/cell x {cells} cells per launch"},
+            "step_roofline": {"achieved_gbs": round(step_gbs, 1), "frac": round(step_gbs / peak, 4),
+                              "bytes_per_cell": STEP_BYTES_PER_CELL},
+            "phases_ms": {k: round(float(v), 4) for k, v in zip(
+                ["velnw_bondv1", "velfg_feedbf_sm", "boundsm_visc_adam", "rhs_rhsav", "gap",
+                 "sor_first_launch", "sor_rest", "pav", "step"], phases.mean(axis=0))},
+            "e2e": {"value": round(e2e_val, 3), "unit": "Mpts/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                    "path": "C ABI: les_set_wind_profile + les_step + les_ctx_halo_read/write x7 + "
+                            "les_last_metrics, pinned host buffers, wall clock"},
+            "clocks": clocks,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+        print(json.dumps(line), flush=True)
+    gpu.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,271 @@
+/*
+ * les_abi.h -- C ABI of liblesb200.so, the B200 (sm_100a) LES time step.
+ *
+ * Drop-in boundary for the LES_Halo reference (Hallot/LES_Halo):
+ *   - a context API that replaces the accelerator driver pair
+ *     initialise_LES_kernel / run_LES_kernel
+ *     (src/OpenCL/module_LES_combined_ocl_TEMPL_V2.f95:18-30 and :219-231);
+ *   - per-routine entry points with the Fortran argument order of the CPU
+ *     routines called from src/Fortran/main_ocl.f95:264-299, so a Fortran
+ *     host binds them with bind(C) interfaces (all scalars by reference);
+ *   - halo pack/unpack entry points with the semantics of
+ *     src/OpenCL/Kernels/halo_exchange.cl (and halo_exchange_correct.cl).
+ *
+ * Arrays crossing this boundary are host arrays in the reference's Fortran
+ * layout (column-major, the bounds of main_ocl.f95:41-167 with ip=im, jp=jm,
+ * kp=km), passed as the address of their first element, unless a function
+ * says it takes device pointers.  The library owns all device memory; it
+ * never keeps a caller's pointer beyond the call.  Every function returns a
+ * les_status; none exits the process.  A context is not thread-safe; distinct
+ * contexts are independent.  There is no CPU fallback: without a usable
+ * B200 every compute call returns LES_ERR_CUDA.
+ */
+#ifndef LES_ABI_H
+#define LES_ABI_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum les_status {
+    LES_OK = 0,
+    LES_ERR_BAD_ARG = 1, /* null pointer, bad size, bad mode            */
+    LES_ERR_DIMS = 2,    /* grid extents unsupported (ifdata.f95:216)   */
+    LES_ERR_CUDA = 3,    /* CUDA runtime error or no usable device      */
+    LES_ERR_TIMEOUT = 4, /* a bounded device wait gave up               */
+    LES_ERR_NAN = 5,     /* non-finite value found by a checking call   */
+    LES_ERR_NOMEM = 6,   /* device allocation failed                    */
+    LES_ERR_STATE = 7    /* call out of order (e.g. step before upload) */
+} les_status;
+
+/* Last error message of the calling thread ("" after success). */
+const char *les_last_error_string(void);
+/* Library version string and the device the library runs on. */
+const char *les_version(void);
+
+/* Inflow modes of bondv1 (bondv1.f95:26-45 power law, or
+ * bondv1_ext_wind_profile.f95:27-35 with an external wind_profile(jp,kp)). */
+enum { LES_INFLOW_POWER_LAW = 0, LES_INFLOW_EXTERNAL = 1 };
+
+typedef struct les_params {
+    int ip, jp, kp;     /* interior extents (im, jm, km)                       */
+    float dt;           /* set.f95:76                                          */
+    float ro, vn;       /* set.f95:78-79                                       */
+    float alpha, beta;  /* IBM feedback gains, set.f95:81-82                  */
+    float cs0;          /* Smagorinsky constant, les.f95:123 (0.1)            */
+    int nmaxp;          /* SOR iteration cap, press.f95:108 (50)               */
+    float pjuge;        /* SOR stop threshold on sum(reltmp^2), press.f95:107  */
+    float omega;        /* SOR relaxation, press.f95:109 (1.0)                 */
+    int inflow_mode;    /* LES_INFLOW_*                                        */
+    int ical;           /* 0: n==1 broadcast of the inflow plane (ICAL=0)      */
+} les_params;
+
+/* Fill p with the reference's constants for an ip x jp x kp grid
+ * (set.f95:76-82, les.f95:123, press.f95:107-109; vn = 15.83*10.**(-6.)). */
+les_status les_params_default(les_params *p, int ip, int jp, int kp);
+
+/* Host arrays in Fortran layout (bounds as in main_ocl.f95). */
+typedef struct les_host_fields {
+    float *u, *v, *w;          /* (0:ip+1,-1:jp+1,0:kp+1), w (...,-1:kp+1) */
+    float *p;                  /* (0:ip+2,0:jp+2,0:kp+1)                   */
+    float *usum, *vsum, *wsum; /* (0:ip,0:jp,0:kp)                         */
+    float *f, *g, *h;          /* (0:ip,0:jp,0:kp)                         */
+    float *fold, *gold, *hold; /* (1:ip,1:jp,1:kp)                         */
+    float *rhs;                /* (0:ip+1,0:jp+1,0:kp+1)                   */
+    float *sm;                 /* (-1:ip+1,-1:jp+1,0:kp+1)                 */
+    float *amask1, *dmask1;    /* (0:ip+1,0:jp+1,0:kp+1)                   */
+    float *bmask1;             /* (-1:ip+1,0:jp+1,0:kp+1)                  */
+    float *cmask1;             /* (0:ip+1,-1:jp+1,0:kp+1)                  */
+    float *cn1;                /* (1:ip,1:jp,1:kp)                         */
+    float *cn2l, *cn2s;        /* (ip)                                     */
+    float *cn3l, *cn3s;        /* (jp)                                     */
+    float *cn4l, *cn4s;        /* (kp)                                     */
+    float *dx1;                /* (-1:ip+1)                                */
+    float *dy1;                /* (0:jp+1)                                 */
+    float *dzn, *dzs;          /* (-1:kp+2)                                */
+    float *dxs;                /* (0:ip)                                   */
+    float *dys;                /* (0:jp)                                   */
+    float *z2;                 /* (1:kp+2)                                 */
+    float *delx1;              /* (1:kp), output of les (may be NULL)       */
+    float *wind_profile;       /* (1:jp,1:kp), LES_INFLOW_EXTERNAL only     */
+} les_host_fields;
+
+/* Per-step record (device-side values copied back by les_last_metrics). */
+typedef struct les_metrics {
+    int n;             /* time step index of the last step          */
+    int sor_iters;     /* SOR iterations executed in that step       */
+    float sor;         /* final sum(reltmp^2) (FP64 sum, rounded)   */
+    float rhsav;       /* volume mean removed from rhs              */
+    float pav;         /* volume mean removed from p                */
+    float uout;        /* advective outflow speed (bondv1.f95:75)   */
+    float p_centre, u_centre, v_centre, w_centre; /* press.f95:183-187 probe */
+} les_metrics;
+
+/* ---- context API: replaces initialise_LES_kernel / run_LES_kernel ---- */
+typedef struct les_ctx les_ctx;
+
+les_status les_ctx_create(const les_params *prm, les_ctx **out);
+les_status les_ctx_destroy(les_ctx *ctx);
+/* initialise_LES_kernel (TEMPL:18-215): copy the model state, metrics,
+ * masks and Poisson coefficients to the device.  Fields the model does not
+ * read (rhs, delx1) may be NULL. */
+les_status les_ctx_upload(les_ctx *ctx, const les_host_fields *hf);
+/* Copy the device state back; any NULL pointer is skipped.  rhs is returned
+ * after the rhsav subtraction (press.f95:80-82), as the reference holds it. */
+les_status les_ctx_download(les_ctx *ctx, les_host_fields *hf);
+/* ifdata.f95:250-284 (ICAL=0, IFBF=1, IADAM=0) on the device: zero f,g,h,
+ * bondv1(n), boundp1/2, velfg, feedbf, les.  Call after les_ctx_upload. */
+les_status les_ctx_warmup(les_ctx *ctx, int n);
+/* run_LES_kernel (TEMPL:219-1072): nsteps time steps n0..n0+nsteps-1 of
+ * velnw, bondv1, velfg, feedbf, les, adam, press (main_ocl.f95:264-299).
+ * Asynchronous on the context stream; les_ctx_sync waits. */
+les_status les_step(les_ctx *ctx, int n0, int nsteps);
+/* Replace the external inflow profile wind_profile(1:jp,1:kp) (host array)
+ * before the next step (run_LES_kernel's per-step wind_profile argument). */
+les_status les_set_wind_profile(les_ctx *ctx, const float *wind_profile);
+les_status les_ctx_sync(les_ctx *ctx);
+les_status les_last_metrics(les_ctx *ctx, les_metrics *m);
+/* CUDA stream (cudaStream_t) the context launches on. */
+void *les_ctx_stream(les_ctx *ctx);
+/* Number of kernels the library launched on this context so far. */
+uint64_t les_ctx_launch_count(les_ctx *ctx);
+/* Per-step phase timing with CUDA events recorded inside the step graph on
+ * the context stream: the next nslots steps each get their own events
+ * (nslots = 0 turns timing off).  les_ctx_phase_times returns, for one
+ * slot, in milliseconds: [0] velnw+bondv1, [1] velfg+feedbf+sm, [2] boundsm
+ * + visc + adam, [3] rhs + rhsav, [4] gap, [5] the first SOR colour sweep
+ * (one launch), [6] the rest of the SOR loop, [7] pav, [8] the whole step. */
+les_status les_ctx_set_timing(les_ctx *ctx, int nslots);
+les_status les_ctx_phase_times(les_ctx *ctx, int slot, float *ms, int n);
+
+/* Device state access for callers that keep fields on the GPU.  The field
+ * is stored in a padded box: element (i,j,k) of the interior-indexed field
+ * lives at ptr + (i + ox) + si*((j + 1) + sj*(k + 1)) (floats), for
+ * -1 <= i <= ip+2, -1 <= j <= jp+2, -1 <= k <= kp+2. */
+enum {
+    LES_F_U = 0, LES_F_V, LES_F_W, LES_F_P, LES_F_USUM, LES_F_VSUM, LES_F_WSUM,
+    LES_F_F, LES_F_G, LES_F_H, LES_F_FOLD, LES_F_GOLD, LES_F_HOLD, LES_F_RHS,
+    LES_F_SM, LES_F_AMASK, LES_F_BMASK, LES_F_CMASK, LES_F_DMASK, LES_NFIELDS
+};
+les_status les_ctx_field(les_ctx *ctx, int field, float **dptr, int *ox, int *si, int *sj,
+                         int *sk);
+
+/* Halo ring of the context state, in the reference's buffer layout
+ * (north|south|west|east, h_w = 1, TEMPL:111-127): the state arrays are
+ * exchanged as the reference's combined arrays p2 (float2, extents
+ * ip+3,jp+3,kp+2), uvw (float4, ip+2,jp+3,kp+3), uvwsum and fgh (float4,
+ * ip+1,jp+1,kp+1), fgh_old (float4, ip,jp,kp), rhs (float, ip+2,jp+2,kp+2)
+ * and sm (float, ip+3,jp+3,kp+2) (LES_combined_kernel.cl:345-364).  Host
+ * buffers; sizes from les_ctx_halo_floats. */
+enum { LES_H_P = 0, LES_H_UVW, LES_H_UVWSUM, LES_H_FGH, LES_H_FGH_OLD, LES_H_RHS, LES_H_SM,
+       LES_NHALOS };
+size_t les_ctx_halo_floats(les_ctx *ctx, int which);
+/* ST_HALO_READ_*: pack the ring of the state array into buf (host). */
+les_status les_ctx_halo_read(les_ctx *ctx, int which, float *buf);
+/* ST_HALO_WRITE_*: unpack buf (host) into the ring of the state array. */
+les_status les_ctx_halo_write(les_ctx *ctx, int which, const float *buf);
+
+/* ---- halo pack/unpack on caller arrays (halo_exchange.cl) -------------
+ * array holds vdim floats per point (vdim = 1, 2, 4 or 16; the reference's
+ * float, float2, float4, float16) with extents im (fastest), jm, km; h_w is
+ * the ring width.  buffer size: les_halo_buffer_floats().  `device` != 0
+ * means both pointers are device pointers (launched on `stream`, a
+ * cudaStream_t or NULL); otherwise they are host pointers. */
+size_t les_halo_buffer_floats(unsigned im, unsigned jm, unsigned km, unsigned h_w, unsigned vdim,
+                              int inner);
+/* exchange_{1,2,4,16}_halo_read, halo_exchange.cl:156-291 */
+les_status les_halo_pack(const float *array, float *buffer, unsigned im, unsigned jm, unsigned km,
+                         unsigned h_w, unsigned vdim, int device, void *stream);
+/* exchange_{1,2,4,16}_halo_write, halo_exchange.cl:3-152 */
+les_status les_halo_unpack(float *array, const float *buffer, unsigned im, unsigned jm,
+                           unsigned km, unsigned h_w, unsigned vdim, int device, void *stream);
+/* halo_exchange_correct.cl read: the owned inner ring, N|S without corners */
+les_status les_halo_pack_inner(const float *array, float *buffer, unsigned im, unsigned jm,
+                               unsigned km, unsigned h_w, unsigned vdim, int device, void *stream);
+/* halo_exchange_correct.cl write (N|S buffer index without the im*w term) */
+les_status les_halo_unpack_inner(float *array, const float *buffer, unsigned im, unsigned jm,
+                                 unsigned km, unsigned h_w, unsigned vdim, int device,
+                                 void *stream);
+
+/* ---- setup feeding the step (a14) ------------------------------------ */
+/* grid.f95:55-82 metric derivation: given dx1(-1:ip+1), dy1(0:jp+1) and
+ * dzn(1:kp+1) (in an array with bounds -1:kp+2), fill dxl, dyl, z2, the
+ * dzn edge rules, dzs, dxs, dys.  grid.f95:42-43 sets z2(1)=dzn(1). */
+les_status les_grid_metrics(int ip, int jp, int kp, float *dx1, float *dxl, float *dy1,
+                            float *dyl, float *z2, float *dzn, float *dzs, float *dxs, float *dys);
+/* init.f95:82-107 Poisson coefficients cn1..cn4s, computed on the device. */
+les_status les_poisson_coeffs(int ip, int jp, int kp, const float *dxs, const float *dys,
+                              const float *dzs, float *cn1, float *cn2l, float *cn2s, float *cn3l,
+                              float *cn3s, float *cn4l, float *cn4s);
+/* feedbfm.f95:21-63 masks from building heights zbm(-1:ip+1,-1:jp+1),
+ * computed on the device; mask entries outside 1..ip,1..jp,1..kp are left
+ * as the caller initialised them. */
+les_status les_building_masks(int ip, int jp, int kp, const float *zbm, const float *z2,
+                              const float *dzn, float *amask1, float *bmask1, float *cmask1,
+                              float *dmask1);
+
+/* ---- per-routine drop-in entries (Fortran order, scalars by reference) --
+ * Each copies its host arrays to the device, runs the routine's kernels and
+ * copies the intent(out/inout) arrays back.  An output the caller does not
+ * need may be NULL (e.g. cov/nou/dfu1 scratch of velfg). */
+/* velnw.f95:5 */
+les_status les_velnw_(const int *km, const int *jm, const int *im, const float *p, const float *ro,
+                      const float *dxs, float *u, const float *dt, const float *f, const float *dys,
+                      float *v, const float *g, const float *dzs, float *w, const float *h);
+/* bondv1.f95:5 */
+les_status les_bondv1_(const int *jm, float *u, const float *z2, const float *dzn, float *v,
+                       float *w, const int *km, const int *n, const int *im, const float *dt,
+                       const float *dxs);
+/* bondv1_ext_wind_profile.f95:5 */
+les_status les_bondv1_ext_wind_profile_(const int *jm, float *u, const float *z2, const float *dzn,
+                                        float *v, float *w, const int *km, const int *n,
+                                        const int *im, const float *dt, const float *dxs,
+                                        const float *wind_profile);
+/* velFG.f95:6 (diu1..9 are produced; cov*, nou*, dfu1/dfv1/dfw1 too when
+ * non-NULL) */
+les_status les_velfg_(const int *km, const int *jm, const int *im, const float *dx1, float *cov1,
+                      float *cov2, float *cov3, float *dfu1, float *diu1, float *diu2,
+                      const float *dy1, float *diu3, const float *dzn, const float *vn, float *f,
+                      float *cov4, float *cov5, float *cov6, float *dfv1, float *diu4, float *diu5,
+                      float *diu6, float *g, float *cov7, float *cov8, float *cov9, float *dfw1,
+                      float *diu7, float *diu8, float *diu9, const float *dzs, float *h,
+                      float *nou1, const float *u, float *nou5, const float *v, float *nou9,
+                      const float *w, float *nou2, float *nou3, float *nou4, float *nou6,
+                      float *nou7, float *nou8);
+/* feedbf.f95:5 */
+les_status les_feedbf_(const int *km, const int *jm, const int *im, float *usum, const float *u,
+                       const float *bmask1, float *vsum, const float *v, const float *cmask1,
+                       float *wsum, const float *w, const float *dmask1, const float *alpha,
+                       const float *dt, const float *beta, float *fx, float *fy, float *fz,
+                       float *f, float *g, float *h);
+/* les.f95:98 (diu1..9 as produced by velfg) */
+les_status les_les_(const int *km, float *delx1, const float *dx1, const float *dy1,
+                    const float *dzn, const int *jm, const int *im, const float *diu1,
+                    const float *diu2, const float *diu3, const float *diu4, const float *diu5,
+                    const float *diu6, const float *diu7, const float *diu8, const float *diu9,
+                    float *sm, float *f, float *g, float *h);
+/* boundsm.f95:5 */
+les_status les_boundsm_(const int *km, const int *jm, float *sm, const int *im);
+/* adam.f95:5 (the data21 file write is the caller's) */
+les_status les_adam_(const int *n, const int *nmax, float *fold, const int *im, const int *jm,
+                     const int *km, float *gold, float *hold, float *f, float *g, float *h);
+/* press.f95:72 (the data20 write and prints are the caller's); sor_iters
+ * (may be NULL) receives the executed SOR iteration count. */
+les_status les_press_(const int *km, const int *jm, const int *im, float *rhs, const float *u,
+                      const float *dx1, const float *v, const float *dy1, const float *w,
+                      const float *dzn, float *f, float *g, float *h, const float *dt,
+                      const float *cn1, const float *cn2l, float *p, const float *cn2s,
+                      const float *cn3l, const float *cn3s, const float *cn4l, const float *cn4s,
+                      const int *n, const int *nmax, int *sor_iters);
+/* bondFG.f95:5 */
+les_status les_bondfg_(const int *km, const int *jm, float *f, const int *im, float *g, float *h);
+/* boundp.f95:36 */
+les_status les_boundp1_(const int *km, const int *jm, float *p, const int *im);
+/* boundp.f95:18 */
+les_status les_boundp2_(const int *jm, const int *im, float *p, const int *km);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

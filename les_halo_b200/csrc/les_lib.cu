@@ -1,0 +1,802 @@
+// les_lib.cu -- host side of liblesb200.so: contexts, the host boundary,
+// the graph-captured time step and the setup routines (les_abi.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "les_abi.h"
+#include "les_halo.cuh"
+#include "les_press.cuh"
+#include "les_step.cuh"
+
+using namespace les;
+
+namespace {
+
+thread_local std::string g_err;
+
+les_status fail(les_status s, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+les_status ok() {
+    g_err.clear();
+    return LES_OK;
+}
+
+}  // namespace
+
+les_status les_internal_fail(les_status s, const char *msg) { return fail(s, "%s", msg); }
+les_status les_internal_ok() { return ok(); }
+
+namespace {
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(LES_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+#define CKL()                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess) return fail(LES_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e_)); \
+    } while (0)
+
+inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Fortran bounds of each state field (main_ocl.f95:41-167).
+struct FBounds {
+    int li, ui, lj, uj, lk, uk;
+    int ni() const { return ui - li + 1; }
+    int nj() const { return uj - lj + 1; }
+    int nk() const { return uk - lk + 1; }
+    size_t n() const { return (size_t)ni() * nj() * nk(); }
+};
+FBounds field_bounds(int f, int ip, int jp, int kp) {
+    switch (f) {
+        case LES_F_U:
+        case LES_F_V: return {0, ip + 1, -1, jp + 1, 0, kp + 1};
+        case LES_F_W: return {0, ip + 1, -1, jp + 1, -1, kp + 1};
+        case LES_F_P: return {0, ip + 2, 0, jp + 2, 0, kp + 1};
+        case LES_F_USUM:
+        case LES_F_VSUM:
+        case LES_F_WSUM:
+        case LES_F_F:
+        case LES_F_G:
+        case LES_F_H: return {0, ip, 0, jp, 0, kp};
+        case LES_F_FOLD:
+        case LES_F_GOLD:
+        case LES_F_HOLD: return {1, ip, 1, jp, 1, kp};
+        case LES_F_RHS: return {0, ip + 1, 0, jp + 1, 0, kp + 1};
+        case LES_F_SM: return {-1, ip + 1, -1, jp + 1, 0, kp + 1};
+        case LES_F_AMASK:
+        case LES_F_DMASK: return {0, ip + 1, 0, jp + 1, 0, kp + 1};
+        case LES_F_BMASK: return {-1, ip + 1, 0, jp + 1, 0, kp + 1};
+        case LES_F_CMASK: return {0, ip + 1, -1, jp + 1, 0, kp + 1};
+    }
+    return {0, 0, 0, 0, 0, 0};
+}
+
+// Offsets of the 1-D tables inside one device buffer (each with slack).
+struct TableLayout {
+    size_t dx1, dy1, dzn, dzs, dxs, dys, cn2l, cn2s, cn3l, cn3s, cn4l, cn4s, cnA, cnB, cnC, smc, wind, total;
+};
+TableLayout table_layout(int ip, int jp, int kp) {
+    TableLayout t;
+    size_t o = 0;
+    auto take = [&](size_t n) {
+        size_t r = o;
+        o += (n + 31) / 32 * 32;
+        return r;
+    };
+    t.dx1 = take(ip + 4);
+    t.dy1 = take(jp + 4);
+    t.dzn = take(kp + 5);
+    t.dzs = take(kp + 5);
+    t.dxs = take(ip + 2);
+    t.dys = take(jp + 2);
+    t.cn2l = take(ip + 2);
+    t.cn2s = take(ip + 2);
+    t.cn3l = take(jp + 2);
+    t.cn3s = take(jp + 2);
+    t.cn4l = take(kp + 2);
+    t.cn4s = take(kp + 2);
+    t.cnA = take(ip + 2);
+    t.cnB = take(jp + 2);
+    t.cnC = take(kp + 2);
+    t.smc = take(kp + 2);
+    t.wind = take((size_t)jp * kp);
+    t.total = o;
+    return t;
+}
+
+}  // namespace
+
+struct les_ctx {
+    les_params prm{};
+    Geo geo{};
+    Fields F{};
+    float *d_fields = nullptr;
+    size_t box_elems = 0;
+    float *d_tables = nullptr;
+    TableLayout tl{};
+    std::vector<float> h_tables;
+    Scal *d_scal = nullptr;
+    FixPart *d_part = nullptr;
+    int npart = 0;
+    float *d_stage = nullptr;
+    size_t stage_elems = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraph_t graph_src[2] = {nullptr, nullptr};
+    uint64_t graph_kernels[2] = {0, 0};
+    // per-step phase timing (les_ctx_set_timing): event record nodes in the
+    // step graphs are pointed at slot `tslot` before each launch
+    int tslots = 0, tslot = 0;
+    std::vector<cudaEvent_t> tev;  // tslots x LES_NTEV
+    std::vector<cudaGraphNode_t> tnode[2];
+    std::vector<int> tnode_idx[2];
+    bool capturing_timed = false;
+    double area = 0.0;
+    uint64_t launches = 0;
+    bool uploaded = false;
+    bool rhs_raw = false;  // interior of rhs holds values before the rhsav subtraction
+    int red_gx = 0, red_gy = 0, red_nk = 0, red_kchunk = 0;
+    int last_n = 0;
+};
+
+namespace {
+
+float *field_ptr(les_ctx *c, int f) { return c->d_fields + (size_t)f * c->box_elems; }
+
+// Host copies of the 1-D tables -> device; builds cnA/B/C, smc, wind.
+les_status build_tables(les_ctx *c, const les_host_fields *hf) {
+    const int ip = c->prm.ip, jp = c->prm.jp, kp = c->prm.kp;
+    const TableLayout &t = c->tl;
+    std::vector<float> &h = c->h_tables;
+    h.assign(t.total, 0.0f);
+    auto cp = [&](size_t off, const float *src, size_t n) {
+        if (src) std::memcpy(&h[off], src, n * sizeof(float));
+    };
+    cp(t.dx1, hf->dx1, ip + 3);  // -1..ip+1
+    cp(t.dy1, hf->dy1, jp + 2);  // 0..jp+1
+    cp(t.dzn, hf->dzn, kp + 4);  // -1..kp+2
+    cp(t.dzs, hf->dzs, kp + 4);
+    cp(t.dxs, hf->dxs, ip + 1);  // 0..ip
+    cp(t.dys, hf->dys, jp + 1);
+    cp(t.cn2l, hf->cn2l, ip);  // 1..ip
+    cp(t.cn2s, hf->cn2s, ip);
+    cp(t.cn3l, hf->cn3l, jp);
+    cp(t.cn3s, hf->cn3s, jp);
+    cp(t.cn4l, hf->cn4l, kp);
+    cp(t.cn4s, hf->cn4s, kp);
+    auto dx1 = [&](int i) { return h[t.dx1 + i + 1]; };
+    auto dy1 = [&](int j) { return h[t.dy1 + j]; };
+    auto dzn = [&](int k) { return h[t.dzn + k + 1]; };
+    auto dzs = [&](int k) { return h[t.dzs + k + 1]; };
+    auto dxs = [&](int i) { return h[t.dxs + i]; };
+    auto dys = [&](int j) { return h[t.dys + j]; };
+    // init.f95:87-93 separable parts of cn1
+    for (int i = 1; i <= ip; ++i) h[t.cnA + i - 1] = 2.0f / (dxs(i - 1) * dxs(i));
+    for (int j = 1; j <= jp; ++j) h[t.cnB + j - 1] = 2.0f / (dys(j - 1) * dys(j));
+    for (int k = 1; k <= kp; ++k) h[t.cnC + k - 1] = 2.0f / (dzs(k - 1) * dzs(k));
+    // les.f95:125-129, 146-148
+    for (int k = 1; k <= kp; ++k) {
+        const float delx1 = powf(dx1(0) * dy1(0) * dzn(k), 1.0f / 3.0f);
+        const float cd = c->prm.cs0 * delx1;
+        h[t.smc + k - 1] = cd * cd;
+    }
+    // inflow table: bondv1.f95:26-45 power law or the external profile
+    if (c->prm.inflow_mode == LES_INFLOW_EXTERNAL) {
+        if (!hf->wind_profile) return fail(LES_ERR_BAD_ARG, "external inflow needs wind_profile");
+        std::memcpy(&h[t.wind], hf->wind_profile, sizeof(float) * (size_t)jp * kp);
+    } else {
+        if (!hf->z2) return fail(LES_ERR_BAD_ARG, "power-law inflow needs z2");
+        std::vector<float> col(kp + 1);
+        for (int k = 1; k <= kp; ++k) {
+            if (k <= 78) {
+                col[k] = 5.0f * powf((hf->z2[k - 1] + 0.5f * dzn(k)) / 600.0f, 0.2f);
+            } else {
+                col[k] = col[77];
+            }
+        }
+        for (int k = 1; k <= kp; ++k)
+            for (int j = 1; j <= jp; ++j) h[t.wind + (j - 1) + (size_t)jp * (k - 1)] = col[k];
+    }
+    // grid-only denominator of rhsav and pav (press.f95:134, 192)
+    i128 acc = 0;
+    int bad = 0;
+    for (int k = 1; k <= kp; ++k)
+        for (int j = 1; j <= jp; ++j)
+            for (int i = 1; i <= ip; ++i) acc += fix_term(dx1(i) * dy1(j) * dzn(k), bad);
+    c->area = fix_finish(acc, bad);
+    CK(cudaMemcpyAsync(c->d_tables, h.data(), sizeof(float) * t.total, cudaMemcpyHostToDevice, c->stream));
+    return ok();
+}
+
+// Phase boundaries recorded by the timing events (les_ctx_phase_times).
+enum { EV_START = 0, EV_BONDV1, EV_VELFG, EV_VISC, EV_RHS, EV_SOR1_START, EV_SOR1_END, EV_SOR_END, EV_PAV, LES_NTEV };
+
+les_status mark(les_ctx *c, int which) {
+    if (!c->capturing_timed) return LES_OK;
+    CK(cudaEventRecordWithFlags(c->tev[which], c->stream, cudaEventRecordExternal));
+    return LES_OK;
+}
+#define MARK(c, w)                                     \
+    do {                                               \
+        les_status ms_ = mark((c), (w));               \
+        if (ms_ != LES_OK) return ms_;                 \
+    } while (0)
+
+// Kernel launch helpers; each counts one launch.
+#define LAUNCH(c, kern, grid, block, ...)                          \
+    do {                                                           \
+        kern<<<(grid), (block), 0, (c)->stream>>>(__VA_ARGS__);    \
+        CKL();                                                     \
+        ++(c)->launches;                                           \
+    } while (0)
+
+dim3 cells_grid(const Geo &g, int i0) {  // i from i0, 32 x 4 blocks, z = k
+    return dim3(cdiv(g.im - i0 + 1, 32), cdiv(g.jm, 4), g.km);
+}
+
+les_status enqueue_bondv1(les_ctx *c, int n, bool velnw) {
+    const Geo &g = c->geo;
+    if (velnw)
+        LAUNCH(c, k_velnw_inflow<true>, cells_grid(g, 0), dim3(32, 4), g, c->F, n, c->prm.ical);
+    else
+        LAUNCH(c, k_velnw_inflow<false>, cells_grid(g, 0), dim3(32, 4), g, c->F, n, c->prm.ical);
+    LAUNCH(c, k_uout_reduce, dim3(cdiv((long long)g.jm * g.km, 256 * 8)), dim3(256), g, c->F.u, c->d_scal);
+    LAUNCH(c, k_outflow, dim3(cdiv((long long)g.jm * g.km, 256)), dim3(256), g, c->F, c->d_scal);
+    const long long ng = 2LL * g.km * (g.im + 2) + 2LL * (g.jm + 2) * (g.im + 2) + 2LL * (g.jm + 3) * (g.im + 2);
+    LAUNCH(c, k_uvw_ghosts, dim3(cdiv(ng, 256)), dim3(256), g, c->F);
+    return LES_OK;
+}
+
+les_status enqueue_velfg_les(les_ctx *c, bool adam) {
+    const Geo &g = c->geo;
+    LAUNCH(c, k_velfg_feedbf_sm, cells_grid(g, 1), dim3(32, 4), g, c->F);
+    MARK(c, EV_VELFG);
+    const long long nb = 2LL * (g.jm + 3) * (g.km + 2) + 2LL * g.im * (g.km + 2) + 2LL * g.im * (g.jm + 1);
+    LAUNCH(c, k_boundsm, dim3(cdiv(nb, 256)), dim3(256), g, c->F.sm);
+    if (adam)
+        LAUNCH(c, k_visc<true>, cells_grid(g, 1), dim3(32, 4), g, c->F);
+    else
+        LAUNCH(c, k_visc<false>, cells_grid(g, 1), dim3(32, 4), g, c->F);
+    MARK(c, EV_VISC);
+    return LES_OK;
+}
+
+les_status enqueue_boundp(les_ctx *c, bool check) {
+    const Geo &g = c->geo;
+    const long long n1 = 2LL * (g.jm + 2) * (g.km + 2) + 2LL * g.im * (g.km + 2);
+    const long long n2 = 2LL * (g.im + 2) * (g.jm + 2);
+    if (check) {
+        LAUNCH(c, k_boundp1<true>, dim3(cdiv(n1, 256)), dim3(256), g, c->F.p, c->d_scal);
+    } else {
+        LAUNCH(c, k_boundp1<false>, dim3(cdiv(n1, 256)), dim3(256), g, c->F.p, c->d_scal);
+        LAUNCH(c, k_boundp2<false>, dim3(cdiv(n2, 256)), dim3(256), g, c->F.p, c->d_scal);
+    }
+    return LES_OK;
+}
+
+les_status enqueue_press(les_ctx *c) {
+    const Geo &g = c->geo;
+    const dim3 rg(c->red_gx, c->red_gy, c->red_nk), rb(kRedBX, kRedBY);
+    const int np = c->red_gx * c->red_gy * c->red_nk;
+    const long long n1 = 2LL * (g.jm + 2) * (g.km + 2) + 2LL * g.im * (g.km + 2);
+    const long long n2 = 2LL * (g.im + 2) * (g.jm + 2);
+    LAUNCH(c, k_rhs, rg, rb, g, c->F, c->red_kchunk, c->d_part);
+    LAUNCH(c, k_final_rhsav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
+    MARK(c, EV_RHS);
+    for (int l = 0; l < c->prm.nmaxp; ++l) {
+        for (int nrd = 0; nrd <= 1; ++nrd) {
+            if (l == 0 && nrd == 0) MARK(c, EV_SOR1_START);
+            LAUNCH(c, k_sor_colour, rg, rb, g, c->F.p, c->F.rhs, nrd, c->red_kchunk, c->d_part + nrd * np, c->d_scal);
+            if (l == 0 && nrd == 0) MARK(c, EV_SOR1_END);
+            LAUNCH(c, k_boundp1<true>, dim3(cdiv(n1, 256)), dim3(256), g, c->F.p, c->d_scal);
+        }
+        LAUNCH(c, k_boundp2<true>, dim3(cdiv(n2, 256)), dim3(256), g, c->F.p, c->d_scal);
+        LAUNCH(c, k_final_sor, dim3(1), dim3(1024), c->d_part, 2 * np, c->prm.pjuge, c->d_scal);
+    }
+    MARK(c, EV_SOR_END);
+    LAUNCH(c, k_pav_reduce, rg, rb, g, c->F.p, c->red_kchunk, c->d_part);
+    LAUNCH(c, k_final_pav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
+    LAUNCH(c, k_pav_adjust, dim3(c->red_gx, c->red_gy, g.km), rb, g, c->F.p, c->d_scal);
+    MARK(c, EV_PAV);
+    return LES_OK;
+}
+
+// One time step after k_step_begin (main_ocl.f95:264-299).
+les_status enqueue_step(les_ctx *c, int n) {
+    les_status s;
+    MARK(c, EV_START);
+    if ((s = enqueue_bondv1(c, n, true)) != LES_OK) return s;
+    MARK(c, EV_BONDV1);
+    if ((s = enqueue_velfg_les(c, true)) != LES_OK) return s;
+    if ((s = enqueue_press(c)) != LES_OK) return s;
+    LAUNCH(c, k_probe, dim3(1), dim3(1), c->geo, c->F, c->d_scal);
+    return LES_OK;
+}
+
+les_status check_params(const les_params *p) {
+    if (!p) return fail(LES_ERR_BAD_ARG, "params is NULL");
+    if (p->ip < 2 || p->jp < 2 || p->kp < 3) return fail(LES_ERR_DIMS, "grid %dx%dx%d too small", p->ip, p->jp, p->kp);
+    if (p->inflow_mode == LES_INFLOW_POWER_LAW && p->kp < 78)
+        return fail(LES_ERR_DIMS, "bondv1 power-law inflow sets k=1..78 (bondv1.f95:26): kp=%d < 78", p->kp);
+    if (p->inflow_mode != LES_INFLOW_POWER_LAW && p->inflow_mode != LES_INFLOW_EXTERNAL)
+        return fail(LES_ERR_BAD_ARG, "bad inflow_mode %d", p->inflow_mode);
+    if (p->nmaxp < 0) return fail(LES_ERR_BAD_ARG, "nmaxp < 0");
+    // set.f95:84-88: the IBM feedback gains bound the time step
+    if (((-p->beta - powf(p->beta * p->beta - 2.0f * p->alpha, 0.5f)) / p->alpha) < p->dt)
+        return fail(LES_ERR_BAD_ARG, "CHECK parameter alpha beta of IBM method (set.f95:84): dt too large");
+    const long long si = ((kOX + p->ip + 3) + 31) / 32 * 32;
+    const long long tot = si * (p->jp + 4LL) * (p->kp + 4LL);
+    if (tot >= (1LL << 31)) return fail(LES_ERR_DIMS, "grid too large for 32-bit box indexing");
+    return LES_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *les_last_error_string(void) { return g_err.c_str(); }
+
+const char *les_version(void) { return "lesb200 0.1 (sm_100a)"; }
+
+les_status les_params_default(les_params *p, int ip, int jp, int kp) {
+    if (!p) return fail(LES_ERR_BAD_ARG, "params is NULL");
+    std::memset(p, 0, sizeof *p);
+    p->ip = ip;
+    p->jp = jp;
+    p->kp = kp;
+    p->dt = 0.2f;
+    p->ro = 1.1763f;
+    p->vn = 15.83f * powf(10.0f, -6.0f);
+    p->alpha = -10.0f;
+    p->beta = -1.0f;
+    p->cs0 = 0.1f;
+    p->nmaxp = 50;
+    p->pjuge = 0.0001f;
+    p->omega = 1.0f;
+    p->inflow_mode = LES_INFLOW_POWER_LAW;
+    p->ical = 0;
+    return ok();
+}
+
+les_status les_ctx_create(const les_params *prm, les_ctx **out) {
+    if (!out) return fail(LES_ERR_BAD_ARG, "out is NULL");
+    *out = nullptr;
+    les_status s = check_params(prm);
+    if (s != LES_OK) return s;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(LES_ERR_CUDA, "no CUDA device");
+    }
+    les_ctx *c = new les_ctx();
+    c->prm = *prm;
+    const int ip = prm->ip, jp = prm->jp, kp = prm->kp;
+    Geo &g = c->geo;
+    g.im = ip;
+    g.jm = jp;
+    g.km = kp;
+    g.ox = kOX;
+    g.si = ((kOX + ip + 3) + 31) / 32 * 32;
+    g.sj = jp + 4;
+    g.sk = kp + 4;
+    g.dt = prm->dt;
+    g.ro = prm->ro;
+    g.vn = prm->vn;
+    g.alpha = prm->alpha;
+    g.beta = prm->beta;
+    g.omega = prm->omega;
+    c->box_elems = (size_t)g.si * g.sj * g.sk;
+    auto cleanup = [&](les_status st) {
+        les_ctx_destroy(c);
+        return st;
+    };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(LES_ERR_CUDA, "cudaStreamCreate failed"));
+    if (cudaMalloc(&c->d_fields, sizeof(float) * c->box_elems * LES_NFIELDS) != cudaSuccess) {
+        cudaGetLastError();
+        return cleanup(fail(LES_ERR_NOMEM, "cannot allocate %.2f GB of fields",
+                            sizeof(float) * c->box_elems * LES_NFIELDS / 1e9));
+    }
+    if (cudaMemsetAsync(c->d_fields, 0, sizeof(float) * c->box_elems * LES_NFIELDS, c->stream) != cudaSuccess)
+        return cleanup(fail(LES_ERR_CUDA, "memset fields"));
+    c->tl = table_layout(ip, jp, kp);
+    if (cudaMalloc(&c->d_tables, sizeof(float) * c->tl.total) != cudaSuccess)
+        return cleanup(fail(LES_ERR_NOMEM, "tables"));
+    if (cudaMalloc(&c->d_scal, sizeof(Scal)) != cudaSuccess) return cleanup(fail(LES_ERR_NOMEM, "scalars"));
+    cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream);
+    // reduction grid: 32x8 blocks over (i,j), k split so there are >= 4 blocks per SM
+    c->red_gx = cdiv(ip, kRedBX);
+    c->red_gy = cdiv(jp, kRedBY);
+    int nk = cdiv(4 * 148, (long long)c->red_gx * c->red_gy);
+    nk = nk < 1 ? 1 : (nk > kp ? kp : nk);
+    c->red_kchunk = cdiv(kp, nk);
+    c->red_nk = cdiv(kp, c->red_kchunk);
+    c->npart = 2 * c->red_gx * c->red_gy * c->red_nk;
+    if (cudaMalloc(&c->d_part, sizeof(FixPart) * c->npart) != cudaSuccess)
+        return cleanup(fail(LES_ERR_NOMEM, "partials"));
+    // staging buffer for Fortran-layout arrays (largest: w or p)
+    size_t mx = 0;
+    for (int f = 0; f < LES_NFIELDS; ++f) mx = std::max(mx, field_bounds(f, ip, jp, kp).n());
+    c->stage_elems = mx;
+    if (cudaMalloc(&c->d_stage, sizeof(float) * mx) != cudaSuccess) return cleanup(fail(LES_ERR_NOMEM, "stage"));
+    float *base = c->d_tables;
+    const TableLayout &t = c->tl;
+    g.dx1 = base + t.dx1 + 1;
+    g.dy1 = base + t.dy1;
+    g.dzn = base + t.dzn + 1;
+    g.dzs = base + t.dzs + 1;
+    g.dxs = base + t.dxs;
+    g.dys = base + t.dys;
+    g.cn2l = base + t.cn2l - 1;
+    g.cn2s = base + t.cn2s - 1;
+    g.cn3l = base + t.cn3l - 1;
+    g.cn3s = base + t.cn3s - 1;
+    g.cn4l = base + t.cn4l - 1;
+    g.cn4s = base + t.cn4s - 1;
+    g.cnA = base + t.cnA - 1;
+    g.cnB = base + t.cnB - 1;
+    g.cnC = base + t.cnC - 1;
+    g.smc = base + t.smc - 1;
+    g.wind = base + t.wind;
+    float **fp[LES_NFIELDS] = {&c->F.u,    &c->F.v,    &c->F.w,    &c->F.p,     &c->F.usum,  &c->F.vsum,  &c->F.wsum,
+                               &c->F.f,    &c->F.g,    &c->F.h,    &c->F.fold,  &c->F.gold,  &c->F.hold,  &c->F.rhs,
+                               &c->F.sm,   &c->F.amask, &c->F.bmask, &c->F.cmask, &c->F.dmask};
+    for (int f = 0; f < LES_NFIELDS; ++f) *fp[f] = field_ptr(c, f);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cleanup(fail(LES_ERR_CUDA, "sync"));
+    *out = c;
+    return ok();
+}
+
+les_status les_ctx_destroy(les_ctx *c) {
+    if (!c) return ok();
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &ge : c->graph)
+        if (ge) cudaGraphExecDestroy(ge);
+    for (auto &gs : c->graph_src)
+        if (gs) cudaGraphDestroy(gs);
+    for (auto e : c->tev) cudaEventDestroy(e);
+    cudaFree(c->d_fields);
+    cudaFree(c->d_tables);
+    cudaFree(c->d_scal);
+    cudaFree(c->d_part);
+    cudaFree(c->d_stage);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ok();
+}
+
+void *les_ctx_stream(les_ctx *c) { return c ? (void *)c->stream : nullptr; }
+uint64_t les_ctx_launch_count(les_ctx *c) { return c ? c->launches : 0; }
+
+les_status les_ctx_field(les_ctx *c, int field, float **dptr, int *ox, int *si, int *sj, int *sk) {
+    if (!c || field < 0 || field >= LES_NFIELDS) return fail(LES_ERR_BAD_ARG, "bad field");
+    if (dptr) *dptr = field_ptr(c, field);
+    if (ox) *ox = c->geo.ox;
+    if (si) *si = c->geo.si;
+    if (sj) *sj = c->geo.sj;
+    if (sk) *sk = c->geo.sk;
+    return ok();
+}
+
+static les_status upload_field(les_ctx *c, int f, const float *host) {
+    if (!host) return LES_OK;
+    const FBounds b = field_bounds(f, c->prm.ip, c->prm.jp, c->prm.kp);
+    CK(cudaMemcpyAsync(c->d_stage, host, sizeof(float) * b.n(), cudaMemcpyHostToDevice, c->stream));
+    LAUNCH(c, k_f2box, dim3(cdiv((long long)b.n(), 256 * 4)), dim3(256), c->geo, field_ptr(c, f), c->d_stage, b.li,
+           b.lj, b.lk, b.ni(), b.nj(), b.nk());
+    return LES_OK;
+}
+
+static les_status download_field(les_ctx *c, int f, float *host) {
+    if (!host) return LES_OK;
+    const FBounds b = field_bounds(f, c->prm.ip, c->prm.jp, c->prm.kp);
+    // rhs is kept before the rhsav subtraction; the caller gets
+    // rhs - rhsav on the interior as press.f95:139-145 leaves it.
+    const bool sub = (f == LES_F_RHS) && c->rhs_raw;
+    float rhsav = 0.0f;
+    if (sub) {
+        Scal sc;
+        CK(cudaMemcpyAsync(&sc, c->d_scal, sizeof sc, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        rhsav = sc.rhsav;
+    }
+    LAUNCH(c, k_box2f, dim3(cdiv((long long)b.n(), 256 * 4)), dim3(256), c->geo, field_ptr(c, f), c->d_stage, b.li,
+           b.lj, b.lk, b.ni(), b.nj(), b.nk(), rhsav, sub ? 1 : 0);
+    CK(cudaMemcpyAsync(host, c->d_stage, sizeof(float) * b.n(), cudaMemcpyDeviceToHost, c->stream));
+    return LES_OK;
+}
+
+les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
+    if (!c || !hf) return fail(LES_ERR_BAD_ARG, "NULL argument");
+    if (!hf->dx1 || !hf->dy1 || !hf->dzn || !hf->dzs || !hf->dxs || !hf->dys || !hf->cn2l || !hf->cn2s ||
+        !hf->cn3l || !hf->cn3s || !hf->cn4l || !hf->cn4s)
+        return fail(LES_ERR_BAD_ARG, "metric tables and Poisson coefficients are required");
+    les_status s = build_tables(c, hf);
+    if (s != LES_OK) return s;
+    const float *src[LES_NFIELDS] = {hf->u,    hf->v,    hf->w,    hf->p,   hf->usum,   hf->vsum,   hf->wsum,
+                                     hf->f,    hf->g,    hf->h,    hf->fold, hf->gold,  hf->hold,   hf->rhs,
+                                     hf->sm,   hf->amask1, hf->bmask1, hf->cmask1, hf->dmask1};
+    for (int f = 0; f < LES_NFIELDS; ++f)
+        if ((s = upload_field(c, f, src[f])) != LES_OK) return s;
+    // cn1 is rebuilt from its separable parts in the SOR kernel; a caller's
+    // cn1 must equal init.f95:87-93 bit for bit.
+    if (hf->cn1) {
+        const int ip = c->prm.ip, jp = c->prm.jp, kp = c->prm.kp;
+        const std::vector<float> &h = c->h_tables;
+        for (int k = 1; k <= kp; ++k)
+            for (int j = 1; j <= jp; ++j)
+                for (int i = 1; i <= ip; ++i) {
+                    const float want = 1.0f / (h[c->tl.cnA + i - 1] + h[c->tl.cnB + j - 1] + h[c->tl.cnC + k - 1]);
+                    const float got = hf->cn1[(size_t)(i - 1) + (size_t)ip * ((j - 1) + (size_t)jp * (k - 1))];
+                    if (std::memcmp(&want, &got, 4) != 0)
+                        return fail(LES_ERR_BAD_ARG,
+                                    "cn1(%d,%d,%d) differs from 1/(2/(dxs*dxs)+2/(dys*dys)+2/(dzs*dzs)) (init.f95:87-93)",
+                                    i, j, k);
+                }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->uploaded = true;
+    c->rhs_raw = false;
+    return ok();
+}
+
+les_status les_ctx_download(les_ctx *c, les_host_fields *hf) {
+    if (!c || !hf) return fail(LES_ERR_BAD_ARG, "NULL argument");
+    float *dst[LES_NFIELDS] = {hf->u,  hf->v,  hf->w,    hf->p,    hf->usum, hf->vsum,   hf->wsum,
+                               hf->f,  hf->g,  hf->h,    hf->fold, hf->gold, hf->hold,   hf->rhs,
+                               hf->sm, hf->amask1, hf->bmask1, hf->cmask1, hf->dmask1};
+    les_status s;
+    for (int f = 0; f < LES_NFIELDS; ++f) {
+        if ((s = download_field(c, f, dst[f])) != LES_OK) return s;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (hf->delx1) {
+        for (int k = 1; k <= c->prm.kp; ++k) {
+            const float *h = c->h_tables.data();
+            hf->delx1[k - 1] = powf(h[c->tl.dx1 + 1] * h[c->tl.dy1] * h[c->tl.dzn + k + 1], 1.0f / 3.0f);
+        }
+    }
+    return ok();
+}
+
+les_status les_ctx_warmup(les_ctx *c, int n) {
+    if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    if (!c->uploaded) return fail(LES_ERR_STATE, "warmup before upload");
+    les_status s;
+    LAUNCH(c, k_step_begin, dim3(1), dim3(1), c->d_scal, n);
+    LAUNCH(c, k_zero_fgh, dim3(cdiv((long long)(c->prm.ip + 1) * (c->prm.jp + 1) * (c->prm.kp + 1), 1024)), dim3(256),
+           c->geo, c->F);
+    if ((s = enqueue_bondv1(c, n, false)) != LES_OK) return s;
+    if ((s = enqueue_boundp(c, false)) != LES_OK) return s;
+    if ((s = enqueue_velfg_les(c, false)) != LES_OK) return s;
+    CK(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+
+les_status les_set_wind_profile(les_ctx *c, const float *wp) {
+    if (!c || !wp) return fail(LES_ERR_BAD_ARG, "NULL argument");
+    if (c->prm.inflow_mode != LES_INFLOW_EXTERNAL) return fail(LES_ERR_STATE, "context uses the power-law inflow");
+    CK(cudaMemcpyAsync(c->d_tables + c->tl.wind, wp, sizeof(float) * (size_t)c->prm.jp * c->prm.kp,
+                       cudaMemcpyHostToDevice, c->stream));
+    return ok();
+}
+
+les_status les_step(les_ctx *c, int n0, int nsteps) {
+    if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    if (!c->uploaded) return fail(LES_ERR_STATE, "step before upload");
+    if (nsteps < 0) return fail(LES_ERR_BAD_ARG, "nsteps < 0");
+    for (int s = 0; s < nsteps; ++s) {
+        const int n = n0 + s;
+        const int gi = (n == 1 && c->prm.ical == 0) ? 1 : 0;
+        if (!c->graph[gi]) {
+            // Capture the step once per kind (n==1 broadcast or not); the
+            // kernels only see n through that distinction.
+            const uint64_t before = c->launches;
+            c->capturing_timed = c->tslots > 0;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            les_status st = enqueue_step(c, gi ? 1 : 2);
+            cudaGraph_t gr = nullptr;
+            cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+            c->capturing_timed = false;
+            c->graph_kernels[gi] = c->launches - before;
+            c->launches = before;  // capturing runs nothing
+            if (st != LES_OK) {
+                if (gr) cudaGraphDestroy(gr);
+                return st;
+            }
+            if (e != cudaSuccess) return fail(LES_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&c->graph[gi], gr, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(gr);
+                return fail(LES_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+            }
+            c->graph_src[gi] = gr;
+            c->tnode[gi].clear();
+            c->tnode_idx[gi].clear();
+            if (c->tslots > 0) {  // find the event record nodes and which event each records
+                size_t nn = 0;
+                CK(cudaGraphGetNodes(gr, nullptr, &nn));
+                std::vector<cudaGraphNode_t> nodes(nn);
+                CK(cudaGraphGetNodes(gr, nodes.data(), &nn));
+                for (auto nd : nodes) {
+                    cudaGraphNodeType ty;
+                    CK(cudaGraphNodeGetType(nd, &ty));
+                    if (ty != cudaGraphNodeTypeEventRecord) continue;
+                    cudaEvent_t ev;
+                    CK(cudaGraphEventRecordNodeGetEvent(nd, &ev));
+                    for (int w = 0; w < LES_NTEV; ++w)
+                        if (ev == c->tev[w]) {
+                            c->tnode[gi].push_back(nd);
+                            c->tnode_idx[gi].push_back(w);
+                        }
+                }
+            }
+        }
+        if (c->tslots > 0) {
+            const int slot = c->tslot < c->tslots ? c->tslot : c->tslots - 1;
+            for (size_t q = 0; q < c->tnode[gi].size(); ++q)
+                CK(cudaGraphExecEventRecordNodeSetEvent(c->graph[gi], c->tnode[gi][q],
+                                                        c->tev[(size_t)slot * LES_NTEV + c->tnode_idx[gi][q]]));
+            if (c->tslot < c->tslots) ++c->tslot;
+        }
+        LAUNCH(c, k_step_begin, dim3(1), dim3(1), c->d_scal, n);
+        CK(cudaGraphLaunch(c->graph[gi], c->stream));
+        c->launches += c->graph_kernels[gi];
+        c->last_n = n;
+        c->rhs_raw = true;
+    }
+    return ok();
+}
+
+les_status les_ctx_set_timing(les_ctx *c, int nslots) {
+    if (!c || nslots < 0) return fail(LES_ERR_BAD_ARG, "bad argument");
+    CK(cudaStreamSynchronize(c->stream));
+    if ((nslots > 0) != (c->tslots > 0)) {  // graphs are re-captured with or without event nodes
+        for (int gi = 0; gi < 2; ++gi) {
+            if (c->graph[gi]) cudaGraphExecDestroy(c->graph[gi]);
+            if (c->graph_src[gi]) cudaGraphDestroy(c->graph_src[gi]);
+            c->graph[gi] = nullptr;
+            c->graph_src[gi] = nullptr;
+        }
+    }
+    // event nodes of existing graphs are re-pointed before every launch, so
+    // the pool can be replaced freely
+    for (auto e : c->tev) cudaEventDestroy(e);
+    c->tev.assign((size_t)nslots * LES_NTEV, nullptr);
+    for (auto &e : c->tev) CK(cudaEventCreate(&e));
+    c->tslots = nslots;
+    c->tslot = 0;
+    return ok();
+}
+
+les_status les_ctx_phase_times(les_ctx *c, int slot, float *ms, int n) {
+    if (!c || !ms || slot < 0 || slot >= c->tslots) return fail(LES_ERR_BAD_ARG, "bad slot");
+    CK(cudaStreamSynchronize(c->stream));
+    // ms[0..7]: consecutive phases between the events; ms[8]: whole step
+    for (int w = 0; w < LES_NTEV && w < n; ++w) {
+        const int a = (w == LES_NTEV - 1) ? EV_START : w, b = (w == LES_NTEV - 1) ? EV_PAV : w + 1;
+        CK(cudaEventElapsedTime(&ms[w], c->tev[(size_t)slot * LES_NTEV + a], c->tev[(size_t)slot * LES_NTEV + b]));
+    }
+    return ok();
+}
+
+les_status les_ctx_sync(les_ctx *c) {
+    if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    CK(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+
+les_status les_last_metrics(les_ctx *c, les_metrics *m) {
+    if (!c || !m) return fail(LES_ERR_BAD_ARG, "NULL argument");
+    Scal s;
+    CK(cudaMemcpyAsync(&s, c->d_scal, sizeof s, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    m->n = s.n;
+    m->sor_iters = s.sor_iters;
+    m->sor = s.sor;
+    m->rhsav = s.rhsav;
+    m->pav = s.pav;
+    m->uout = s.uout;
+    m->p_centre = s.probe[0];
+    m->u_centre = s.probe[1];
+    m->v_centre = s.probe[2];
+    m->w_centre = s.probe[3];
+    return ok();
+}
+
+// ---- context halo (TEMPL:111-127, LES_combined_kernel.cl:345-364) ----
+static bool ctx_halo_view(les_ctx *c, int which, CombView &cv, HaloDims &d) {
+    const int ip = c->prm.ip, jp = c->prm.jp, kp = c->prm.kp;
+    std::memset(&cv, 0, sizeof cv);
+    int ext[3] = {0, 0, 0}, vdim = 1;
+    Fields &F = c->F;
+    switch (which) {
+        case LES_H_P:  // p2 = float2(p, p), (0:ip+2,0:jp+2,0:kp+1)
+            cv.comp[0] = F.p;
+            cv.comp[1] = F.p;
+            vdim = 2;
+            ext[0] = ip + 3, ext[1] = jp + 3, ext[2] = kp + 2;
+            cv.li = 0, cv.lj = 0, cv.lk = 0;
+            break;
+        case LES_H_UVW:  // float4(u,v,w,0), (0:ip+1,-1:jp+1,-1:kp+1); u,v start at k=0
+            cv.comp[0] = F.u, cv.comp[1] = F.v, cv.comp[2] = F.w;
+            cv.klo[0] = 0, cv.klo[1] = 0, cv.klo[2] = -1, cv.klo[3] = -1;
+            vdim = 4;
+            ext[0] = ip + 2, ext[1] = jp + 3, ext[2] = kp + 3;
+            cv.li = 0, cv.lj = -1, cv.lk = -1;
+            break;
+        case LES_H_UVWSUM:
+        case LES_H_FGH:
+            if (which == LES_H_UVWSUM)
+                cv.comp[0] = F.usum, cv.comp[1] = F.vsum, cv.comp[2] = F.wsum;
+            else
+                cv.comp[0] = F.f, cv.comp[1] = F.g, cv.comp[2] = F.h;
+            vdim = 4;
+            ext[0] = ip + 1, ext[1] = jp + 1, ext[2] = kp + 1;
+            break;
+        case LES_H_FGH_OLD:
+            cv.comp[0] = F.fold, cv.comp[1] = F.gold, cv.comp[2] = F.hold;
+            vdim = 4;
+            ext[0] = ip, ext[1] = jp, ext[2] = kp;
+            cv.li = 1, cv.lj = 1, cv.lk = 1;
+            break;
+        case LES_H_RHS:
+            cv.comp[0] = F.rhs;
+            ext[0] = ip + 2, ext[1] = jp + 2, ext[2] = kp + 2;
+            break;
+        case LES_H_SM:
+            cv.comp[0] = F.sm;
+            ext[0] = ip + 3, ext[1] = jp + 3, ext[2] = kp + 2;
+            cv.li = -1, cv.lj = -1, cv.lk = 0;
+            break;
+        default: return false;
+    }
+    if (which != LES_H_UVW)
+        for (int v = 0; v < 4; ++v) cv.klo[v] = cv.lk;
+    d = halo_dims(ext[0], ext[1], ext[2], 1, vdim, 0);
+    return true;
+}
+
+size_t les_ctx_halo_floats(les_ctx *c, int which) {
+    CombView cv;
+    HaloDims d;
+    if (!c || !ctx_halo_view(c, which, cv, d)) return 0;
+    return d.vsz * d.vdim;
+}
+
+static les_status ctx_halo(les_ctx *c, int which, float *buf, int write) {
+    CombView cv;
+    HaloDims d;
+    if (!c || !buf) return fail(LES_ERR_BAD_ARG, "NULL argument");
+    if (!ctx_halo_view(c, which, cv, d)) return fail(LES_ERR_BAD_ARG, "bad halo id %d", which);
+    const size_t n = d.vsz * d.vdim;
+    if (n > c->stage_elems) return fail(LES_ERR_DIMS, "halo larger than the staging buffer");
+    if (write) CK(cudaMemcpyAsync(c->d_stage, buf, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+    LAUNCH(c, k_ctx_halo, dim3(cdiv((long long)n, 256)), dim3(256), c->geo, cv, c->d_stage, d, write);
+    if (!write) CK(cudaMemcpyAsync(buf, c->d_stage, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+les_status les_ctx_halo_read(les_ctx *c, int which, float *buf) { return ctx_halo(c, which, buf, 0); }
+les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
+    return ctx_halo(c, which, const_cast<float *>(buf), 1);
+}
+
+}  // extern "C"

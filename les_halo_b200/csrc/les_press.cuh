@@ -1,0 +1,250 @@
+// les_press.cuh -- pressure part of the time step (press.f95:49-146).
+//
+// Global sums use the exact fixed-point definition of les_fix.h: each
+// reducing kernel writes one FixPart per block to a scratch array and a
+// one-block kernel finishes the total.  The SOR loop runs on the device
+// without host round trips: the residual kernel sets a converged flag and
+// every later kernel of the loop returns at once when it is set.
+#pragma once
+#include "les_dev.cuh"
+
+namespace les {
+namespace {  // kernels get internal linkage: each .cu has its own copy
+
+constexpr int kRedBX = 32, kRedBY = 8, kRedNT = kRedBX * kRedBY;
+
+// bondFG.f95:15-31 fused with the rhs of press.f95:114-125 and the partial
+// sums of press.f95:128-137.  rhs is stored before the rhsav subtraction
+// (every reader subtracts the scalar itself).  Threads loop over a k chunk.
+__global__ void __launch_bounds__(kRedNT) k_rhs(Geo g, Fields F, int kchunk, FixPart *part) {
+    const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
+    const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
+    const int k0 = 1 + blockIdx.z * kchunk;
+    const int k1 = min(g.km, k0 + kchunk - 1);
+    i128 acc = 0;
+    int bad = 0;
+    if (i <= g.im && j <= g.jm) {
+        const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn;
+        for (int k = k0; k <= k1; ++k) {
+            const int c = IX(g, i, j, k);
+            const float fc = F.f[c], gc = F.g[c];
+            float hc = F.h[c];
+            // bondfg: f(0,j,k)=f(1,j,k); g(i,0,k)=g(i,jm,k); h(i,j,0)=h(i,j,km)=0
+            if (i == 1) F.f[IX(g, 0, j, k)] = fc;
+            if (j == g.jm) F.g[IX(g, i, 0, k)] = gc;
+            if (k == g.km) {
+                F.h[c] = 0.0f;
+                hc = 0.0f;
+            }
+            if (k == 1) F.h[IX(g, i, j, 0)] = 0.0f;
+            const float fm = (i == 1) ? fc : F.f[IX(g, i - 1, j, k)];
+            const float gm = (j == 1) ? F.g[IX(g, i, g.jm, k)] : F.g[IX(g, i, j - 1, k)];
+            const float hm = (k == 1) ? 0.0f : F.h[IX(g, i, j, k - 1)];
+            float r = (-F.u[IX(g, i - 1, j, k)] + F.u[c]) / dx1[i] + (-F.v[IX(g, i, j - 1, k)] + F.v[c]) / dy1[j] +
+                      (-F.w[IX(g, i, j, k - 1)] + F.w[c]) / dzn[k];
+            r = (fc - fm) / dx1[i] + (gc - gm) / dy1[j] + (hc - hm) / dzn[k] + r / g.dt;
+            F.rhs[c] = r;
+            acc += fix_term(dx1[i] * dy1[j] * dzn[k] * r, bad);
+        }
+    }
+    block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
+}
+
+// Sum FixParts with one block; the finisher maps the total to the scalars.
+__device__ __forceinline__ void final_fix(const FixPart *part, int n, i128 &tot, int &bad) {
+    __shared__ unsigned long long s_lo[32];
+    __shared__ long long s_hi[32];
+    __shared__ int s_bad[32];
+    i128 acc = 0;
+    int b = 0;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        acc += fix_from_part(part[t]);
+        b |= part[t].bad;
+    }
+    for (int off = 16; off >= 1; off >>= 1) {
+        acc += shfl_down_i128(acc, off);
+        b |= __shfl_down_sync(0xffffffffu, b, off);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_lo[wid] = (unsigned long long)acc;
+        s_hi[wid] = (long long)(acc >> 64);
+        s_bad[wid] = b;
+    }
+    __syncthreads();
+    tot = 0;
+    bad = 0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            tot += (i128)(((unsigned __int128)(unsigned long long)s_hi[w] << 64) | (unsigned __int128)s_lo[w]);
+            bad |= s_bad[w];
+        }
+    }
+}
+
+// rhsav = num/area (press.f95:138), area given (grid-only, finished on the host).
+__global__ void __launch_bounds__(1024) k_final_rhsav(const FixPart *part, int n, double area, Scal *s) {
+    i128 tot;
+    int bad;
+    final_fix(part, n, tot, bad);
+    if (threadIdx.x == 0) s->rhsav = (float)(fix_finish(tot, bad) / area);
+}
+
+// One SOR colour sweep, press.f95:153-163 with nrd = colour: cells with
+// (i+j+k+nrd) odd.  Within a colour every update reads only cells of the
+// other colour and ghost cells, so the in-place parallel sweep equals the
+// reference's sequential one.  cn1 is rebuilt from its separable parts.
+__global__ void __launch_bounds__(kRedNT) k_sor_colour(Geo g, float *__restrict__ p, const float *__restrict__ rhs,
+                                                        int nrd, int kchunk, FixPart *part, const Scal *s) {
+    if (s->converged) return;
+    const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
+    const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
+    const int k0 = 1 + blockIdx.z * kchunk;
+    const int k1 = min(g.km, k0 + kchunk - 1);
+    const float rhsav = s->rhsav;
+    i128 acc = 0;
+    int bad = 0;
+    if (i <= g.im && j <= g.jm) {
+        const float cA = g.cnA[i], c2l = g.cn2l[i], c2s = g.cn2s[i];
+        const float cB = g.cnB[j], c3l = g.cn3l[j], c3s = g.cn3s[j];
+        int k = k0 + (((i + j + k0 + nrd) & 1) ? 0 : 1);
+        for (; k <= k1; k += 2) {
+            const int c = IX(g, i, j, k);
+            const float cn1 = 1.0f / (cA + cB + g.cnC[k]);
+            const float pc = p[c];
+            const float reltmp =
+                g.omega * (cn1 * (c2l * p[c + 1] + c2s * p[c - 1] + c3l * p[c + g.si] + c3s * p[c - g.si] +
+                                  g.cn4l[k] * p[c + g.si * g.sj] + g.cn4s[k] * p[c - g.si * g.sj] -
+                                  (rhs[c] - rhsav)) -
+                           pc);
+            p[c] = pc + reltmp;
+            acc += fix_term(reltmp * reltmp, bad);
+        }
+    }
+    block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
+}
+
+// boundp.f95:23-44 (boundp1) as final values: ghost (i,j,k), k in 0..km+1,
+// = p(ci, pj, k) with ci clamping i to 1..im and pj the periodic j map.
+// CHECK=true: part of the SOR loop (skipped once converged).
+template <bool CHECK>
+__global__ void __launch_bounds__(256) k_boundp1(Geo g, float *__restrict__ p, const Scal *s) {
+    if (CHECK && s->converged) return;
+    const int im = g.im, jm = g.jm, km = g.km;
+    const int nI = 2 * (jm + 2) * (km + 2);  // i=0,im+1 ; j=0..jm+1
+    const int nJ = 2 * im * (km + 2);        // j=0,jm+1 ; i=1..im
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (t < nI) {
+        i = (t & 1) ? im + 1 : 0;
+        const int r = t >> 1;
+        j = r % (jm + 2);
+        k = r / (jm + 2);
+    } else if ((t -= nI) < nJ) {
+        j = (t & 1) ? jm + 1 : 0;
+        const int r = t >> 1;
+        i = 1 + r % im;
+        k = r / im;
+    } else {
+        return;
+    }
+    const int ci = i < 1 ? 1 : (i > im ? im : i);
+    const int pj = (j == 0) ? jm : (j == jm + 1 ? 1 : j);
+    p[IX(g, i, j, k)] = p[IX(g, ci, pj, k)];
+}
+
+// boundp.f95:5-21 (boundp2): p(i,j,0)=p(i,j,1), p(i,j,km+1)=p(i,j,km).
+template <bool CHECK>
+__global__ void __launch_bounds__(256) k_boundp2(Geo g, float *__restrict__ p, const Scal *s) {
+    if (CHECK && s->converged) return;
+    const int ni = g.im + 2, nj = g.jm + 2;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * ni * nj) return;
+    const int i = t % ni, r = t / ni;
+    const int j = r % nj;
+    const bool top = (r / nj) != 0;
+    if (top)
+        p[IX(g, i, j, g.km + 1)] = p[IX(g, i, j, g.km)];
+    else
+        p[IX(g, i, j, 0)] = p[IX(g, i, j, 1)];
+}
+
+// press.f95:114: after iteration l, stop when sor < pjuge.
+__global__ void __launch_bounds__(1024) k_final_sor(const FixPart *part, int n, float pjuge, Scal *s) {
+    if (s->converged) return;
+    i128 tot;
+    int bad;
+    final_fix(part, n, tot, bad);
+    if (threadIdx.x == 0) {
+        const float sor = (float)fix_finish(tot, bad);
+        s->sor = sor;
+        s->sor_iters += 1;
+        if (sor < pjuge) s->converged = 1;
+    }
+}
+
+// press.f95:186-195 partial sums of p*dx1*dy1*dzn.
+__global__ void __launch_bounds__(kRedNT) k_pav_reduce(Geo g, const float *__restrict__ p, int kchunk, FixPart *part) {
+    const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
+    const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
+    const int k0 = 1 + blockIdx.z * kchunk;
+    const int k1 = min(g.km, k0 + kchunk - 1);
+    i128 acc = 0;
+    int bad = 0;
+    if (i <= g.im && j <= g.jm) {
+        for (int k = k0; k <= k1; ++k)
+            acc += fix_term(p[IX(g, i, j, k)] * g.dx1[i] * g.dy1[j] * g.dzn[k], bad);
+    }
+    block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
+}
+
+__global__ void __launch_bounds__(1024) k_final_pav(const FixPart *part, int n, double area, Scal *s) {
+    i128 tot;
+    int bad;
+    final_fix(part, n, tot, bad);
+    if (threadIdx.x == 0) s->pav = (float)(fix_finish(tot, bad) / area);
+}
+
+// press.f95:197-209: p -= pav on the interior, then boundp1 and boundp2.
+// The interior thread writes its new value and every ghost whose final
+// source it is: ghost (i,j,k) <- (clamp(i), periodic(j), clamp(k)).
+__global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *__restrict__ p, const Scal *s) {
+    const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
+    const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
+    const int k = 1 + blockIdx.z;
+    if (i > g.im || j > g.jm) return;
+    const float val = p[IX(g, i, j, k)] - s->pav;
+    int is[2], js[2], ks[2];
+    int ni = 0, nj = 0, nk = 0;
+    is[ni++] = i;
+    if (i == 1) is[ni++] = 0;
+    if (i == g.im) is[ni++] = g.im + 1;  // (im >= 2 so at most one extra)
+    js[nj++] = j;
+    if (j == g.jm) js[nj++] = 0;
+    if (j == 1) js[nj++] = g.jm + 1;
+    ks[nk++] = k;
+    if (k == 1) ks[nk++] = 0;
+    if (k == g.km) ks[nk++] = g.km + 1;
+    for (int a = 0; a < ni; ++a)
+        for (int b = 0; b < nj; ++b)
+            for (int c = 0; c < nk; ++c) p[IX(g, is[a], js[b], ks[c])] = val;
+}
+
+// Per-step scalars reset and the centre probe of press.f95:183-187.
+__global__ void k_step_begin(Scal *s, int n) {
+    s->uout_pos = 0u;
+    s->uout_neg = 0u;
+    s->converged = 0;
+    s->sor_iters = 0;
+    s->n = n;
+}
+__global__ void k_probe(Geo g, Fields F, Scal *s) {
+    const int c = IX(g, g.im / 2, g.jm / 2, g.km / 2);
+    s->probe[0] = F.p[c];
+    s->probe[1] = F.u[c];
+    s->probe[2] = F.v[c];
+    s->probe[3] = F.w[c];
+}
+
+}  // namespace
+}  // namespace les

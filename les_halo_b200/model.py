@@ -1,0 +1,163 @@
+"""Host-side mirror of the reference's LES driver for the B200 library.
+
+``LesCase`` holds the model arrays in the reference's Fortran layout (what
+main_ocl.f95 allocates); ``synthetic_case`` builds one from the seeded
+generators of les_synth.h; ``GpuLes`` is the accelerator driver, mirroring
+``initialise_LES_kernel`` / ``run_LES_kernel``
+(src/OpenCL/module_LES_combined_ocl_TEMPL_V2.f95:18-30, 219-231) on top of
+the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+from . import fields as FL
+
+
+@dataclass
+class LesCase:
+    ip: int
+    jp: int
+    kp: int
+    params: abi.LesParams
+    arrays: dict = field(default_factory=dict)
+    built_fraction: float = 0.0
+
+    def a(self, name):
+        return self.arrays[name]
+
+    def copy(self) -> "LesCase":
+        return LesCase(self.ip, self.jp, self.kp, _copy_params(self.params),
+                       {k: v.copy(order="F") for k, v in self.arrays.items()}, self.built_fraction)
+
+    def host_fields(self) -> abi.LesHostFields:
+        hf = abi.LesHostFields()
+        for n in abi.HOST_FIELD_NAMES:
+            arr = self.arrays.get(n)
+            setattr(hf, n, FL.ptr(arr) if arr is not None else None)
+        return hf
+
+
+def _copy_params(p: abi.LesParams) -> abi.LesParams:
+    q = abi.LesParams()
+    C.memmove(C.byref(q), C.byref(p), C.sizeof(p))
+    return q
+
+
+def default_params(ip, jp, kp, dt=0.05, inflow="external", nmaxp=50) -> abi.LesParams:
+    p = abi.LesParams()
+    abi.check(abi.lib().les_params_default(C.byref(p), ip, jp, kp))
+    p.dt = dt
+    p.nmaxp = nmaxp
+    p.inflow_mode = abi.LES_INFLOW_EXTERNAL if inflow == "external" else abi.LES_INFLOW_POWER_LAW
+    return p
+
+
+def synth_cfg(ip, jp, kp, seed=1, **over) -> abi.LesSynthCfg:
+    cfg = abi.LesSynthCfg()
+    abi.lib().les_synth_default(C.byref(cfg), ip, jp, kp, seed)
+    for k, v in over.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def synthetic_case(ip, jp, kp, seed=1, dt=0.05, inflow="external", nmaxp=50,
+                   masks_and_poisson=None, **cfg_over) -> LesCase:
+    """Grid, terrain and inflow from the seeded generators; state zeroed as
+    init.f95:46-69 leaves it.  Masks and Poisson coefficients are filled by
+    `masks_and_poisson(case, zbm)` if given, else on the device with
+    les_building_masks / les_poisson_coeffs."""
+    L = abi.lib()
+    cfg = synth_cfg(ip, jp, kp, seed, **cfg_over)
+    case = LesCase(ip, jp, kp, default_params(ip, jp, kp, dt=dt, inflow=inflow, nmaxp=nmaxp))
+    A = case.arrays
+    for n in FL.METRICS:
+        A[n] = FL.alloc(n, ip, jp, kp)
+    abi.check(L.les_synth_grid(C.byref(cfg), *[FL.ptr(A[n]) for n in
+                                               ("dx1", "dxl", "dy1", "dyl", "z2", "dzn", "dzs",
+                                                "dxs", "dys")]))
+    zbm = FL.alloc("zbm", ip, jp, kp)
+    case.built_fraction = float(L.les_synth_terrain(C.byref(cfg), FL.ptr(zbm)))
+    A["zbm"] = zbm
+    A["wind_profile"] = FL.alloc("wind_profile", ip, jp, kp)
+    abi.check(L.les_synth_inflow(C.byref(cfg), FL.ptr(A["z2"]), FL.ptr(A["dzn"]),
+                                 FL.ptr(A["wind_profile"])))
+    if inflow != "external":
+        del A["wind_profile"]
+    for n in FL.STATE + FL.MASKS + FL.POISSON + ["delx1"]:
+        A[n] = FL.alloc(n, ip, jp, kp)
+    if masks_and_poisson is not None:
+        masks_and_poisson(case, zbm)
+    else:
+        abi.check(L.les_building_masks(ip, jp, kp, FL.ptr(zbm), FL.ptr(A["z2"]), FL.ptr(A["dzn"]),
+                                       *[FL.ptr(A[n]) for n in FL.MASKS]))
+        abi.check(L.les_poisson_coeffs(ip, jp, kp, FL.ptr(A["dxs"]), FL.ptr(A["dys"]),
+                                       FL.ptr(A["dzs"]), *[FL.ptr(A[n]) for n in FL.POISSON]))
+    return case
+
+
+class GpuLes:
+    """Device-resident LES state; the B200 twin of run_LES_kernel."""
+
+    def __init__(self, case: LesCase):
+        self.case = case
+        self.ctx = C.c_void_p()
+        abi.check(abi.lib().les_ctx_create(C.byref(case.params), C.byref(self.ctx)))
+        self._hf = case.host_fields()
+        abi.check(abi.lib().les_ctx_upload(self.ctx, C.byref(self._hf)))
+
+    def close(self):
+        if self.ctx:
+            abi.lib().les_ctx_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def warmup(self, n=1):
+        abi.check(abi.lib().les_ctx_warmup(self.ctx, n))
+
+    def step(self, n0, nsteps=1):
+        abi.check(abi.lib().les_step(self.ctx, n0, nsteps))
+
+    def sync(self):
+        abi.check(abi.lib().les_ctx_sync(self.ctx))
+
+    def set_wind_profile(self, wp: np.ndarray):
+        abi.check(abi.lib().les_set_wind_profile(self.ctx, FL.ptr(wp)))
+
+    def metrics(self) -> dict:
+        m = abi.LesMetrics()
+        abi.check(abi.lib().les_last_metrics(self.ctx, C.byref(m)))
+        return {n: getattr(m, n) for n, _ in m._fields_}
+
+    def download(self, names=None) -> dict:
+        """Fortran-layout copies of the state arrays."""
+        names = names or FL.STATE + FL.MASKS
+        out = {n: FL.alloc(n, self.case.ip, self.case.jp, self.case.kp) for n in names}
+        hf = abi.LesHostFields()
+        for n in names:
+            setattr(hf, n, FL.ptr(out[n]))
+        abi.check(abi.lib().les_ctx_download(self.ctx, C.byref(hf)))
+        return out
+
+    def launches(self) -> int:
+        return int(abi.lib().les_ctx_launch_count(self.ctx))
+
+    def stream(self) -> int:
+        return int(abi.lib().les_ctx_stream(self.ctx) or 0)
+
+    def field(self, name):
+        """(device pointer, ox, si, sj, sk) of a state field's box."""
+        d = C.c_void_p()
+        ox, si, sj, sk = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        abi.check(abi.lib().les_ctx_field(self.ctx, abi.FIELD_IDS.index(name), C.byref(d),
+                                          C.byref(ox), C.byref(si), C.byref(sj), C.byref(sk)))
+        return d.value, ox.value, si.value, sj.value, sk.value

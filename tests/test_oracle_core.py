@@ -1,0 +1,108 @@
+"""The oracle on its own (CPU): reduction definition, grid, quirks, invariants."""
+import ctypes as C
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+import oracle
+from les_halo_b200 import fields as FL
+from les_halo_b200 import synthetic_case
+
+
+def exact_canonical(vals):
+    """Python statement of the canonical sum (les_fix.h): Q63.64 truncation,
+    exact integer sum, two-word conversion to double, scale by 2^-64."""
+    T = 0
+    for x in vals.astype(np.float32).tolist():
+        T += int(Fraction(x) * (1 << 64))  # int() truncates toward zero
+    hi, lo = T >> 64, T & ((1 << 64) - 1)
+    return (float(hi) * 18446744073709551616.0 + float(lo)) / 18446744073709551616.0
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_canonical_sum_matches_exact_statement(seed):
+    rng = np.random.default_rng(seed)
+    im, jm, km = 37, 5, 4
+    x = (rng.standard_normal((im, jm, km)) * 10.0 ** rng.integers(-12, 8, (im, jm, km)))
+    x = np.asfortranarray(x.astype(np.float32))
+    got = oracle.lib().oracle_canonical_sum(im, jm, km, x.ctypes.data)
+    want = exact_canonical(x.ravel(order="F"))
+    assert got == want
+    # order independence: any permutation gives the same bits
+    perm = np.asfortranarray(rng.permutation(x.ravel()).reshape(x.shape, order="F"))
+    assert oracle.lib().oracle_canonical_sum(im, jm, km, perm.ctypes.data) == got
+
+
+def test_reference_grid_values():
+    ip, jp, kp = 150, 150, 90
+    a = {n: FL.alloc(n, ip, jp, kp) for n in FL.METRICS}
+    oracle.lib().oracle_grid_reference(ip, jp, kp, *[FL.ptr(a[n]) for n in
+                                                     ("dx1", "dxl", "dy1", "dyl", "z2", "dzn",
+                                                      "dzs", "dxs", "dys")])
+    dzn = a["dzn"]  # (-1:kp+2)
+    assert dzn[1 + 1] == np.float32(2.5)
+    assert dzn[2 + 1] == np.float32(2.5) * np.float32(1.05)
+    assert dzn[16 + 1] == np.float32(5.0)
+    assert dzn[kp + 1 + 1] == dzn[kp + 1]      # dzn(kp+1) = dzn(kp)
+    assert a["z2"][0] == np.float32(2.5)       # z2(1)
+    assert np.all(a["dx1"] == 20.0) and np.all(a["dy1"] == 20.0)
+    assert a["dxl"][ip] == 20.0 * ip
+
+
+@pytest.fixture(scope="module")
+def stepped_case():
+    case = synthetic_case(24, 20, 16, seed=5, masks_and_poisson=oracle.masks_and_poisson)
+    oracle.ifdata(case, 1)
+    iters = oracle.run_steps(case, 1, 3)
+    return case, iters
+
+
+def test_step_is_finite_and_sor_capped(stepped_case):
+    case, iters = stepped_case
+    for n in FL.STATE:
+        assert np.isfinite(case.a(n)).all(), n
+    assert all(1 <= it <= case.params.nmaxp for it in iters)
+
+
+def test_boundary_invariants_after_step(stepped_case):
+    case, _ = stepped_case
+    ip, jp, kp = case.ip, case.jp, case.kp
+    P = lambda i, j, k: case.a("p")[FL.index("p", ip, jp, kp, i, j, k)]
+    # boundp1/boundp2 final state (press.f95:207-209)
+    for k in (0, 1, kp // 2, kp, kp + 1):
+        for j in range(0, jp + 2):
+            assert P(0, j, k) == P(1, j, k) and P(ip + 1, j, k) == P(ip, j, k)
+        for i in range(0, ip + 2):
+            assert P(i, 0, k) == P(i, jp, k) and P(i, jp + 1, k) == P(i, 1, k)
+    U = lambda n, i, j, k: case.a(n)[FL.index(n, ip, jp, kp, i, j, k)]
+    # bondv1 periodic rows and the w(-1,...) aliasing write (bondv1.f95:132-137)
+    assert U("u", 3, 0, 4) == U("u", 3, jp, 4) and U("u", 3, jp + 1, 4) == U("u", 3, 1, 4)
+    assert U("w", ip + 1, jp + 1, kp - 1) == 0.0
+    assert U("w", ip + 1, jp + 1, kp - 2) == U("w", ip + 1, 1, kp - 2)
+    # boundsm (boundsm.f95:13-32): ground plane is the negated first level
+    S = lambda i, j, k: case.a("sm")[FL.index("sm", ip, jp, kp, i, j, k)]
+    assert S(5, 4, 0) == -S(5, 4, 1) and S(0, 4, 3) == S(1, 4, 3) and S(5, 0, 3) == S(5, 1, 3)
+
+
+def test_faithful_and_canonical_reductions_agree_closely():
+    res = {}
+    for mode in (oracle.RED_CANONICAL, oracle.RED_FAITHFUL):
+        oracle.set_reduction_mode(mode)
+        try:
+            case = synthetic_case(24, 20, 16, seed=7, masks_and_poisson=oracle.masks_and_poisson)
+            oracle.ifdata(case, 1)
+            oracle.run_steps(case, 1, 2)
+            res[mode] = case
+        finally:
+            oracle.set_reduction_mode(oracle.RED_CANONICAL)
+    a, b = res[oracle.RED_CANONICAL], res[oracle.RED_FAITHFUL]
+    for n in ("u", "v", "w", "p"):
+        x, y = a.a(n).astype(np.float64), b.a(n).astype(np.float64)
+        assert np.linalg.norm(x - y) <= 1e-3 * np.linalg.norm(y) + 1e-12, n
+
+
+def test_ibm_gains_bound_dt():
+    # set.f95:84: (-beta - sqrt(beta^2 - 2 alpha))/alpha must not be < dt
+    a, b = -10.0, -1.0
+    assert (-b - np.sqrt(b * b - 2 * a)) / a > 0.2
