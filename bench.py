@@ -32,7 +32,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "time-step Mpts/s: plain vs FP64-refined press at ≤1e-5 err; adjoint/fwd cost"
 WORKLOAD = dict(ip=600, jp=600, kp=120, plan_area=0.35, h_max=120.0, dt=0.05, nmaxp=50, seed=1)
-SOR_BYTES_PER_CELL_PER_COLOUR = 6.0   # 12 B/cell per SOR iteration (p read, rhs read, p write) over 2 colour sweeps
+SOR_BYTES_PER_CELL_PER_ITER = 12.0   # p read, rhs read, p write per SOR iteration (SURVEY 8d accounting)
 STEP_BYTES_PER_CELL = 204.0 + 12.0 * 50  # algorithmic bytes per cell per step at 50 SOR iterations
 
 
@@ -204,12 +204,15 @@ def run_ours(args):
     gpu.sync()
     L = abi.lib()
     # capture the timed step graph (with its event nodes) before timing, then
-    # reset the slots so the K timed steps use slots 0..K-1
-    abi.check(L.les_ctx_set_timing(gpu.ctx, args.steps))
+    # reset the slots so the K timed steps use slots 0..K-1.  Profiling runs
+    # (--profile) leave the graph without event nodes.
+    if not args.profile:
+        abi.check(L.les_ctx_set_timing(gpu.ctx, args.steps))
     gpu.step(n, 1)
     n += 1
     gpu.sync()
-    abi.check(L.les_ctx_set_timing(gpu.ctx, args.steps))
+    if not args.profile:
+        abi.check(L.les_ctx_set_timing(gpu.ctx, args.steps))
 
     stream = torch.cuda.ExternalStream(gpu.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -232,7 +235,7 @@ def run_ours(args):
     launches = gpu.launches() - launches0
     phases = np.zeros((args.steps, 9), np.float32)
     buf = (C.c_float * 9)()
-    for s in range(args.steps):
+    for s in range(args.steps if not args.profile else 0):
         abi.check(L.les_ctx_phase_times(gpu.ctx, s, buf, 9))
         phases[s] = np.frombuffer(buf, np.float32)
     m = gpu.metrics()
@@ -272,9 +275,12 @@ def run_ours(args):
     value = ws * cells * args.steps / (ms_total / 1e3) / 1e6
     e2e_val = ws * cells * e2e_steps / e2e_s / 1e6
 
-    sor_launch_ms = float(np.mean(phases[:, 5]))
+    sor_launch_ms = float(np.mean(phases[:, 5])) if not args.profile else float("nan")
     peak, peak_kind = _peaks()
-    achieved = SOR_BYTES_PER_CELL_PER_COLOUR * cells / (sor_launch_ms / 1e3) / 1e9
+    ipl = float(L.les_ctx_sor_iters_per_launch(gpu.ctx))
+    tT, tY = C.c_int(), C.c_int()
+    abi.check(L.les_ctx_sor_tile(gpu.ctx, C.byref(tT), C.byref(tY)))
+    achieved = SOR_BYTES_PER_CELL_PER_ITER * ipl * cells / (sor_launch_ms / 1e3) / 1e9
     step_gbs = STEP_BYTES_PER_CELL * cells / (ms_step / 1e3) / 1e9
     traffic = None
     tf = ROOT / "profiles" / "sor_traffic.json"
@@ -289,17 +295,19 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded terrain + log-law inflow)",
-            "config": {"workload": "LES plain FP32 step 600x600x120 (35% plan area, heights <=120 m, "
-                                   "dt=0.05, SOR 50 sweeps/step)",
+            "config": {"workload": f"LES plain FP32 step {case.ip}x{case.jp}x{case.kp} (35% plan area, "
+                                   "heights <=120 m, dt=0.05, SOR 50 sweeps/step)",
                        "grid": [case.ip, case.jp, case.kp], "sor_iters": int(m["sor_iters"]),
                        "parallelism": f"replicas x{ws}",
+                       "sor_tile": {"iters_per_pass": tT.value, "rows": tY.value, "cols": 64 - 4 * tT.value},
                        "l2": "inputs larger than L2 (19 state fields, 3.5 GB)"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_sor_colour",
+            "roofline": {"bound": "hbm", "kernel": "k_sor_tb" if ipl > 1 else "k_sor_colour",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": peak_kind,
-                         "algorithmic": f"{SOR_BYTES_PER_CELL_PER_COLOUR} B/cell x {cells} cells per launch"},
+                         "algorithmic": f"{SOR_BYTES_PER_CELL_PER_ITER} B/cell/iteration x {ipl} iterations "
+                                        f"per launch x {cells} cells"},
             "step_roofline": {"achieved_gbs": round(step_gbs, 1), "frac": round(step_gbs / peak, 4),
                               "bytes_per_cell": STEP_BYTES_PER_CELL},
             "phases_ms": {k: round(float(v), 4) for k, v in zip(
@@ -327,7 +335,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="no in-graph timing events (for runs under ncu)")
+    ap.add_argument("--grid", default=None,
+                    help="IP,JP,KP: run a smaller grid (profiling captures); the line names it")
     args = ap.parse_args()
+    if args.grid:
+        ip, jp, kp = (int(x) for x in args.grid.split(","))
+        WORKLOAD.update(ip=ip, jp=jp, kp=kp)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -137,6 +137,18 @@ uint64_t les_ctx_launch_count(les_ctx *ctx);
  * + visc + adam, [3] rhs + rhsav, [4] gap, [5] the first SOR colour sweep
  * (one launch), [6] the rest of the SOR loop, [7] pav, [8] the whole step. */
 les_status les_ctx_set_timing(les_ctx *ctx, int nslots);
+/* Diagnostic: exact != 0 makes every following step run the SOR one colour
+ * sweep at a time with materialised ghosts (boundp1 per colour, boundp2 per
+ * iteration, press.f95:87-115) instead of the multi-iteration passes.  Both
+ * give identical results; odd jp and a just-uploaded p whose ghosts are not
+ * boundary-consistent always use the per-colour sweeps. */
+les_status les_ctx_set_sor_path(les_ctx *ctx, int exact);
+/* SOR iterations one SOR kernel launch of the next step carries: 0.5 for a
+ * colour sweep, 2 for a multi-iteration pass. */
+float les_ctx_sor_iters_per_launch(les_ctx *ctx);
+/* Iterations per pass and tile rows the autotuner chose for the
+ * multi-iteration SOR (0, 0 before the first step that uses it). */
+les_status les_ctx_sor_tile(les_ctx *ctx, int *iters_per_pass, int *tile_rows);
 les_status les_ctx_phase_times(les_ctx *ctx, int slot, float *ms, int n);
 
 /* Device state access for callers that keep fields on the GPU.  The field
@@ -264,6 +276,7 @@ les_status les_bondfg_(const int *km, const int *jm, float *f, const int *im, fl
 les_status les_boundp1_(const int *km, const int *jm, float *p, const int *im);
 /* boundp.f95:18 */
 les_status les_boundp2_(const int *jm, const int *im, float *p, const int *km);
+
 
 #ifdef __cplusplus
 }

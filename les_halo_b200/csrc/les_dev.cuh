@@ -25,8 +25,16 @@ struct Geo {
     const float *cnA, *cnB, *cnC;  // cn1 = 1/((cnA(i)+cnB(j))+cnC(k)), init.f95:87-93
     const float *smc;              // (cs0*delx1(k))**2, les.f95:128,148
     const float *wind;             // inflow u(0:1,j,k): wind[(j-1) + jm*(k-1)]
+    // Exact reciprocals of the x/y divisors that are powers of two, else 0:
+    // rdx1(i)=1/dx1(i), rsx(i)=1/(dx1(i)+dx1(i+1)), rdy1, rsy alike.  For a
+    // power-of-two divisor d, a*(1/d) and a/d are the correctly rounded
+    // value of the same real number, so they are bit-identical.
+    const float *rdx1, *rsx, *rdy1, *rsy;
     float dt, ro, vn, alpha, beta, omega;
 };
+
+// a/d with d's exact reciprocal r when d is a power of two (r != 0).
+__device__ __forceinline__ float fdiv(float a, float d, float r) { return r != 0.0f ? a * r : a / d; }
 
 struct Fields {
     float *u, *v, *w, *p, *usum, *vsum, *wsum, *f, *g, *h, *fold, *gold, *hold, *rhs, *sm;
@@ -39,6 +47,8 @@ struct Scal {
     unsigned int uout_neg;  // max of -u(im,j,k) for negative u, float bits
     float uout, rhsav, pav, sor;
     int sor_iters, converged, n, pad;
+    int pbuf;  // SOR result buffer: 0 = p, 1 = the second p buffer
+    int redo;  // iterations to redo after a pass that converged part-way
     float probe[4];
 };
 
@@ -53,69 +63,91 @@ __device__ __forceinline__ int IX(const Geo &g, int i, int j, int k) {
 // boundary copies of vel2.f95:125-188, and 0 (from zero_arrays,
 // ifdata.f95:15-127) everywhere nothing ever writes.
 // ---------------------------------------------------------------------------
+// u, v, w read straight from the state boxes.
 struct UVW {
     const float *__restrict__ u;
     const float *__restrict__ v;
     const float *__restrict__ w;
+    __device__ __forceinline__ float U(const Geo &g, int i, int j, int k) const { return __ldg(&u[IX(g, i, j, k)]); }
+    __device__ __forceinline__ float V(const Geo &g, int i, int j, int k) const { return __ldg(&v[IX(g, i, j, k)]); }
+    __device__ __forceinline__ float W(const Geo &g, int i, int j, int k) const { return __ldg(&w[IX(g, i, j, k)]); }
 };
 
-#define LU(i, j, k) __ldg(&q.u[IX(g, (i), (j), (k))])
-#define LV(i, j, k) __ldg(&q.v[IX(g, (i), (j), (k))])
-#define LW(i, j, k) __ldg(&q.w[IX(g, (i), (j), (k))])
+#define LU(i, j, k) q.U(g, (i), (j), (k))
+#define LV(i, j, k) q.V(g, (i), (j), (k))
+#define LW(i, j, k) q.W(g, (i), (j), (k))
 
-__device__ __forceinline__ float nou1_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float nou1_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (LU(i - 1, j, k) + LU(i, j, k)) / 2.0f;
 }
-__device__ __forceinline__ float diu1_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return (-LU(i - 1, j, k) + LU(i, j, k)) / g.dx1[i];
+template <class Q>
+__device__ __forceinline__ float diu1_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(-LU(i - 1, j, k) + LU(i, j, k), g.dx1[i], g.rdx1[i]);
 }
-__device__ __forceinline__ float nou5_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float nou5_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (LV(i, j - 1, k) + LV(i, j, k)) / 2.0f;
 }
-__device__ __forceinline__ float diu5_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return (-LV(i, j - 1, k) + LV(i, j, k)) / g.dy1[j];
+template <class Q>
+__device__ __forceinline__ float diu5_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(-LV(i, j - 1, k) + LV(i, j, k), g.dy1[j], g.rdy1[j]);
 }
-__device__ __forceinline__ float nou9_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float nou9_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (LW(i, j, k - 1) + LW(i, j, k)) / 2.0f;
 }
-__device__ __forceinline__ float diu9_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu9_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (-LW(i, j, k - 1) + LW(i, j, k)) / g.dzn[k];
 }
-__device__ __forceinline__ float nou2_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return (g.dx1[i + 1] * LV(i, j - 1, k) + g.dx1[i] * LV(i + 1, j - 1, k)) / (g.dx1[i] + g.dx1[i + 1]);
+template <class Q>
+__device__ __forceinline__ float nou2_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(g.dx1[i + 1] * LV(i, j - 1, k) + g.dx1[i] * LV(i + 1, j - 1, k), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
 }
-__device__ __forceinline__ float diu2_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return 2.0f * (-LU(i, j - 1, k) + LU(i, j, k)) / (g.dy1[j - 1] + g.dy1[j]);
+template <class Q>
+__device__ __forceinline__ float diu2_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(2.0f * (-LU(i, j - 1, k) + LU(i, j, k)), g.dy1[j - 1] + g.dy1[j], g.rsy[j - 1]);
 }
-__device__ __forceinline__ float nou3_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return (g.dx1[i + 1] * LW(i, j, k - 1) + g.dx1[i] * LW(i + 1, j, k - 1)) / (g.dx1[i] + g.dx1[i + 1]);
+template <class Q>
+__device__ __forceinline__ float nou3_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(g.dx1[i + 1] * LW(i, j, k - 1) + g.dx1[i] * LW(i + 1, j, k - 1), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
 }
-__device__ __forceinline__ float diu3_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu3_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (-LU(i, j, k - 1) + LU(i, j, k)) / g.dzs[k - 1];
 }
-__device__ __forceinline__ float nou4_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return (g.dy1[j + 1] * LU(i - 1, j, k) + g.dy1[j] * LU(i - 1, j + 1, k)) / (g.dy1[j] + g.dy1[j + 1]);
+template <class Q>
+__device__ __forceinline__ float nou4_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(g.dy1[j + 1] * LU(i - 1, j, k) + g.dy1[j] * LU(i - 1, j + 1, k), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
 }
-__device__ __forceinline__ float diu4_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return 2.0f * (-LV(i - 1, j, k) + LV(i, j, k)) / (g.dx1[i - 1] + g.dx1[i]);
+template <class Q>
+__device__ __forceinline__ float diu4_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(2.0f * (-LV(i - 1, j, k) + LV(i, j, k)), g.dx1[i - 1] + g.dx1[i], g.rsx[i - 1]);
 }
-__device__ __forceinline__ float nou6_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return (g.dy1[j + 1] * LW(i, j, k - 1) + g.dy1[j] * LW(i, j + 1, k - 1)) / (g.dy1[j] + g.dy1[j + 1]);
+template <class Q>
+__device__ __forceinline__ float nou6_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(g.dy1[j + 1] * LW(i, j, k - 1) + g.dy1[j] * LW(i, j + 1, k - 1), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
 }
-__device__ __forceinline__ float diu6_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu6_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (-LV(i, j, k - 1) + LV(i, j, k)) / g.dzs[k - 1];
 }
-__device__ __forceinline__ float nou7_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float nou7_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (g.dzn[k + 1] * LU(i - 1, j, k) + g.dzn[k] * LU(i - 1, j, k + 1)) / (g.dzn[k] + g.dzn[k + 1]);
 }
-__device__ __forceinline__ float diu7_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return 2.0f * (-LW(i - 1, j, k) + LW(i, j, k)) / (g.dx1[i - 1] + g.dx1[i]);
+template <class Q>
+__device__ __forceinline__ float diu7_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(2.0f * (-LW(i - 1, j, k) + LW(i, j, k)), g.dx1[i - 1] + g.dx1[i], g.rsx[i - 1]);
 }
-__device__ __forceinline__ float nou8_raw(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float nou8_raw(const Geo &g, const Q &q, int i, int j, int k) {
     return (g.dzn[k + 1] * LV(i, j - 1, k) + g.dzn[k] * LV(i, j - 1, k + 1)) / (g.dzn[k] + g.dzn[k + 1]);
 }
-__device__ __forceinline__ float diu8_raw(const Geo &g, const UVW &q, int i, int j, int k) {
-    return 2.0f * (-LW(i, j - 1, k) + LW(i, j, k)) / (g.dy1[j - 1] + g.dy1[j]);
+template <class Q>
+__device__ __forceinline__ float diu8_raw(const Geo &g, const Q &q, int i, int j, int k) {
+    return fdiv(2.0f * (-LW(i, j - 1, k) + LW(i, j, k)), g.dy1[j - 1] + g.dy1[j], g.rsy[j - 1]);
 }
 
 // j index of the periodic copies X(i,0,k)=X(i,jm,k), X(i,jm+1,k)=X(i,1,k);
@@ -125,42 +157,50 @@ __device__ __forceinline__ int jper(const Geo &g, int j) {
 }
 
 // group 1 (vel2.f95:48-63, copy :125-131): range 1..im x 1..jm x 1..km, i=im+1 <- im
-__device__ __forceinline__ float diu1_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu1_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (j < 1 || j > g.jm || k < 1 || k > g.km || i < 1 || i > g.im + 1) return 0.0f;
     return diu1_raw(g, q, i > g.im ? g.im : i, j, k);
 }
-__device__ __forceinline__ float cov1_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov1_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (j < 1 || j > g.jm || k < 1 || k > g.km || i < 1 || i > g.im + 1) return 0.0f;
     const int ii = i > g.im ? g.im : i;
     return nou1_raw(g, q, ii, j, k) * diu1_raw(g, q, ii, j, k);
 }
 // group 5 (copies :149-158): j periodic on 1..im x * x 1..km
-__device__ __forceinline__ float diu5_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu5_e(const Geo &g, const Q &q, int i, int j, int k) {
     const int jj = jper(g, j);
     if (i < 1 || i > g.im || k < 1 || k > g.km || jj == 0) return 0.0f;
     return diu5_raw(g, q, i, jj, k);
 }
-__device__ __forceinline__ float cov5_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov5_e(const Geo &g, const Q &q, int i, int j, int k) {
     const int jj = jper(g, j);
     if (i < 1 || i > g.im || k < 1 || k > g.km || jj == 0) return 0.0f;
     return nou5_raw(g, q, i, jj, k) * diu5_raw(g, q, i, jj, k);
 }
 // group 9: 1..im x 1..jm x 1..km, no copies
-__device__ __forceinline__ float diu9_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu9_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (i < 1 || i > g.im || j < 1 || j > g.jm || k < 1 || k > g.km) return 0.0f;
     return diu9_raw(g, q, i, j, k);
 }
-__device__ __forceinline__ float cov9_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov9_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (i < 1 || i > g.im || j < 1 || j > g.jm || k < 1 || k > g.km) return 0.0f;
     return nou9_raw(g, q, i, j, k) * diu9_raw(g, q, i, j, k);
 }
 // group 2 (:65-73, copies :132-141), diu2 also (im+1,1..jm+1,1..km+1) <- im (:177-182)
-__device__ __forceinline__ float cov2_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov2_e(const Geo &g, const Q &q, int i, int j, int k) {
     const int jj = jper(g, j);
     if (i < 1 || i > g.im || k < 1 || k > g.km || jj == 0) return 0.0f;
     return nou2_raw(g, q, i, jj, k) * diu2_raw(g, q, i, jj, k);
 }
-__device__ __forceinline__ float diu2_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu2_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (i == g.im + 1) {
         if (j < 1 || j > g.jm + 1 || k < 1 || k > g.km + 1) return 0.0f;
         i = g.im;
@@ -170,11 +210,13 @@ __device__ __forceinline__ float diu2_e(const Geo &g, const UVW &q, int i, int j
     return diu2_raw(g, q, i, jj, k);
 }
 // group 3 (:75-83): 1..im x 1..jm x 1..km+1; diu3 (im+1,1..jm+1,1..km+1) <- im
-__device__ __forceinline__ float cov3_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov3_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (i < 1 || i > g.im || j < 1 || j > g.jm || k < 1 || k > g.km + 1) return 0.0f;
     return nou3_raw(g, q, i, j, k) * diu3_raw(g, q, i, j, k);
 }
-__device__ __forceinline__ float diu3_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu3_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (i == g.im + 1) {
         if (j < 1 || j > g.jm + 1 || k < 1 || k > g.km + 1) return 0.0f;
         i = g.im;  // diu3(im, jm+1, k) is never computed: stays 0 below
@@ -183,43 +225,51 @@ __device__ __forceinline__ float diu3_e(const Geo &g, const UVW &q, int i, int j
     return diu3_raw(g, q, i, j, k);
 }
 // group 4 (:85-93, copy :142-148): 1..jm x 1..km, i=im+1 <- im; diu4(1..im+1,0,1..km+1) <- jm (:183-188)
-__device__ __forceinline__ float cov4_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov4_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (j < 1 || j > g.jm || k < 1 || k > g.km || i < 1 || i > g.im + 1) return 0.0f;
     const int ii = i > g.im ? g.im : i;
     return (nou4_raw(g, q, ii, j, k) - 0.0f) * diu4_raw(g, q, ii, j, k);
 }
-__device__ __forceinline__ float diu4_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu4_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (j == 0 && i >= 1 && i <= g.im + 1 && k >= 1 && k <= g.km + 1) j = g.jm;
     if (j < 1 || j > g.jm || k < 1 || k > g.km || i < 1 || i > g.im + 1) return 0.0f;
     return diu4_raw(g, q, i > g.im ? g.im : i, j, k);
 }
 // group 6 (:95-103): 1..im x 1..jm x 1..km+1; diu6(1..im+1,0,1..km+1) <- jm
-__device__ __forceinline__ float cov6_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov6_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (i < 1 || i > g.im || j < 1 || j > g.jm || k < 1 || k > g.km + 1) return 0.0f;
     return nou6_raw(g, q, i, j, k) * diu6_raw(g, q, i, j, k);
 }
-__device__ __forceinline__ float diu6_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu6_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (j == 0 && i >= 1 && i <= g.im + 1 && k >= 1 && k <= g.km + 1) j = g.jm;
     if (i < 1 || i > g.im || j < 1 || j > g.jm || k < 1 || k > g.km + 1) return 0.0f;
     return diu6_raw(g, q, i, j, k);
 }
 // group 7 (:105-113, copy :159-165): 1..jm x 1..km-1, i=im+1 <- im
-__device__ __forceinline__ float cov7_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov7_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (j < 1 || j > g.jm || k < 1 || k > g.km - 1 || i < 1 || i > g.im + 1) return 0.0f;
     const int ii = i > g.im ? g.im : i;
     return (nou7_raw(g, q, ii, j, k) - 0.0f) * diu7_raw(g, q, ii, j, k);
 }
-__device__ __forceinline__ float diu7_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu7_e(const Geo &g, const Q &q, int i, int j, int k) {
     if (j < 1 || j > g.jm || k < 1 || k > g.km - 1 || i < 1 || i > g.im + 1) return 0.0f;
     return diu7_raw(g, q, i > g.im ? g.im : i, j, k);
 }
 // group 8 (:115-123, copies :166-175): 1..im x 1..km-1, j periodic
-__device__ __forceinline__ float cov8_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float cov8_e(const Geo &g, const Q &q, int i, int j, int k) {
     const int jj = jper(g, j);
     if (i < 1 || i > g.im || k < 1 || k > g.km - 1 || jj == 0) return 0.0f;
     return nou8_raw(g, q, i, jj, k) * diu8_raw(g, q, i, jj, k);
 }
-__device__ __forceinline__ float diu8_e(const Geo &g, const UVW &q, int i, int j, int k) {
+template <class Q>
+__device__ __forceinline__ float diu8_e(const Geo &g, const Q &q, int i, int j, int k) {
     const int jj = jper(g, j);
     if (i < 1 || i > g.im || k < 1 || k > g.km - 1 || jj == 0) return 0.0f;
     return diu8_raw(g, q, i, jj, k);

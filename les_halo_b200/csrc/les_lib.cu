@@ -4,6 +4,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -12,7 +16,10 @@
 
 #include "les_abi.h"
 #include "les_halo.cuh"
+#include "les_mom.cuh"
 #include "les_press.cuh"
+#include "les_routines.cuh"
+#include "les_sor_tb.cuh"
 #include "les_step.cuh"
 
 using namespace les;
@@ -90,7 +97,8 @@ FBounds field_bounds(int f, int ip, int jp, int kp) {
 
 // Offsets of the 1-D tables inside one device buffer (each with slack).
 struct TableLayout {
-    size_t dx1, dy1, dzn, dzs, dxs, dys, cn2l, cn2s, cn3l, cn3s, cn4l, cn4s, cnA, cnB, cnC, smc, wind, total;
+    size_t dx1, dy1, dzn, dzs, dxs, dys, cn2l, cn2s, cn3l, cn3s, cn4l, cn4s, cnA, cnB, cnC, smc, wind;
+    size_t rdx1, rsx, rdy1, rsy, cn1k, total;
 };
 TableLayout table_layout(int ip, int jp, int kp) {
     TableLayout t;
@@ -117,6 +125,11 @@ TableLayout table_layout(int ip, int jp, int kp) {
     t.cnC = take(kp + 2);
     t.smc = take(kp + 2);
     t.wind = take((size_t)jp * kp);
+    t.rdx1 = take(ip + 4);
+    t.rsx = take(ip + 4);
+    t.rdy1 = take(jp + 4);
+    t.rsy = take(jp + 4);
+    t.cn1k = take(kp + 2);
     t.total = o;
     return t;
 }
@@ -138,15 +151,16 @@ struct les_ctx {
     float *d_stage = nullptr;
     size_t stage_elems = 0;
     cudaStream_t stream = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    cudaGraph_t graph_src[2] = {nullptr, nullptr};
-    uint64_t graph_kernels[2] = {0, 0};
+    // step graphs: index = (n==1 broadcast) + 2 * (exact per-colour SOR)
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaGraph_t graph_src[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t graph_kernels[4] = {0, 0, 0, 0};
     // per-step phase timing (les_ctx_set_timing): event record nodes in the
     // step graphs are pointed at slot `tslot` before each launch
     int tslots = 0, tslot = 0;
     std::vector<cudaEvent_t> tev;  // tslots x LES_NTEV
-    std::vector<cudaGraphNode_t> tnode[2];
-    std::vector<int> tnode_idx[2];
+    std::vector<cudaGraphNode_t> tnode[4];
+    std::vector<int> tnode_idx[4];
     bool capturing_timed = false;
     double area = 0.0;
     uint64_t launches = 0;
@@ -154,14 +168,25 @@ struct les_ctx {
     bool rhs_raw = false;  // interior of rhs holds values before the rhsav subtraction
     int red_gx = 0, red_gy = 0, red_nk = 0, red_kchunk = 0;
     int last_n = 0;
+    std::vector<float *> extra;      // scratch boxes of the per-routine entries
+    const float *cn1_box = nullptr;  // caller's cn1 (per-routine press only)
+    // temporal-blocked SOR (les_sor_tb.cuh)
+    float *d_p2 = nullptr;           // second p buffer
+    int tb_T = 0, tb_ty = 0, tb_gx = 0, tb_gy = 0;  // tile chosen by the autotuner
+    size_t tb_smem = 0;
+    bool cn1_by_k = false;           // uniform dx, dy: cn1 from a per-k table
+    bool p_ghosts_ok = false;        // p's ghosts hold what boundp1/boundp2 give
+    bool force_exact_sor = false;    // testing: always the per-colour path
 };
 
 namespace {
 
 float *field_ptr(les_ctx *c, int f) { return c->d_fields + (size_t)f * c->box_elems; }
+les_status launch_sor_tb(les_ctx *c, int T, int ty, bool cn1k, int niter, int mode);
 
 // Host copies of the 1-D tables -> device; builds cnA/B/C, smc, wind.
-les_status build_tables(les_ctx *c, const les_host_fields *hf) {
+// Tables not given stay zero (the per-routine entries pass only theirs).
+les_status build_tables(les_ctx *c, const les_host_fields *hf, bool require_inflow) {
     const int ip = c->prm.ip, jp = c->prm.jp, kp = c->prm.kp;
     const TableLayout &t = c->tl;
     std::vector<float> &h = c->h_tables;
@@ -199,9 +224,9 @@ les_status build_tables(les_ctx *c, const les_host_fields *hf) {
     }
     // inflow table: bondv1.f95:26-45 power law or the external profile
     if (c->prm.inflow_mode == LES_INFLOW_EXTERNAL) {
-        if (!hf->wind_profile) return fail(LES_ERR_BAD_ARG, "external inflow needs wind_profile");
-        std::memcpy(&h[t.wind], hf->wind_profile, sizeof(float) * (size_t)jp * kp);
-    } else {
+        if (!hf->wind_profile && require_inflow) return fail(LES_ERR_BAD_ARG, "external inflow needs wind_profile");
+        if (hf->wind_profile) std::memcpy(&h[t.wind], hf->wind_profile, sizeof(float) * (size_t)jp * kp);
+    } else if (hf->z2 || require_inflow) {
         if (!hf->z2) return fail(LES_ERR_BAD_ARG, "power-law inflow needs z2");
         std::vector<float> col(kp + 1);
         for (int k = 1; k <= kp; ++k) {
@@ -214,6 +239,26 @@ les_status build_tables(les_ctx *c, const les_host_fields *hf) {
         for (int k = 1; k <= kp; ++k)
             for (int j = 1; j <= jp; ++j) h[t.wind + (j - 1) + (size_t)jp * (k - 1)] = col[k];
     }
+    // cn1 depends on k only when cnA and cnB are constant (uniform dx, dy):
+    // cn1k(k) = 1/((cnA+cnB)+cnC(k)) is then bit-identical to init.f95:87-93
+    {
+        bool uni = true;
+        for (int i = 2; i <= ip && uni; ++i) uni = std::memcmp(&h[t.cnA], &h[t.cnA + i - 1], 4) == 0;
+        for (int j = 2; j <= jp && uni; ++j) uni = std::memcmp(&h[t.cnB], &h[t.cnB + j - 1], 4) == 0;
+        c->cn1_by_k = uni && hf->dxs && hf->dys && hf->dzs;
+        for (int k = 1; k <= kp; ++k) h[t.cn1k + k] = 1.0f / (h[t.cnA] + h[t.cnB] + h[t.cnC + k - 1]);
+    }
+    // exact reciprocals of power-of-two x/y divisors (0 otherwise)
+    auto recip = [](float d) -> float {
+        int e = 0;
+        const float m = std::frexp(d, &e);
+        if (!(d > 0.0f) || m != 0.5f || e < -120 || e > 120) return 0.0f;
+        return std::ldexp(1.0f, 1 - e);  // d = 2^(e-1)
+    };
+    for (int i = -1; i <= ip + 1; ++i) h[t.rdx1 + i + 1] = recip(dx1(i));
+    for (int i = -1; i <= ip; ++i) h[t.rsx + i + 1] = recip(dx1(i) + dx1(i + 1));
+    for (int j = 0; j <= jp + 1; ++j) h[t.rdy1 + j] = recip(dy1(j));
+    for (int j = 0; j <= jp; ++j) h[t.rsy + j] = recip(dy1(j) + dy1(j + 1));
     // grid-only denominator of rhsav and pav (press.f95:134, 192)
     i128 acc = 0;
     int bad = 0;
@@ -246,6 +291,12 @@ les_status mark(les_ctx *c, int which) {
         CKL();                                                     \
         ++(c)->launches;                                           \
     } while (0)
+#define LAUNCH_SMEM(c, kern, grid, block, smem, ...)                  \
+    do {                                                              \
+        kern<<<(grid), (block), (smem), (c)->stream>>>(__VA_ARGS__);  \
+        CKL();                                                        \
+        ++(c)->launches;                                              \
+    } while (0)
 
 dim3 cells_grid(const Geo &g, int i0) {  // i from i0, 32 x 4 blocks, z = k
     return dim3(cdiv(g.im - i0 + 1, 32), cdiv(g.jm, 4), g.km);
@@ -266,14 +317,24 @@ les_status enqueue_bondv1(les_ctx *c, int n, bool velnw) {
 
 les_status enqueue_velfg_les(les_ctx *c, bool adam) {
     const Geo &g = c->geo;
-    LAUNCH(c, k_velfg_feedbf_sm, cells_grid(g, 1), dim3(32, 4), g, c->F);
+    const dim3 mg(cdiv(g.im, kMX), cdiv(g.jm, kMY));
+    const bool band = g.jm >= kBH;  // the staged band must not wrap onto itself
+    if (band)
+        LAUNCH_SMEM(c, k_mom1<true>, mg, dim3(kMNT), mom_smem(false), g, c->F);
+    else
+        LAUNCH_SMEM(c, k_mom1<false>, mg, dim3(kMNT), mom_smem(false), g, c->F);
     MARK(c, EV_VELFG);
     const long long nb = 2LL * (g.jm + 3) * (g.km + 2) + 2LL * g.im * (g.km + 2) + 2LL * g.im * (g.jm + 1);
     LAUNCH(c, k_boundsm, dim3(cdiv(nb, 256)), dim3(256), g, c->F.sm);
-    if (adam)
-        LAUNCH(c, k_visc<true>, cells_grid(g, 1), dim3(32, 4), g, c->F);
+    const size_t sm2 = mom_smem(true);
+    if (adam && band)
+        LAUNCH_SMEM(c, (k_mom2<true, true>), mg, dim3(kMNT), sm2, g, c->F);
+    else if (adam)
+        LAUNCH_SMEM(c, (k_mom2<true, false>), mg, dim3(kMNT), sm2, g, c->F);
+    else if (band)
+        LAUNCH_SMEM(c, (k_mom2<false, true>), mg, dim3(kMNT), sm2, g, c->F);
     else
-        LAUNCH(c, k_visc<false>, cells_grid(g, 1), dim3(32, 4), g, c->F);
+        LAUNCH_SMEM(c, (k_mom2<false, false>), mg, dim3(kMNT), sm2, g, c->F);
     MARK(c, EV_VISC);
     return LES_OK;
 }
@@ -291,7 +352,10 @@ les_status enqueue_boundp(les_ctx *c, bool check) {
     return LES_OK;
 }
 
-les_status enqueue_press(les_ctx *c) {
+// press.f95:49-146.  exact=true: per-colour sweeps with materialised
+// boundp1/boundp2 ghosts (any jm, any ghost state); otherwise the
+// temporal-blocked sweeps of les_sor_tb.cuh (even jm, consistent ghosts).
+les_status enqueue_press(les_ctx *c, bool exact) {
     const Geo &g = c->geo;
     const dim3 rg(c->red_gx, c->red_gy, c->red_nk), rb(kRedBX, kRedBY);
     const int np = c->red_gx * c->red_gy * c->red_nk;
@@ -300,32 +364,53 @@ les_status enqueue_press(les_ctx *c) {
     LAUNCH(c, k_rhs, rg, rb, g, c->F, c->red_kchunk, c->d_part);
     LAUNCH(c, k_final_rhsav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
     MARK(c, EV_RHS);
-    for (int l = 0; l < c->prm.nmaxp; ++l) {
-        for (int nrd = 0; nrd <= 1; ++nrd) {
-            if (l == 0 && nrd == 0) MARK(c, EV_SOR1_START);
-            LAUNCH(c, k_sor_colour, rg, rb, g, c->F.p, c->F.rhs, nrd, c->red_kchunk, c->d_part + nrd * np, c->d_scal);
-            if (l == 0 && nrd == 0) MARK(c, EV_SOR1_END);
-            LAUNCH(c, k_boundp1<true>, dim3(cdiv(n1, 256)), dim3(256), g, c->F.p, c->d_scal);
+    if (exact) {
+        for (int l = 0; l < c->prm.nmaxp; ++l) {
+            for (int nrd = 0; nrd <= 1; ++nrd) {
+                if (l == 0 && nrd == 0) MARK(c, EV_SOR1_START);
+                if (c->cn1_box)
+                    LAUNCH(c, k_sor_colour<true>, rg, rb, g, c->F.p, c->F.rhs, c->cn1_box, nrd, c->red_kchunk,
+                           c->d_part + nrd * np, c->d_scal);
+                else
+                    LAUNCH(c, k_sor_colour<false>, rg, rb, g, c->F.p, c->F.rhs, nullptr, nrd, c->red_kchunk,
+                           c->d_part + nrd * np, c->d_scal);
+                if (l == 0 && nrd == 0) MARK(c, EV_SOR1_END);
+                LAUNCH(c, k_boundp1<true>, dim3(cdiv(n1, 256)), dim3(256), g, c->F.p, c->d_scal);
+            }
+            LAUNCH(c, k_boundp2<true>, dim3(cdiv(n2, 256)), dim3(256), g, c->F.p, c->d_scal);
+            LAUNCH(c, k_final_sor, dim3(1), dim3(1024), c->d_part, 2 * np, c->prm.pjuge, c->d_scal);
         }
-        LAUNCH(c, k_boundp2<true>, dim3(cdiv(n2, 256)), dim3(256), g, c->F.p, c->d_scal);
-        LAUNCH(c, k_final_sor, dim3(1), dim3(1024), c->d_part, 2 * np, c->prm.pjuge, c->d_scal);
+    } else {
+        const int nblk = c->tb_gx * c->tb_gy;
+        for (int done = 0, pass = 0; done < c->prm.nmaxp; ++pass) {
+            const int nit = std::min(c->tb_T, c->prm.nmaxp - done);
+            if (pass == 0) MARK(c, EV_SOR1_START);
+            les_status st = launch_sor_tb(c, c->tb_T, c->tb_ty, c->cn1_by_k, nit, 0);
+            if (st != LES_OK) return st;
+            if (pass == 0) MARK(c, EV_SOR1_END);
+            LAUNCH(c, k_final_tb, dim3(1), dim3(1024), c->d_part, nblk, nit, c->prm.pjuge, c->d_scal);
+            if ((st = launch_sor_tb(c, c->tb_T, c->tb_ty, c->cn1_by_k, nit, 1)) != LES_OK) return st;
+            LAUNCH(c, k_finish_redo, dim3(1), dim3(1), c->d_scal);
+            done += nit;
+        }
     }
     MARK(c, EV_SOR_END);
-    LAUNCH(c, k_pav_reduce, rg, rb, g, c->F.p, c->red_kchunk, c->d_part);
+    LAUNCH(c, k_pav_reduce, rg, rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, c->red_kchunk, c->d_part, c->d_scal);
     LAUNCH(c, k_final_pav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
-    LAUNCH(c, k_pav_adjust, dim3(c->red_gx, c->red_gy, g.km), rb, g, c->F.p, c->d_scal);
+    LAUNCH(c, k_pav_adjust, dim3(c->red_gx, c->red_gy, g.km), rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p,
+           c->d_scal);
     MARK(c, EV_PAV);
     return LES_OK;
 }
 
 // One time step after k_step_begin (main_ocl.f95:264-299).
-les_status enqueue_step(les_ctx *c, int n) {
+les_status enqueue_step(les_ctx *c, int n, bool exact_sor) {
     les_status s;
     MARK(c, EV_START);
     if ((s = enqueue_bondv1(c, n, true)) != LES_OK) return s;
     MARK(c, EV_BONDV1);
     if ((s = enqueue_velfg_les(c, true)) != LES_OK) return s;
-    if ((s = enqueue_press(c)) != LES_OK) return s;
+    if ((s = enqueue_press(c, exact_sor)) != LES_OK) return s;
     LAUNCH(c, k_probe, dim3(1), dim3(1), c->geo, c->F, c->d_scal);
     return LES_OK;
 }
@@ -345,6 +430,147 @@ les_status check_params(const les_params *p) {
     const long long tot = si * (p->jp + 4LL) * (p->kp + 4LL);
     if (tot >= (1LL << 31)) return fail(LES_ERR_DIMS, "grid too large for 32-bit box indexing");
     return LES_OK;
+}
+
+// Launch one temporal-blocked SOR pass (T iterations per pass, tile rows ty).
+les_status launch_sor_tb(les_ctx *c, int T, int ty, bool cn1k, int niter, int mode) {
+    const dim3 grid(cdiv(c->prm.ip, tb_tx(T)), cdiv(c->prm.jp, ty));
+    const size_t sm = tb_smem(T, ty);
+    const float *tab = c->geo.cnC ? c->d_tables + c->tl.cn1k : nullptr;
+    const Geo &g = c->geo;
+#define TBL(TT, KT)                                                                                      \
+    LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, dim3(kTbNT), sm, g, c->F.p, c->d_p2, c->F.rhs, tab, ty, niter, \
+                mode, c->d_part, c->d_scal)
+    switch (T * 2 + (cn1k ? 1 : 0)) {
+        case 2: TBL(1, false); break;
+        case 3: TBL(1, true); break;
+        case 4: TBL(2, false); break;
+        case 5: TBL(2, true); break;
+        case 6: TBL(3, false); break;
+        case 7: TBL(3, true); break;
+        default: return fail(LES_ERR_BAD_ARG, "SOR pass depth %d", T);
+    }
+#undef TBL
+    return LES_OK;
+}
+
+les_status set_tb_smem_attrs() {
+    // dynamic shared memory allowed on top of the kernel's static buffers
+    int dev = 0, optin = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const int mx = optin - 1024;
+#define TBA(TT, KT)                                                                                  \
+    CK(cudaFuncSetAttribute(k_sor_tb<TT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    TBA(1, false) TBA(1, true) TBA(2, false) TBA(2, true) TBA(3, false) TBA(3, true)
+#undef TBA
+    return LES_OK;
+}
+
+// Process-wide cache of autotuned SOR tiles: (ip, jp, kp, SMs) -> (T, ty).
+struct TuneKey {
+    int ip, jp, kp, nsm;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(ip, jp, kp, nsm) < std::tie(o.ip, o.jp, o.kp, o.nsm);
+    }
+};
+std::map<TuneKey, std::pair<int, int>> g_tune;
+std::mutex g_tune_mu;
+
+// Autotuner: time each candidate (T, ty) on this context's buffers with CUDA
+// events (two passes after one warm-up pass) and keep the fastest time per
+// SOR iteration.  Runs once per grid shape and device; LES_SOR_TILE=T,ty
+// overrides it.  Results persist in the file named by LES_TUNE_CACHE.
+les_status autotune_sor(les_ctx *c) {
+    int dev = 0, nsm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const TuneKey key{c->prm.ip, c->prm.jp, c->prm.kp, nsm};
+    int bestT = 0, bestTy = 0;
+    if (const char *ov = std::getenv("LES_SOR_TILE")) {
+        std::sscanf(ov, "%d,%d", &bestT, &bestTy);
+    } else {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            bestT = it->second.first;
+            bestTy = it->second.second;
+        }
+    }
+    const char *cache = std::getenv("LES_TUNE_CACHE");
+    if (!bestT && cache) {
+        if (FILE *fp = std::fopen(cache, "r")) {
+            int a, b, cc, d, t, y;
+            while (std::fscanf(fp, "%d %d %d %d %d %d", &a, &b, &cc, &d, &t, &y) == 6)
+                if (a == key.ip && b == key.jp && cc == key.kp && d == key.nsm) bestT = t, bestTy = y;
+            std::fclose(fp);
+        }
+    }
+    if (!bestT) {
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        double best = 0.0;
+        const int tys[] = {8, 12, 16, 20, 24, 28, 32, 40, 48, 56};
+        for (int T = 1; T <= kTbTMax; ++T)
+            for (int ty : tys) {
+                if (!tb_fits(T, ty) || tb_smem(T, ty) > 226 * 1024) continue;
+                const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(T)) * cdiv(c->prm.jp, ty);
+                if (nblk * kTbTMax > c->npart) continue;
+                CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
+                les_status st = launch_sor_tb(c, T, ty, c->cn1_by_k, T, 0);
+                if (st != LES_OK) return st;
+                CK(cudaEventRecord(e0, c->stream));
+                for (int r = 0; r < 2; ++r)
+                    if ((st = launch_sor_tb(c, T, ty, c->cn1_by_k, T, 0)) != LES_OK) return st;
+                CK(cudaEventRecord(e1, c->stream));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                const double per_iter = ms / (2.0 * T);
+                if (!bestT || per_iter < best) best = per_iter, bestT = T, bestTy = ty;
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (!bestT) return fail(LES_ERR_DIMS, "no SOR tile shape fits");
+        if (cache)
+            if (FILE *fp = std::fopen(cache, "a")) {
+                std::fprintf(fp, "%d %d %d %d %d %d\n", key.ip, key.jp, key.kp, key.nsm, bestT, bestTy);
+                std::fclose(fp);
+            }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = {bestT, bestTy};
+    }
+    if (bestT < 1 || bestT > kTbTMax || !tb_fits(bestT, bestTy) || tb_smem(bestT, bestTy) > 226 * 1024)
+        return fail(LES_ERR_BAD_ARG, "SOR tile %d,%d out of range", bestT, bestTy);
+    c->tb_T = bestT;
+    c->tb_ty = bestTy;
+    c->tb_smem = tb_smem(bestT, bestTy);
+    c->tb_gx = cdiv(c->prm.ip, tb_tx(bestT));
+    c->tb_gy = cdiv(c->prm.jp, bestTy);
+    return LES_OK;
+}
+
+// True when p's ghosts hold what boundp1 then boundp2 would give
+// (boundp.f95:5-44), the state every press ends in.
+bool p_ghosts_consistent(const float *p, int ip, int jp, int kp) {
+    const size_t ni = ip + 3, nj = jp + 3;
+    auto P = [&](int i, int j, int k) { return p[(size_t)i + ni * ((size_t)j + nj * (size_t)k)]; };
+    auto same = [](float a, float b) { return std::memcmp(&a, &b, 4) == 0; };
+    for (int k = 1; k <= kp; ++k)
+        for (int j = 1; j <= jp; ++j)
+            if (!same(P(0, j, k), P(1, j, k)) || !same(P(ip + 1, j, k), P(ip, j, k))) return false;
+    for (int k = 1; k <= kp; ++k)
+        for (int i = 1; i <= ip; ++i)
+            if (!same(P(i, 0, k), P(i, jp, k)) || !same(P(i, jp + 1, k), P(i, 1, k))) return false;
+    for (int j = 1; j <= jp; ++j)
+        for (int i = 1; i <= ip; ++i)
+            if (!same(P(i, j, 0), P(i, j, 1)) || !same(P(i, j, kp + 1), P(i, j, kp))) return false;
+    return true;
 }
 
 }  // namespace
@@ -404,7 +630,9 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     g.omega = prm->omega;
     c->box_elems = (size_t)g.si * g.sj * g.sk;
     auto cleanup = [&](les_status st) {
+        const std::string msg = g_err;  // destroy resets the error string
         les_ctx_destroy(c);
+        g_err = msg;
         return st;
     };
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -429,10 +657,27 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     c->red_kchunk = cdiv(kp, nk);
     c->red_nk = cdiv(kp, c->red_kchunk);
     c->npart = 2 * c->red_gx * c->red_gy * c->red_nk;
+    if (set_tb_smem_attrs() != LES_OK) return cleanup(LES_ERR_CUDA);
+    {
+        const int ms = (int)mom_smem(false);
+        const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        if (cudaFuncSetAttribute(k_mom1<true>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom1<false>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<true, true>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<true, false>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<false, true>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<false, false>, A, ms) != cudaSuccess)
+            return cleanup(fail(LES_ERR_CUDA, "shared memory attribute"));
+    }
+    c->npart = std::max(c->npart, kTbTMax * cdiv(ip, tb_tx(kTbTMax)) * cdiv(jp, 8));
     if (cudaMalloc(&c->d_part, sizeof(FixPart) * c->npart) != cudaSuccess)
         return cleanup(fail(LES_ERR_NOMEM, "partials"));
-    // staging buffer for Fortran-layout arrays (largest: w or p)
-    size_t mx = 0;
+    if (cudaMalloc(&c->d_p2, sizeof(float) * c->box_elems) != cudaSuccess)
+        return cleanup(fail(LES_ERR_NOMEM, "second p buffer"));
+    cudaMemsetAsync(c->d_p2, 0, sizeof(float) * c->box_elems, c->stream);
+    // staging buffer for Fortran-layout arrays: the largest is diu1/diu5
+    // (-1:ip+2, 0:jp+2, 0:kp+2) of the per-routine velfg/les entries
+    size_t mx = (size_t)(ip + 4) * (jp + 3) * (kp + 3);
     for (int f = 0; f < LES_NFIELDS; ++f) mx = std::max(mx, field_bounds(f, ip, jp, kp).n());
     c->stage_elems = mx;
     if (cudaMalloc(&c->d_stage, sizeof(float) * mx) != cudaSuccess) return cleanup(fail(LES_ERR_NOMEM, "stage"));
@@ -455,6 +700,10 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     g.cnC = base + t.cnC - 1;
     g.smc = base + t.smc - 1;
     g.wind = base + t.wind;
+    g.rdx1 = base + t.rdx1 + 1;
+    g.rsx = base + t.rsx + 1;
+    g.rdy1 = base + t.rdy1;
+    g.rsy = base + t.rsy;
     float **fp[LES_NFIELDS] = {&c->F.u,    &c->F.v,    &c->F.w,    &c->F.p,     &c->F.usum,  &c->F.vsum,  &c->F.wsum,
                                &c->F.f,    &c->F.g,    &c->F.h,    &c->F.fold,  &c->F.gold,  &c->F.hold,  &c->F.rhs,
                                &c->F.sm,   &c->F.amask, &c->F.bmask, &c->F.cmask, &c->F.dmask};
@@ -472,11 +721,13 @@ les_status les_ctx_destroy(les_ctx *c) {
     for (auto &gs : c->graph_src)
         if (gs) cudaGraphDestroy(gs);
     for (auto e : c->tev) cudaEventDestroy(e);
+    for (auto x : c->extra) cudaFree(x);
     cudaFree(c->d_fields);
     cudaFree(c->d_tables);
     cudaFree(c->d_scal);
     cudaFree(c->d_part);
     cudaFree(c->d_stage);
+    cudaFree(c->d_p2);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ok();
@@ -528,7 +779,7 @@ les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
     if (!hf->dx1 || !hf->dy1 || !hf->dzn || !hf->dzs || !hf->dxs || !hf->dys || !hf->cn2l || !hf->cn2s ||
         !hf->cn3l || !hf->cn3s || !hf->cn4l || !hf->cn4s)
         return fail(LES_ERR_BAD_ARG, "metric tables and Poisson coefficients are required");
-    les_status s = build_tables(c, hf);
+    les_status s = build_tables(c, hf, true);
     if (s != LES_OK) return s;
     const float *src[LES_NFIELDS] = {hf->u,    hf->v,    hf->w,    hf->p,   hf->usum,   hf->vsum,   hf->wsum,
                                      hf->f,    hf->g,    hf->h,    hf->fold, hf->gold,  hf->hold,   hf->rhs,
@@ -554,6 +805,7 @@ les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
     CK(cudaStreamSynchronize(c->stream));
     c->uploaded = true;
     c->rhs_raw = false;
+    c->p_ghosts_ok = hf->p ? p_ghosts_consistent(hf->p, c->prm.ip, c->prm.jp, c->prm.kp) : false;
     return ok();
 }
 
@@ -587,6 +839,26 @@ les_status les_ctx_warmup(les_ctx *c, int n) {
     if ((s = enqueue_boundp(c, false)) != LES_OK) return s;
     if ((s = enqueue_velfg_les(c, false)) != LES_OK) return s;
     CK(cudaStreamSynchronize(c->stream));
+    c->p_ghosts_ok = true;  // ifdata.f95:260-262 applied boundp1, boundp2
+    return ok();
+}
+
+les_status les_ctx_sor_tile(les_ctx *c, int *T, int *ty) {
+    if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    if (T) *T = c->tb_T;
+    if (ty) *ty = c->tb_ty;
+    return ok();
+}
+
+float les_ctx_sor_iters_per_launch(les_ctx *c) {
+    if (!c) return 0.0f;
+    const bool exact = c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok;
+    return exact ? 0.5f : (float)(c->tb_T ? c->tb_T : 2);
+}
+
+les_status les_ctx_set_sor_path(les_ctx *c, int exact) {
+    if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    c->force_exact_sor = exact != 0;
     return ok();
 }
 
@@ -604,14 +876,19 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
     if (nsteps < 0) return fail(LES_ERR_BAD_ARG, "nsteps < 0");
     for (int s = 0; s < nsteps; ++s) {
         const int n = n0 + s;
-        const int gi = (n == 1 && c->prm.ical == 0) ? 1 : 0;
+        const bool exact = c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok;
+        const int gi = ((n == 1 && c->prm.ical == 0) ? 1 : 0) + (exact ? 2 : 0);
+        if (!exact && c->tb_T == 0) {
+            les_status st = autotune_sor(c);
+            if (st != LES_OK) return st;
+        }
         if (!c->graph[gi]) {
             // Capture the step once per kind (n==1 broadcast or not); the
             // kernels only see n through that distinction.
             const uint64_t before = c->launches;
             c->capturing_timed = c->tslots > 0;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            les_status st = enqueue_step(c, gi ? 1 : 2);
+            les_status st = enqueue_step(c, (gi & 1) ? 1 : 2, exact);
             cudaGraph_t gr = nullptr;
             cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
             c->capturing_timed = false;
@@ -661,6 +938,7 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
         c->launches += c->graph_kernels[gi];
         c->last_n = n;
         c->rhs_raw = true;
+        c->p_ghosts_ok = true;  // press ends with boundp1/boundp2
     }
     return ok();
 }
@@ -668,16 +946,18 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
 les_status les_ctx_set_timing(les_ctx *c, int nslots) {
     if (!c || nslots < 0) return fail(LES_ERR_BAD_ARG, "bad argument");
     CK(cudaStreamSynchronize(c->stream));
-    if ((nslots > 0) != (c->tslots > 0)) {  // graphs are re-captured with or without event nodes
-        for (int gi = 0; gi < 2; ++gi) {
-            if (c->graph[gi]) cudaGraphExecDestroy(c->graph[gi]);
-            if (c->graph_src[gi]) cudaGraphDestroy(c->graph_src[gi]);
-            c->graph[gi] = nullptr;
-            c->graph_src[gi] = nullptr;
-        }
+    if (nslots > 0 && c->tslots > 0 && (size_t)nslots * LES_NTEV <= c->tev.size()) {
+        c->tslots = nslots;  // re-arm: the pool and the captured graphs stay
+        c->tslot = 0;
+        return ok();
     }
-    // event nodes of existing graphs are re-pointed before every launch, so
-    // the pool can be replaced freely
+    // graphs are re-captured with (or without) event nodes for the new pool
+    for (int gi = 0; gi < 4; ++gi) {
+        if (c->graph[gi]) cudaGraphExecDestroy(c->graph[gi]);
+        if (c->graph_src[gi]) cudaGraphDestroy(c->graph_src[gi]);
+        c->graph[gi] = nullptr;
+        c->graph_src[gi] = nullptr;
+    }
     for (auto e : c->tev) cudaEventDestroy(e);
     c->tev.assign((size_t)nslots * LES_NTEV, nullptr);
     for (auto &e : c->tev) CK(cudaEventCreate(&e));
@@ -800,3 +1080,5 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 }
 
 }  // extern "C"
+
+#include "les_routines_api.inc"

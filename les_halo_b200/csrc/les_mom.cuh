@@ -1,0 +1,325 @@
+// les_mom.cuh -- momentum kernels built on a 2.5-D tile of face quantities.
+//
+// vel2.f95 materialises 27 face arrays (nou/diu/cov 1..9) that velFG.f95
+// and les.f95 then read around every cell.  Here a CTA owns a 32 x 8 tile of
+// (i,j) columns plus a one-cell ring, marches k, and evaluates the 18 values
+// diu1..9 / cov1..9 of every ring position once per plane into a two-plane
+// shared-memory ring (diu7/diu8 of the plane below are kept aside).  The
+// cell formulas then read their neighbours from shared memory.  Each value
+// equals what the reference's array holds after vel2 (the formula on its
+// computed range, the boundary copies of vel2.f95:125-188, zero elsewhere),
+// so results are bit-identical to the per-cell kernels of les_step.cuh.
+#pragma once
+#include "les_step.cuh"
+
+namespace les {
+namespace {  // kernels get internal linkage: each .cu has its own copy
+
+constexpr int kMX = 32, kMY = 8, kMNT = 256;
+constexpr int kMEX = kMX + 2, kMEY = kMY + 2, kMPOS = kMEX * kMEY;
+enum { V_D1 = 0, V_C1 = 9, NV = 18 };
+
+// u, v, w staged in shared memory: a band of (32+4) x (8+4) columns/rows
+// around the tile per plane, five plane slots (k-1..k+2 in use, k+3 loading).
+// Band row b holds real row jwrap(jb2 + b); a real row j is found by moving
+// it by +-jm into the band.  Valid when the band is not taller than jm.
+constexpr int kBW = kMX + 4, kBH = kMY + 4, kBA = kBW * kBH, kBS = 5;
+struct UVWBand {
+    const float *base;  // slot s, field f at base + (s*3 + f)*kBA
+    int ib2, jb2;       // real (i, j) of band position (0, 0)
+    __device__ __forceinline__ int off(const Geo &g, int i, int j, int k) const {
+        int r = j - jb2;
+        if (r >= kBH) r -= g.jm;
+        if (r < 0) r += g.jm;
+        return ((k + 1) % kBS) * 3 * kBA + r * kBW + (i - ib2);
+    }
+    __device__ __forceinline__ float U(const Geo &g, int i, int j, int k) const { return base[off(g, i, j, k)]; }
+    __device__ __forceinline__ float V(const Geo &g, int i, int j, int k) const { return base[off(g, i, j, k) + kBA]; }
+    __device__ __forceinline__ float W(const Geo &g, int i, int j, int k) const {
+        return base[off(g, i, j, k) + 2 * kBA];
+    }
+};
+
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Issue the copies of plane k (k in -1..kp+2) of u, v, w into its slot.  A
+// band row is 36 floats starting at an even box offset (ib2 + 31 = 32*bx +
+// 30), copied as 18 pairs; columns past the box row end read the next row
+// (still inside the allocation) and are never used.
+__device__ __forceinline__ void band_load(const Geo &g, const Fields &F, float *base, int ib2, int jb2, int k) {
+    float *slot = base + ((k + 1) % kBS) * 3 * kBA;
+    const int npair = kBW / 2;
+    for (int e = threadIdx.x; e < 3 * kBH * npair; e += kMNT) {
+        const int f = e / (kBH * npair), rem = e % (kBH * npair);
+        const int b = rem / npair, pr = rem % npair;
+        const int j = ((jb2 + b - 1) % g.jm + g.jm) % g.jm + 1;
+        const float *src = (f == 0 ? F.u : (f == 1 ? F.v : F.w)) + IX(g, ib2 + 2 * pr, j, k);
+        cp_async8(slot + f * kBA + b * kBW + 2 * pr, src);
+    }
+}
+
+// diu_n and cov_n at (i,j,k) (n = 1..9), as the arrays hold them after vel2.
+template <class Q>
+__device__ __forceinline__ void vel2_pair(const Geo &g, const Q &q, int n, int i, int j, int k, float &d, float &c) {
+    const int im = g.im, jm = g.jm, km = g.km;
+    auto in = [](int x, int a, int b) { return x >= a && x <= b; };
+    d = 0.0f;
+    c = 0.0f;
+    switch (n) {
+        case 1:
+            if (in(j, 1, jm) && in(k, 1, km) && in(i, 1, im + 1)) {
+                const int ii = min(i, im);
+                d = diu1_raw(g, q, ii, j, k);
+                c = nou1_raw(g, q, ii, j, k) * d;
+            }
+            break;
+        case 5: {
+            const int jj = jper(g, j);
+            if (jj && in(i, 1, im) && in(k, 1, km)) {
+                d = diu5_raw(g, q, i, jj, k);
+                c = nou5_raw(g, q, i, jj, k) * d;
+            }
+        } break;
+        case 9:
+            if (in(i, 1, im) && in(j, 1, jm) && in(k, 1, km)) {
+                d = diu9_raw(g, q, i, j, k);
+                c = nou9_raw(g, q, i, j, k) * d;
+            }
+            break;
+        case 2: {
+            const int jj = jper(g, j);
+            if (jj && in(i, 1, im) && in(k, 1, km)) {
+                d = diu2_raw(g, q, i, jj, k);
+                c = nou2_raw(g, q, i, jj, k) * d;
+            } else if (i == im + 1 && in(j, 1, jm + 1) && in(k, 1, km)) {
+                d = diu2_raw(g, q, im, jper(g, j), k);  // vel2.f95:177-182
+            }
+        } break;
+        case 3:
+            if (in(i, 1, im) && in(j, 1, jm) && in(k, 1, km + 1)) {
+                d = diu3_raw(g, q, i, j, k);
+                c = nou3_raw(g, q, i, j, k) * d;
+            } else if (i == im + 1 && in(j, 1, jm) && in(k, 1, km + 1)) {
+                d = diu3_raw(g, q, im, j, k);
+            }
+            break;
+        case 4:
+            if (in(j, 1, jm) && in(k, 1, km) && in(i, 1, im + 1)) {
+                const int ii = min(i, im);
+                d = diu4_raw(g, q, ii, j, k);
+                c = (nou4_raw(g, q, ii, j, k) - 0.0f) * d;
+            } else if (j == 0 && in(i, 1, im + 1) && in(k, 1, km)) {
+                d = diu4_raw(g, q, min(i, im), jm, k);  // vel2.f95:183-188
+            }
+            break;
+        case 6:
+            if (in(i, 1, im) && in(j, 1, jm) && in(k, 1, km + 1)) {
+                d = diu6_raw(g, q, i, j, k);
+                c = nou6_raw(g, q, i, j, k) * d;
+            } else if (j == 0 && in(i, 1, im) && in(k, 1, km + 1)) {
+                d = diu6_raw(g, q, i, jm, k);
+            }
+            break;
+        case 7:
+            if (in(j, 1, jm) && in(k, 1, km - 1) && in(i, 1, im + 1)) {
+                const int ii = min(i, im);
+                d = diu7_raw(g, q, ii, j, k);
+                c = (nou7_raw(g, q, ii, j, k) - 0.0f) * d;
+            }
+            break;
+        default: {  // 8
+            const int jj = jper(g, j);
+            if (jj && in(i, 1, im) && in(k, 1, km - 1)) {
+                d = diu8_raw(g, q, i, jj, k);
+                c = nou8_raw(g, q, i, jj, k) * d;
+            }
+        } break;
+    }
+}
+
+// Shared-memory view: plane slots cur (k), nxt (k+1) and prv78 (diu7, diu8
+// of k-1), for the cell policies of les_step.cuh.
+struct TileView {
+    const float *cur, *nxt, *prv7, *prv8;
+    int ib, jb, kc;  // i, j of ring position 0 and the current plane
+    __device__ __forceinline__ int pos(int i, int j) const { return (j - jb) * kMEX + (i - ib); }
+    __device__ __forceinline__ float dv(int n, int i, int j, int k) const {
+        const int p = pos(i, j);
+        if (k == kc) return cur[(V_D1 + n - 1) * kMPOS + p];
+        if (k == kc + 1) return nxt[(V_D1 + n - 1) * kMPOS + p];
+        return (n == 7) ? prv7[p] : prv8[p];  // k == kc-1: only diu7, diu8 are read
+    }
+    __device__ __forceinline__ float cv(int n, int i, int j, int k) const {
+        const int p = pos(i, j);
+        return (k == kc ? cur : nxt)[(V_C1 + n - 1) * kMPOS + p];
+    }
+    __device__ __forceinline__ float d1(int i, int j, int k) const { return dv(1, i, j, k); }
+    __device__ __forceinline__ float d2(int i, int j, int k) const { return dv(2, i, j, k); }
+    __device__ __forceinline__ float d3(int i, int j, int k) const { return dv(3, i, j, k); }
+    __device__ __forceinline__ float d4(int i, int j, int k) const { return dv(4, i, j, k); }
+    __device__ __forceinline__ float d5(int i, int j, int k) const { return dv(5, i, j, k); }
+    __device__ __forceinline__ float d6(int i, int j, int k) const { return dv(6, i, j, k); }
+    __device__ __forceinline__ float d7(int i, int j, int k) const { return dv(7, i, j, k); }
+    __device__ __forceinline__ float d8(int i, int j, int k) const { return dv(8, i, j, k); }
+    __device__ __forceinline__ float d9(int i, int j, int k) const { return dv(9, i, j, k); }
+};
+
+// velFG.f95:58-105 for one cell from the tile.
+__device__ __forceinline__ void velfg_tile(const Geo &g, const TileView &t, int i, int j, int k, float &fv, float &gv,
+                                           float &hv) {
+    const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn, *dzs = g.dzs;
+    {
+        float covx1 = fdiv(dx1[i + 1] * t.cv(1, i, j, k) + dx1[i] * t.cv(1, i + 1, j, k), dx1[i] + dx1[i + 1], g.rsx[i]);
+        float covy1 = (t.cv(2, i, j, k) + t.cv(2, i, j + 1, k)) / 2.0f;
+        float covz1 = (t.cv(3, i, j, k) + t.cv(3, i, j, k + 1)) / 2.0f;
+        float covc = covx1 + covy1 + covz1;
+        float dfu1 = fdiv(2.0f * (-t.d1(i, j, k) + t.d1(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]) +
+                     fdiv(-t.d2(i, j, k) + t.d2(i, j + 1, k), dy1[j], g.rdy1[j]) +
+                     (-t.d3(i, j, k) + t.d3(i, j, k + 1)) / dzn[k];
+        fv = (-covc + g.vn * dfu1);
+    }
+    {
+        float covx1 = (t.cv(4, i, j, k) + t.cv(4, i + 1, j, k)) / 2.0f;
+        float covy1 = fdiv(dy1[j + 1] * t.cv(5, i, j, k) + dy1[j] * t.cv(5, i, j + 1, k), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float covz1 = (t.cv(6, i, j, k) + t.cv(6, i, j, k + 1)) / 2.0f;
+        float covc = covx1 + covy1 + covz1;
+        float dfv1 = fdiv(-t.d4(i, j, k) + t.d4(i + 1, j, k), dx1[i], g.rdx1[i]) +
+                     fdiv(2.0f * (-t.d5(i, j, k) + t.d5(i, j + 1, k)), dy1[j] + dy1[j + 1], g.rsy[j]) +
+                     (-t.d6(i, j, k) + t.d6(i, j, k + 1)) / dzn[k];
+        gv = (-covc + g.vn * dfv1);
+    }
+    if (k <= g.km - 1) {
+        float covx1 = (t.cv(7, i, j, k) + t.cv(7, i + 1, j, k)) / 2.0f;
+        float covy1 = (t.cv(8, i, j, k) + t.cv(8, i, j + 1, k)) / 2.0f;
+        float covz1 = (dzn[k + 1] * t.cv(9, i, j, k) + dzn[k] * t.cv(9, i, j, k + 1)) / (dzn[k] + dzn[k + 1]);
+        float covc = covx1 + covy1 + covz1;
+        float dfw1 = fdiv(-t.d7(i, j, k) + t.d7(i + 1, j, k), dx1[i], g.rdx1[i]) +
+                     fdiv(-t.d8(i, j, k) + t.d8(i, j + 1, k), dy1[j], g.rdy1[j]) +
+                     (-t.d9(i, j, k) + t.d9(i, j, k + 1)) / dzs[k];
+        hv = (-covc + g.vn * dfw1);
+    }
+}
+
+// Fill plane slot `dst` with the 18 values of plane k over the ring; copy
+// the diu7/diu8 the slot held (plane k-2) into prv7/prv8 first if asked.
+template <bool DIU_ONLY, class Q>
+__device__ __forceinline__ void tile_plane(const Geo &g, const Q &q, float *dst, float *prv7, float *prv8, int ib,
+                                           int jb, int k, bool save_prev) {
+    for (int p = threadIdx.x; p < kMPOS; p += kMNT) {
+        const int i = ib + p % kMEX, j = jb + p / kMEX;
+        if (save_prev) {
+            prv7[p] = dst[(V_D1 + 6) * kMPOS + p];
+            prv8[p] = dst[(V_D1 + 7) * kMPOS + p];
+        }
+#pragma unroll
+        for (int n = 1; n <= 9; ++n) {
+            float d, c;
+            vel2_pair(g, q, n, i, j, k, d, c);
+            dst[(V_D1 + n - 1) * kMPOS + p] = d;
+            if (!DIU_ONLY) dst[(V_C1 + n - 1) * kMPOS + p] = c;
+        }
+    }
+}
+
+// shared memory: two face-value planes (18 or 9 values), diu7/diu8 of the
+// plane below, and the u,v,w band slots
+__host__ __device__ constexpr size_t mom_smem(bool diu_only) {
+    return sizeof(float) * (2 * (diu_only ? 9 : NV) * kMPOS + 2 * kMPOS + kBS * 3 * kBA);
+}
+
+// Shared prologue/march of both momentum kernels: stage u,v,w planes, fill
+// the face-value ring plane by plane, call `cell` for every tile cell.
+template <bool DIU_ONLY, bool BAND, class CellFn>
+__device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn cell) {
+    extern __shared__ float sh[];
+    constexpr int NVU = DIU_ONLY ? 9 : NV;
+    float *slot[2] = {sh, sh + NVU * kMPOS};
+    float *prv7 = sh + 2 * NVU * kMPOS, *prv8 = prv7 + kMPOS;
+    float *band = prv8 + kMPOS;
+    const int i0 = 1 + blockIdx.x * kMX, j0 = 1 + blockIdx.y * kMY;
+    const int ib = i0 - 1, jb = j0 - 1;
+    const UVW qg{F.u, F.v, F.w};
+    const UVWBand qb{band, i0 - 2, j0 - 2};
+    auto fill = [&](float *dst, int k, bool save) {
+        if (BAND)
+            tile_plane<DIU_ONLY>(g, qb, dst, prv7, prv8, ib, jb, k, save);
+        else
+            tile_plane<DIU_ONLY>(g, qg, dst, prv7, prv8, ib, jb, k, save);
+    };
+    if (BAND) {  // planes -1..1 and 0..2 fill the first two face planes; 3 is needed at k=1
+        for (int k = -1; k <= 3; ++k) band_load(g, F, band, i0 - 2, j0 - 2, k);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+    }
+    fill(slot[0], 0, false);
+    fill(slot[1], 1, false);
+    __syncthreads();
+    for (int k = 1; k <= g.km; ++k) {
+        if (BAND) {  // plane k+3 streams in while plane k+1 is filled from k..k+2
+            if (k + 3 <= g.km + 2) band_load(g, F, band, i0 - 2, j0 - 2, k + 3);
+            cp_async_commit();
+        }
+        // slot (k+1)&1 holds plane k-1: keep its diu7/diu8, then plane k+1
+        fill(slot[(k + 1) & 1], k + 1, true);
+        __syncthreads();
+        const TileView t{slot[k & 1], slot[(k + 1) & 1], prv7, prv8, ib, jb, k};
+        cell(t, k);
+        if (BAND) cp_async_wait<0>();
+        __syncthreads();
+    }
+}
+
+// velFG + feedbf + sgs viscosity (les.f95:132-152) for a 32 x 8 tile, all k.
+template <bool BAND>
+__global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
+    const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
+    const bool mine = (i <= g.im && j <= g.jm);
+    mom_march<false, BAND>(g, F, [&](const TileView &t, int k) {
+        if (!mine) return;
+        const int c = IX(g, i, j, k);
+        float fv, gv, hv = F.h[c];
+        velfg_tile(g, t, i, j, k, fv, gv, hv);
+        float fx, fy, fz;
+        feedbf_cell(g, F, c, __ldg(&F.u[c]), __ldg(&F.v[c]), __ldg(&F.w[c]), fx, fy, fz);
+        F.f[c] = fv + fx;
+        F.g[c] = gv + fy;
+        F.h[c] = hv + fz;
+        F.sm[c] = sgs_sm(g, t, i, j, k);
+    });
+}
+
+// les.f95:170-274 viscous terms (+ adam.f95:32-46) for a 32 x 8 tile, all k.
+template <bool ADAM, bool BAND>
+__global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
+    const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
+    const bool mine = (i <= g.im && j <= g.jm);
+    mom_march<true, BAND>(g, F, [&](const TileView &t, int k) {
+        if (!mine) return;
+        float vfu, vfv, vfw;
+        visc_cell(g, t, F.sm, i, j, k, vfu, vfv, vfw);
+        const int c = IX(g, i, j, k);
+        const float fv = F.f[c] + vfu, gv = F.g[c] + vfv, hv = F.h[c] + vfw;
+        if (ADAM) {
+            F.f[c] = 1.5f * fv - 0.5f * F.fold[c];
+            F.g[c] = 1.5f * gv - 0.5f * F.gold[c];
+            F.h[c] = 1.5f * hv - 0.5f * F.hold[c];
+            F.fold[c] = fv;
+            F.gold[c] = gv;
+            F.hold[c] = hv;
+        } else {
+            F.f[c] = fv;
+            F.g[c] = gv;
+            F.h[c] = hv;
+        }
+    });
+}
+
+}  // namespace
+}  // namespace les

@@ -50,6 +50,42 @@ __global__ void __launch_bounds__(kRedNT) k_rhs(Geo g, Fields F, int kchunk, Fix
     block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
 }
 
+// Sum FixParts part[b*stride + off], b < n, with one block; thread 0 gets
+// the total.  Ends with the block synchronised.
+__device__ __forceinline__ void final_fix_strided(const FixPart *part, int n, int stride, int off, i128 &tot,
+                                                  int &bad) {
+    __shared__ unsigned long long s_lo[32];
+    __shared__ long long s_hi[32];
+    __shared__ int s_bad[32];
+    i128 acc = 0;
+    int b = 0;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const FixPart &q = part[(size_t)t * stride + off];
+        acc += fix_from_part(q);
+        b |= q.bad;
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        acc += shfl_down_i128(acc, o);
+        b |= __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_lo[wid] = (unsigned long long)acc;
+        s_hi[wid] = (long long)(acc >> 64);
+        s_bad[wid] = b;
+    }
+    __syncthreads();
+    tot = 0;
+    bad = 0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            tot += (i128)(((unsigned __int128)(unsigned long long)s_hi[w] << 64) | (unsigned __int128)s_lo[w]);
+            bad |= s_bad[w];
+        }
+    }
+    __syncthreads();
+}
+
 // Sum FixParts with one block; the finisher maps the total to the scalars.
 __device__ __forceinline__ void final_fix(const FixPart *part, int n, i128 &tot, int &bad) {
     __shared__ unsigned long long s_lo[32];
@@ -93,9 +129,12 @@ __global__ void __launch_bounds__(1024) k_final_rhsav(const FixPart *part, int n
 // One SOR colour sweep, press.f95:153-163 with nrd = colour: cells with
 // (i+j+k+nrd) odd.  Within a colour every update reads only cells of the
 // other colour and ghost cells, so the in-place parallel sweep equals the
-// reference's sequential one.  cn1 is rebuilt from its separable parts.
+// reference's sequential one.  cn1 is rebuilt from its separable parts, or
+// read from the caller's array (CN1MEM, the per-routine press entry).
+template <bool CN1MEM>
 __global__ void __launch_bounds__(kRedNT) k_sor_colour(Geo g, float *__restrict__ p, const float *__restrict__ rhs,
-                                                        int nrd, int kchunk, FixPart *part, const Scal *s) {
+                                                        const float *__restrict__ cn1b, int nrd, int kchunk,
+                                                        FixPart *part, const Scal *s) {
     if (s->converged) return;
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
@@ -110,7 +149,7 @@ __global__ void __launch_bounds__(kRedNT) k_sor_colour(Geo g, float *__restrict_
         int k = k0 + (((i + j + k0 + nrd) & 1) ? 0 : 1);
         for (; k <= k1; k += 2) {
             const int c = IX(g, i, j, k);
-            const float cn1 = 1.0f / (cA + cB + g.cnC[k]);
+            const float cn1 = CN1MEM ? cn1b[c] : 1.0f / (cA + cB + g.cnC[k]);
             const float pc = p[c];
             const float reltmp =
                 g.omega * (cn1 * (c2l * p[c + 1] + c2s * p[c - 1] + c3l * p[c + g.si] + c3s * p[c - g.si] +
@@ -184,7 +223,9 @@ __global__ void __launch_bounds__(1024) k_final_sor(const FixPart *part, int n, 
 }
 
 // press.f95:186-195 partial sums of p*dx1*dy1*dzn.
-__global__ void __launch_bounds__(kRedNT) k_pav_reduce(Geo g, const float *__restrict__ p, int kchunk, FixPart *part) {
+__global__ void __launch_bounds__(kRedNT) k_pav_reduce(Geo g, const float *p0, const float *p1, int kchunk,
+                                                        FixPart *part, const Scal *sc) {
+    const float *__restrict__ p = sc->pbuf ? p1 : p0;
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
     const int k0 = 1 + blockIdx.z * kchunk;
@@ -207,13 +248,15 @@ __global__ void __launch_bounds__(1024) k_final_pav(const FixPart *part, int n, 
 
 // press.f95:197-209: p -= pav on the interior, then boundp1 and boundp2.
 // The interior thread writes its new value and every ghost whose final
-// source it is: ghost (i,j,k) <- (clamp(i), periodic(j), clamp(k)).
-__global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *__restrict__ p, const Scal *s) {
+// source it is: ghost (i,j,k) <- (clamp(i), periodic(j), clamp(k)).  The
+// SOR result may sit in the second buffer (s->pbuf); the state p is written.
+__global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *p, const float *p1, const Scal *s) {
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
     const int k = 1 + blockIdx.z;
     if (i > g.im || j > g.jm) return;
-    const float val = p[IX(g, i, j, k)] - s->pav;
+    const float *src = s->pbuf ? p1 : p;
+    const float val = src[IX(g, i, j, k)] - s->pav;
     int is[2], js[2], ks[2];
     int ni = 0, nj = 0, nk = 0;
     is[ni++] = i;
@@ -236,6 +279,8 @@ __global__ void k_step_begin(Scal *s, int n) {
     s->uout_neg = 0u;
     s->converged = 0;
     s->sor_iters = 0;
+    s->redo = 0;
+    s->pbuf = 0;
     s->n = n;
 }
 __global__ void k_probe(Geo g, Fields F, Scal *s) {

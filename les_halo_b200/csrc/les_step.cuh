@@ -13,15 +13,17 @@ namespace {  // kernels get internal linkage: each .cu has its own copy
 // velnw.f95:27-59 fused with the inflow of bondv1.f95:26-45 /
 // bondv1_ext_wind_profile.f95:27-35 and the n==1 broadcast of
 // bondv1.f95:47-59 (ICAL=0).  Cells i in 0..im, j in 1..jm, k in 1..km.
-// VELNW=false gives the bondv1 part alone (ifdata.f95:258).
-template <bool VELNW>
+// VELNW=false gives the bondv1 part alone (ifdata.f95:258); INFLOW=false
+// gives velnw alone (velnw.f95, the per-routine entry).
+template <bool VELNW, bool INFLOW = true>
 __global__ void __launch_bounds__(128) k_velnw_inflow(Geo g, Fields F, int n, int ical) {
     const int i = blockIdx.x * 32 + threadIdx.x;  // 0..
     const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int k = 1 + blockIdx.z;
     if (i > g.im || j > g.jm) return;
+    if (!INFLOW && i == 0) return;
     const int c = IX(g, i, j, k);
-    const bool bc = (i <= 1) || (n == 1 && ical == 0);
+    const bool bc = INFLOW && ((i <= 1) || (n == 1 && ical == 0));
     if (bc) {
         F.u[c] = g.wind[(j - 1) + g.jm * (k - 1)];
         F.v[c] = 0.0f;
@@ -141,27 +143,51 @@ __global__ void __launch_bounds__(256) k_uvw_ghosts(Geo g, Fields F) {
     }
 }
 
-// velFG.f95:58-105 + feedbf.f95:38-67 + les.f95:124-152 (sm) for one cell.
-// h(i,j,km) is not written by velfg (its loop stops at km-1): it keeps the
-// value it had, to which feedbf adds fz.
-__global__ void __launch_bounds__(128) k_velfg_feedbf_sm(Geo g, Fields F) {
-    const int i = 1 + blockIdx.x * 32 + threadIdx.x;
-    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = 1 + blockIdx.z;
-    if (i > g.im || j > g.jm) return;
-    const UVW q{F.u, F.v, F.w};
+// Sources of the nine strain-rate arrays diu1..9 read by les.f95: computed
+// on the fly from u,v,w (the fused step), or the caller's arrays held in
+// box layout (the les per-routine entry, which receives diu as input).
+struct DiuOnFly {
+    Geo g;
+    UVW q;
+    __device__ __forceinline__ float d1(int i, int j, int k) const { return diu1_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d2(int i, int j, int k) const { return diu2_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d3(int i, int j, int k) const { return diu3_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d4(int i, int j, int k) const { return diu4_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d5(int i, int j, int k) const { return diu5_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d6(int i, int j, int k) const { return diu6_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d7(int i, int j, int k) const { return diu7_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d8(int i, int j, int k) const { return diu8_e(g, q, i, j, k); }
+    __device__ __forceinline__ float d9(int i, int j, int k) const { return diu9_e(g, q, i, j, k); }
+};
+struct DiuBoxes {
+    Geo g;
+    const float *a[9];
+    __device__ __forceinline__ float at(int n, int i, int j, int k) const { return __ldg(&a[n][IX(g, i, j, k)]); }
+    __device__ __forceinline__ float d1(int i, int j, int k) const { return at(0, i, j, k); }
+    __device__ __forceinline__ float d2(int i, int j, int k) const { return at(1, i, j, k); }
+    __device__ __forceinline__ float d3(int i, int j, int k) const { return at(2, i, j, k); }
+    __device__ __forceinline__ float d4(int i, int j, int k) const { return at(3, i, j, k); }
+    __device__ __forceinline__ float d5(int i, int j, int k) const { return at(4, i, j, k); }
+    __device__ __forceinline__ float d6(int i, int j, int k) const { return at(5, i, j, k); }
+    __device__ __forceinline__ float d7(int i, int j, int k) const { return at(6, i, j, k); }
+    __device__ __forceinline__ float d8(int i, int j, int k) const { return at(7, i, j, k); }
+    __device__ __forceinline__ float d9(int i, int j, int k) const { return at(8, i, j, k); }
+};
+
+// velFG.f95:58-105 for one cell: f and g always, h when k <= km-1.  The
+// dfu1/dfv1/dfw1 terms are returned too.
+__device__ __forceinline__ void velfg_cell(const Geo &g, const UVW &q, int i, int j, int k, float &fv, float &gv,
+                                           float &hv, float &dfu1, float &dfv1, float &dfw1) {
     const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn, *dzs = g.dzs;
-    const int c = IX(g, i, j, k);
-    float fv, gv, hv;
     {  // --u velocity, velFG.f95:59-72
         float covx1 = (dx1[i + 1] * cov1_e(g, q, i, j, k) + dx1[i] * cov1_e(g, q, i + 1, j, k)) /
                       (dx1[i] + dx1[i + 1]);
         float covy1 = (cov2_e(g, q, i, j, k) + cov2_e(g, q, i, j + 1, k)) / 2.0f;
         float covz1 = (cov3_e(g, q, i, j, k) + cov3_e(g, q, i, j, k + 1)) / 2.0f;
         float covc = covx1 + covy1 + covz1;
-        float dfu1 = 2.0f * (-diu1_e(g, q, i, j, k) + diu1_e(g, q, i + 1, j, k)) / (dx1[i] + dx1[i + 1]) +
-                     (-diu2_e(g, q, i, j, k) + diu2_e(g, q, i, j + 1, k)) / dy1[j] +
-                     (-diu3_e(g, q, i, j, k) + diu3_e(g, q, i, j, k + 1)) / dzn[k];
+        dfu1 = 2.0f * (-diu1_e(g, q, i, j, k) + diu1_e(g, q, i + 1, j, k)) / (dx1[i] + dx1[i + 1]) +
+               (-diu2_e(g, q, i, j, k) + diu2_e(g, q, i, j + 1, k)) / dy1[j] +
+               (-diu3_e(g, q, i, j, k) + diu3_e(g, q, i, j, k + 1)) / dzn[k];
         float df = g.vn * dfu1;
         fv = (-covc + df);
     }
@@ -171,9 +197,9 @@ __global__ void __launch_bounds__(128) k_velfg_feedbf_sm(Geo g, Fields F) {
                       (dy1[j] + dy1[j + 1]);
         float covz1 = (cov6_e(g, q, i, j, k) + cov6_e(g, q, i, j, k + 1)) / 2.0f;
         float covc = covx1 + covy1 + covz1;
-        float dfv1 = (-diu4_e(g, q, i, j, k) + diu4_e(g, q, i + 1, j, k)) / dx1[i] +
-                     2.0f * (-diu5_e(g, q, i, j, k) + diu5_e(g, q, i, j + 1, k)) / (dy1[j] + dy1[j + 1]) +
-                     (-diu6_e(g, q, i, j, k) + diu6_e(g, q, i, j, k + 1)) / dzn[k];
+        dfv1 = (-diu4_e(g, q, i, j, k) + diu4_e(g, q, i + 1, j, k)) / dx1[i] +
+               2.0f * (-diu5_e(g, q, i, j, k) + diu5_e(g, q, i, j + 1, k)) / (dy1[j] + dy1[j + 1]) +
+               (-diu6_e(g, q, i, j, k) + diu6_e(g, q, i, j, k + 1)) / dzn[k];
         float df = g.vn * dfv1;
         gv = (-covc + df);
     }
@@ -183,59 +209,131 @@ __global__ void __launch_bounds__(128) k_velfg_feedbf_sm(Geo g, Fields F) {
         float covz1 = (dzn[k + 1] * cov9_e(g, q, i, j, k) + dzn[k] * cov9_e(g, q, i, j, k + 1)) /
                       (dzn[k] + dzn[k + 1]);
         float covc = covx1 + covy1 + covz1;
-        float dfw1 = (-diu7_e(g, q, i, j, k) + diu7_e(g, q, i + 1, j, k)) / dx1[i] +
-                     (-diu8_e(g, q, i, j, k) + diu8_e(g, q, i, j + 1, k)) / dy1[j] +
-                     (-diu9_e(g, q, i, j, k) + diu9_e(g, q, i, j, k + 1)) / dzs[k];
+        dfw1 = (-diu7_e(g, q, i, j, k) + diu7_e(g, q, i + 1, j, k)) / dx1[i] +
+               (-diu8_e(g, q, i, j, k) + diu8_e(g, q, i, j + 1, k)) / dy1[j] +
+               (-diu9_e(g, q, i, j, k) + diu9_e(g, q, i, j, k + 1)) / dzs[k];
         float df = g.vn * dfw1;
         hv = (-covc + df);
-    } else {
-        hv = F.h[c];
     }
-    {  // feedbf.f95:38-66
-        const float uc = __ldg(&F.u[c]), vc = __ldg(&F.v[c]), wc = __ldg(&F.w[c]);
-        const float bm = F.bmask[c], cm = F.cmask[c], dm = F.dmask[c];
-        const float us = (F.usum[c] + uc) * bm;
-        const float vs = (F.vsum[c] + vc) * cm;
-        const float ws = (F.wsum[c] + wc) * dm;
-        F.usum[c] = us;
-        F.vsum[c] = vs;
-        F.wsum[c] = ws;
-        float f1x = g.alpha * us * g.dt, f1y = g.alpha * vs * g.dt, f1z = g.alpha * ws * g.dt;
-        float f2x = g.beta * uc * bm, f2y = g.beta * vc * cm, f2z = g.beta * wc * dm;
-        F.f[c] = fv + (f1x + f2x);
-        F.g[c] = gv + (f1y + f2y);
-        F.h[c] = hv + (f1z + f2z);
+}
+
+// les.f95:132-150 sgs eddy viscosity at one interior cell.
+template <class D>
+__device__ __forceinline__ float sgs_sm(const Geo &g, const D &d, int i, int j, int k) {
+    float dudxx1 = d.d1(i, j, k);
+    float dudyx1 = (d.d2(i - 1, j, k) + d.d2(i - 1, j + 1, k) + d.d2(i, j, k) + d.d2(i, j + 1, k)) * 0.25f;
+    float dudzx1 = (d.d3(i - 1, j, k) + d.d3(i - 1, j, k + 1) + d.d3(i, j, k) + d.d3(i, j, k + 1)) * 0.25f;
+    float dvdxx1 = (d.d4(i, j, k) + d.d4(i, j - 1, k) + d.d4(i + 1, j, k) + d.d4(i + 1, j - 1, k)) * 0.25f;
+    float dvdyx1 = d.d5(i, j, k);
+    float dvdzx1 = (d.d6(i, j - 1, k) + d.d6(i, j - 1, k + 1) + d.d6(i, j, k) + d.d6(i, j, k + 1)) * 0.25f;
+    float dwdxx1 = (d.d7(i, j, k) + d.d7(i, j, k - 1) + d.d7(i + 1, j, k) + d.d7(i + 1, j, k - 1)) * 0.25f;
+    float dwdyx1 = (d.d8(i, j, k) + d.d8(i, j, k - 1) + d.d8(i, j + 1, k) + d.d8(i, j + 1, k - 1)) * 0.25f;
+    float dwdzx1 = d.d9(i, j, k);
+    float a = dudyx1 + dvdxx1, b = dwdyx1 + dvdzx1, cc = dudzx1 + dwdxx1;
+    return g.smc[k] * sqrtf(2.0f * (dudxx1 * dudxx1 + dvdyx1 * dvdyx1 + dwdzx1 * dwdzx1) + a * a + b * b + cc * cc);
+}
+
+// les.f95:170-274 viscous flux divergence at one interior cell.
+template <class D>
+__device__ __forceinline__ void visc_cell(const Geo &g, const D &d, const float *__restrict__ sm, int i, int j, int k,
+                                          float &vfu, float &vfv, float &vfw) {
+    const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn;
+#define SM(a, b, c) __ldg(&sm[IX(g, (a), (b), (c))])
+    {  // x-comp, les.f95:170-201
+        float evsx2 = SM(i + 1, j, k);
+        float evsx1 = SM(i, j, k);
+        float evsy2 = fdiv((dy1[j + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dy1[j] * (fdiv((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsy1 = fdiv((dy1[j + 1] * (fdiv((dx1[i + 1] * SM(i, j - 1, k) + dx1[i] * SM(i + 1, j - 1, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dy1[j] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsz2 = (dzn[k + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
+                      (dzn[k] + dzn[k + 1]);
+        float evsz1 = (dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k - 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
+                      (dzn[k - 1] + dzn[k]);
+        float visux2 = (evsx2) * 2.0f * d.d1(i + 1, j, k);
+        float visux1 = (evsx1) * 2.0f * d.d1(i, j, k);
+        float visuy2 = (evsy2) * (d.d2(i, j + 1, k) + d.d4(i + 1, j, k));
+        float visuy1 = (evsy1) * (d.d2(i, j, k) + d.d4(i + 1, j - 1, k));
+        float visuz2 = (evsz2) * (d.d3(i, j, k + 1) + d.d7(i + 1, j, k));
+        float visuz1 = (evsz1) * (d.d3(i, j, k) + d.d7(i + 1, j, k - 1));
+        vfu = fdiv(visux2 - visux1, dx1[i], g.rdx1[i]) + fdiv(visuy2 - visuy1, dy1[j], g.rdy1[j]) + (visuz2 - visuz1) / dzn[k];
     }
-    {  // les.f95:132-152 sgs eddy viscosity
-        float dudxx1 = diu1_e(g, q, i, j, k);
-        float dudyx1 = (diu2_e(g, q, i - 1, j, k) + diu2_e(g, q, i - 1, j + 1, k) + diu2_e(g, q, i, j, k) +
-                        diu2_e(g, q, i, j + 1, k)) * 0.25f;
-        float dudzx1 = (diu3_e(g, q, i - 1, j, k) + diu3_e(g, q, i - 1, j, k + 1) + diu3_e(g, q, i, j, k) +
-                        diu3_e(g, q, i, j, k + 1)) * 0.25f;
-        float dvdxx1 = (diu4_e(g, q, i, j, k) + diu4_e(g, q, i, j - 1, k) + diu4_e(g, q, i + 1, j, k) +
-                        diu4_e(g, q, i + 1, j - 1, k)) * 0.25f;
-        float dvdyx1 = diu5_e(g, q, i, j, k);
-        float dvdzx1 = (diu6_e(g, q, i, j - 1, k) + diu6_e(g, q, i, j - 1, k + 1) + diu6_e(g, q, i, j, k) +
-                        diu6_e(g, q, i, j, k + 1)) * 0.25f;
-        float dwdxx1 = (diu7_e(g, q, i, j, k) + diu7_e(g, q, i, j, k - 1) + diu7_e(g, q, i + 1, j, k) +
-                        diu7_e(g, q, i + 1, j, k - 1)) * 0.25f;
-        float dwdyx1 = (diu8_e(g, q, i, j, k) + diu8_e(g, q, i, j, k - 1) + diu8_e(g, q, i, j + 1, k) +
-                        diu8_e(g, q, i, j + 1, k - 1)) * 0.25f;
-        float dwdzx1 = diu9_e(g, q, i, j, k);
-        float a = dudyx1 + dvdxx1, b = dwdyx1 + dvdzx1, cc = dudzx1 + dwdxx1;
-        F.sm[c] = g.smc[k] * sqrtf(2.0f * (dudxx1 * dudxx1 + dvdyx1 * dvdyx1 + dwdzx1 * dwdzx1) + a * a +
-                                   b * b + cc * cc);
+    {  // y-comp, les.f95:204-235
+        float evsy2 = SM(i, j + 1, k);
+        float evsy1 = SM(i, j, k);
+        float evsx2 = fdiv((dy1[j + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dy1[j] * (fdiv((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsx1 = fdiv((dy1[j + 1] * (fdiv((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1])) +
+                       dy1[j] * (fdiv((dx1[i] * SM(i - 1, j + 1, k) + dx1[i - 1] * SM(i, j + 1, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsz2 = (dzn[k + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
+                      (dzn[k] + dzn[k + 1]);
+        float evsz1 = (dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k - 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
+                      (dzn[k - 1] + dzn[k]);
+        float visvx2 = (evsx2) * (d.d2(i, j + 1, k) + d.d4(i + 1, j, k));
+        float visvx1 = (evsx1) * (d.d2(i - 1, j + 1, k) + d.d4(i, j, k));
+        float visvy2 = (evsy2) * 2.0f * d.d5(i, j + 1, k);
+        float visvy1 = (evsy1) * 2.0f * d.d5(i, j, k);
+        float visvz2 = (evsz2) * (d.d6(i, j, k + 1) + d.d8(i, j + 1, k));
+        float visvz1 = (evsz1) * (d.d6(i, j, k) + d.d8(i, j + 1, k - 1));
+        vfv = fdiv(visvx2 - visvx1, dx1[i], g.rdx1[i]) + fdiv(visvy2 - visvy1, dy1[j], g.rdy1[j]) + (visvz2 - visvz1) / dzn[k];
     }
+    {  // z-comp, les.f95:238-272
+        float evsz2 = SM(i, j, k + 1);
+        float evsz1 = SM(i, j, k);
+        float evsx2 = (dzn[k + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
+                      (dzn[k] + dzn[k + 1]);
+        float evsx1 = (dzn[k + 1] * (fdiv((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1])) +
+                       dzn[k] * (fdiv((dx1[i] * SM(i - 1, j, k + 1) + dx1[i - 1] * SM(i, j, k + 1)), dx1[i - 1] + dx1[i], g.rsx[i - 1]))) /
+                      (dzn[k] + dzn[k + 1]);
+        float evsy2 = (dzn[k + 1] * (fdiv((dy1[j + 1] * SM(i, j, k) + dy1[j] * SM(i, j + 1, k)), dy1[j] + dy1[j + 1], g.rsy[j])) +
+                       dzn[k] * (fdiv((dy1[j + 1] * SM(i, j, k + 1) + dy1[j] * SM(i, j + 1, k + 1)), dy1[j] + dy1[j + 1], g.rsy[j]))) /
+                      (dzn[k] + dzn[k + 1]);
+        float evsy1 = (dzn[k + 1] * (fdiv((dy1[j] * SM(i, j - 1, k) + dy1[j - 1] * SM(i, j, k)), dy1[j - 1] + dy1[j], g.rsy[j - 1])) +
+                       dzn[k] * (fdiv((dy1[j] * SM(i, j - 1, k + 1) + dy1[j - 1] * SM(i, j, k + 1)), dy1[j - 1] + dy1[j], g.rsy[j - 1]))) /
+                      (dzn[k] + dzn[k + 1]);
+        float viswx2 = (evsx2) * (d.d3(i, j, k + 1) + d.d7(i + 1, j, k));
+        float viswx1 = (evsx1) * (d.d3(i - 1, j, k + 1) + d.d7(i, j, k));
+        float viswy2 = (evsy2) * (d.d6(i, j, k + 1) + d.d8(i, j + 1, k));
+        float viswy1 = (evsy1) * (d.d6(i, j - 1, k + 1) + d.d8(i, j, k));
+        float viswz2 = (evsz2) * 2.0f * d.d9(i, j, k + 1);
+        float viswz1 = (evsz1) * 2.0f * d.d9(i, j, k);
+        vfw = fdiv(viswx2 - viswx1, dx1[i], g.rdx1[i]) + fdiv(viswy2 - viswy1, dy1[j], g.rdy1[j]) + (viswz2 - viswz1) / dzn[k];
+    }
+#undef SM
+}
+
+// feedbf.f95:38-66 for one cell: updates usum/vsum/wsum, returns fx,fy,fz.
+__device__ __forceinline__ void feedbf_cell(const Geo &g, Fields &F, int c, float uc, float vc, float wc, float &fx,
+                                            float &fy, float &fz) {
+    const float bm = F.bmask[c], cm = F.cmask[c], dm = F.dmask[c];
+    const float us = (F.usum[c] + uc) * bm;
+    const float vs = (F.vsum[c] + vc) * cm;
+    const float ws = (F.wsum[c] + wc) * dm;
+    F.usum[c] = us;
+    F.vsum[c] = vs;
+    F.wsum[c] = ws;
+    float f1x = g.alpha * us * g.dt, f1y = g.alpha * vs * g.dt, f1z = g.alpha * ws * g.dt;
+    float f2x = g.beta * uc * bm, f2y = g.beta * vc * cm, f2z = g.beta * wc * dm;
+    fx = f1x + f2x;
+    fy = f1y + f2y;
+    fz = f1z + f2z;
 }
 
 // boundsm.f95:13-32 as final values: ghost (i,j,k) = sign * sm(ci, cj, ck)
 // with ci/cj/ck clamping 0->1 and im+1->im (jm, km alike) and sign -1 on
 // the k=0 plane.  The j=-1 row keeps the values only the i-copy reaches.
+// Every source is an interior cell or a j=-1 cell, neither of which this
+// kernel writes.
 __global__ void __launch_bounds__(256) k_boundsm(Geo g, float *__restrict__ sm) {
     const int im = g.im, jm = g.jm, km = g.km;
     const int nI = 2 * (jm + 3) * (km + 2);  // i = 0, im+1 ; j=-1..jm+1 ; k=0..km+1
     const int nJ = 2 * im * (km + 2);        // j = 0, jm+1 ; i=1..im ; k=0..km+1
-    const int nK = 2 * im * (jm + 1);        // k = 0, km+1 ; i=1..im ; j=-1..jm+1 minus j=0,jm+1
+    const int nK = 2 * im * (jm + 1);        // k = 0, km+1 ; i=1..im ; j=-1 and 1..jm
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     if (t < nI) {
@@ -262,105 +360,6 @@ __global__ void __launch_bounds__(256) k_boundsm(Geo g, float *__restrict__ sm) 
     const int ck = k < 1 ? 1 : (k > km ? km : k);
     const float s = sm[IX(g, ci, cj, ck)];
     sm[IX(g, i, j, k)] = (k == 0) ? -s : s;
-}
-
-// les.f95:170-274 viscous terms, fused with adam.f95:32-46 (ADAM=true).
-template <bool ADAM>
-__global__ void __launch_bounds__(128) k_visc(Geo g, Fields F) {
-    const int i = 1 + blockIdx.x * 32 + threadIdx.x;
-    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = 1 + blockIdx.z;
-    if (i > g.im || j > g.jm) return;
-    const UVW q{F.u, F.v, F.w};
-    const float *__restrict__ sm = F.sm;
-    const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn;
-#define SM(a, b, c) __ldg(&sm[IX(g, (a), (b), (c))])
-    const int c = IX(g, i, j, k);
-    float vfu, vfv, vfw;
-    {  // x-comp, les.f95:170-201
-        float evsx2 = SM(i + 1, j, k);
-        float evsx1 = SM(i, j, k);
-        float evsy2 = (dy1[j + 1] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1])) +
-                       dy1[j] * ((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)) / (dx1[i] + dx1[i + 1]))) /
-                      (dy1[j] + dy1[j + 1]);
-        float evsy1 = (dy1[j + 1] * ((dx1[i + 1] * SM(i, j - 1, k) + dx1[i] * SM(i + 1, j - 1, k)) / (dx1[i] + dx1[i + 1])) +
-                       dy1[j] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1]))) /
-                      (dy1[j] + dy1[j + 1]);
-        float evsz2 = (dzn[k + 1] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1])) +
-                       dzn[k] * ((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)) / (dx1[i] + dx1[i + 1]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsz1 = (dzn[k] * ((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)) / (dx1[i] + dx1[i + 1])) +
-                       dzn[k - 1] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1]))) /
-                      (dzn[k - 1] + dzn[k]);
-        float visux2 = (evsx2) * 2.0f * diu1_e(g, q, i + 1, j, k);
-        float visux1 = (evsx1) * 2.0f * diu1_e(g, q, i, j, k);
-        float visuy2 = (evsy2) * (diu2_e(g, q, i, j + 1, k) + diu4_e(g, q, i + 1, j, k));
-        float visuy1 = (evsy1) * (diu2_e(g, q, i, j, k) + diu4_e(g, q, i + 1, j - 1, k));
-        float visuz2 = (evsz2) * (diu3_e(g, q, i, j, k + 1) + diu7_e(g, q, i + 1, j, k));
-        float visuz1 = (evsz1) * (diu3_e(g, q, i, j, k) + diu7_e(g, q, i + 1, j, k - 1));
-        vfu = (visux2 - visux1) / dx1[i] + (visuy2 - visuy1) / dy1[j] + (visuz2 - visuz1) / dzn[k];
-    }
-    {  // y-comp, les.f95:204-235
-        float evsy2 = SM(i, j + 1, k);
-        float evsy1 = SM(i, j, k);
-        float evsx2 = (dy1[j + 1] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1])) +
-                       dy1[j] * ((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)) / (dx1[i] + dx1[i + 1]))) /
-                      (dy1[j] + dy1[j + 1]);
-        float evsx1 = (dy1[j + 1] * ((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)) / (dx1[i - 1] + dx1[i])) +
-                       dy1[j] * ((dx1[i] * SM(i - 1, j + 1, k) + dx1[i - 1] * SM(i, j + 1, k)) / (dx1[i - 1] + dx1[i]))) /
-                      (dy1[j] + dy1[j + 1]);
-        float evsz2 = (dzn[k + 1] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1])) +
-                       dzn[k] * ((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)) / (dx1[i] + dx1[i + 1]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsz1 = (dzn[k] * ((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)) / (dx1[i] + dx1[i + 1])) +
-                       dzn[k - 1] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1]))) /
-                      (dzn[k - 1] + dzn[k]);
-        float visvx2 = (evsx2) * (diu2_e(g, q, i, j + 1, k) + diu4_e(g, q, i + 1, j, k));
-        float visvx1 = (evsx1) * (diu2_e(g, q, i - 1, j + 1, k) + diu4_e(g, q, i, j, k));
-        float visvy2 = (evsy2) * 2.0f * diu5_e(g, q, i, j + 1, k);
-        float visvy1 = (evsy1) * 2.0f * diu5_e(g, q, i, j, k);
-        float visvz2 = (evsz2) * (diu6_e(g, q, i, j, k + 1) + diu8_e(g, q, i, j + 1, k));
-        float visvz1 = (evsz1) * (diu6_e(g, q, i, j, k) + diu8_e(g, q, i, j + 1, k - 1));
-        vfv = (visvx2 - visvx1) / dx1[i] + (visvy2 - visvy1) / dy1[j] + (visvz2 - visvz1) / dzn[k];
-    }
-    {  // z-comp, les.f95:238-272
-        float evsz2 = SM(i, j, k + 1);
-        float evsz1 = SM(i, j, k);
-        float evsx2 = (dzn[k + 1] * ((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)) / (dx1[i] + dx1[i + 1])) +
-                       dzn[k] * ((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)) / (dx1[i] + dx1[i + 1]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsx1 = (dzn[k + 1] * ((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)) / (dx1[i - 1] + dx1[i])) +
-                       dzn[k] * ((dx1[i] * SM(i - 1, j, k + 1) + dx1[i - 1] * SM(i, j, k + 1)) / (dx1[i - 1] + dx1[i]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsy2 = (dzn[k + 1] * ((dy1[j + 1] * SM(i, j, k) + dy1[j] * SM(i, j + 1, k)) / (dy1[j] + dy1[j + 1])) +
-                       dzn[k] * ((dy1[j + 1] * SM(i, j, k + 1) + dy1[j] * SM(i, j + 1, k + 1)) / (dy1[j] + dy1[j + 1]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsy1 = (dzn[k + 1] * ((dy1[j] * SM(i, j - 1, k) + dy1[j - 1] * SM(i, j, k)) / (dy1[j - 1] + dy1[j])) +
-                       dzn[k] * ((dy1[j] * SM(i, j - 1, k + 1) + dy1[j - 1] * SM(i, j, k + 1)) / (dy1[j - 1] + dy1[j]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float viswx2 = (evsx2) * (diu3_e(g, q, i, j, k + 1) + diu7_e(g, q, i + 1, j, k));
-        float viswx1 = (evsx1) * (diu3_e(g, q, i - 1, j, k + 1) + diu7_e(g, q, i, j, k));
-        float viswy2 = (evsy2) * (diu6_e(g, q, i, j, k + 1) + diu8_e(g, q, i, j + 1, k));
-        float viswy1 = (evsy1) * (diu6_e(g, q, i, j - 1, k + 1) + diu8_e(g, q, i, j, k));
-        float viswz2 = (evsz2) * 2.0f * diu9_e(g, q, i, j, k + 1);
-        float viswz1 = (evsz1) * 2.0f * diu9_e(g, q, i, j, k);
-        vfw = (viswx2 - viswx1) / dx1[i] + (viswy2 - viswy1) / dy1[j] + (viswz2 - viswz1) / dzn[k];
-    }
-#undef SM
-    const float fv = F.f[c] + vfu, gv = F.g[c] + vfv, hv = F.h[c] + vfw;
-    if (ADAM) {  // adam.f95:32-46: fold = f before the update
-        const int o = c;
-        F.f[c] = 1.5f * fv - 0.5f * F.fold[o];
-        F.g[c] = 1.5f * gv - 0.5f * F.gold[o];
-        F.h[c] = 1.5f * hv - 0.5f * F.hold[o];
-        F.fold[o] = fv;
-        F.gold[o] = gv;
-        F.hold[o] = hv;
-    } else {
-        F.f[c] = fv;
-        F.g[c] = gv;
-        F.h[c] = hv;
-    }
 }
 
 // ifdata.f95:117-125 zero_arrays for f,g,h on (0:ip,0:jp,0:kp).

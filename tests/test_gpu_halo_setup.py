@@ -66,8 +66,9 @@ def test_reference_kats_through_gpu(require_gpu):
     im, jm, km, hw, vd = p["im"], p["jm"], p["km"], p["h_w"], p["v_dim"]
     arr = np.arange(vd * im * jm * km, dtype=np.float32)
     buf = np.full(abi.lib().les_halo_buffer_floats(im, jm, km, hw, vd, 1), -1.0, np.float32)
-    abi.check(abi.lib().les_halo_pack_inner(_soa_to_aos(arr, vd).ctypes.data, buf.ctypes.data, im,
-                                            jm, km, hw, vd, 0, None))
+    aos = _soa_to_aos(arr, vd)  # named: a temporary could be freed before the call reads it
+    abi.check(abi.lib().les_halo_pack_inner(aos.ctypes.data, buf.ctypes.data, im, jm, km, hw, vd,
+                                            0, None))
     printed = np.array(KAT["test_halo_read_correct"]["printed"], np.float32)
     np.testing.assert_array_equal(buf, printed[arr.size:])
     for prog, fn in (("test_halo_write", "les_halo_unpack"),

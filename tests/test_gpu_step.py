@@ -91,3 +91,93 @@ def test_multi_step_call_and_metrics(require_gpu):
     P = ref.a("p")[FL.index("p", ip, jp, kp, ip // 2, jp // 2, kp // 2)]
     assert m["p_centre"] == P
     gpu.close()
+
+
+@pytest.mark.parametrize("pjuge", [2.0e4, 6.0e3, 2.0e3, 7.0e2])
+def test_sor_stops_midway_through_a_pass(require_gpu, pjuge):
+    # thresholds chosen so the SOR stops at different iteration counts,
+    # odd ones included (the multi-iteration pass is then redone)
+    ip, jp, kp = 20, 16, 10
+    ref, dev = _pair(ip, jp, kp, seed=4)
+    for c in (ref, dev):
+        c.params.pjuge = pjuge
+        c.params.nmaxp = 25
+    gpu = GpuLes(dev)
+    oracle.ifdata(ref, 1)
+    gpu.warmup(1)
+    seen = []
+    for n in range(1, 4):
+        iters = oracle.run_steps(ref, n, 1)
+        gpu.step(n, 1)
+        assert gpu.metrics()["sor_iters"] == iters[0]
+        seen.append(iters[0])
+        _compare(gpu, ref)
+    gpu.close()
+
+
+def test_multi_iteration_passes_equal_per_colour_sweeps(require_gpu):
+    from les_halo_b200 import abi
+    ip, jp, kp = 150, 150, 90
+    ref, a = _pair(ip, jp, kp, seed=1)
+    b = a.copy()
+    g1, g2 = GpuLes(a), GpuLes(b)
+    abi.check(abi.lib().les_ctx_set_sor_path(g2.ctx, 1))
+    oracle.ifdata(ref, 1)
+    for g in (g1, g2):
+        g.warmup(1)
+        g.step(1, 2)
+    oracle.run_steps(ref, 1, 2)
+    d1, d2 = g1.download(ALL), g2.download(ALL)
+    assert_bitexact(d1, d2, ip, jp, kp, ALL)
+    _compare(g1, ref)
+    g1.close()
+    g2.close()
+
+
+def test_upload_with_inconsistent_p_ghosts(require_gpu):
+    # p ghosts that boundp1/boundp2 would not produce: the first SOR
+    # iteration must read them as given (per-colour path), as the reference does
+    ip, jp, kp = 24, 20, 12
+    ref, dev = _pair(ip, jp, kp, seed=6)
+    oracle.ifdata(ref, 1)
+    oracle.run_steps(ref, 1, 1)
+    rng = np.random.default_rng(0)
+    p = ref.a("p")
+    p[FL.index("p", ip, jp, kp, 0, slice(1, jp), slice(1, kp))] = rng.standard_normal((jp, kp))
+    for n in FL.STATE:
+        dev.arrays[n] = ref.a(n).copy(order="F")
+    gpu = GpuLes(dev)
+    oracle.run_steps(ref, 2, 2)
+    gpu.step(2, 2)
+    _compare(gpu, ref)
+    gpu.close()
+
+
+@pytest.mark.parametrize("tile", ["1,8", "1,44", "2,20", "3,12", "3,24"])
+def test_each_sor_tile_equals_per_colour_sweeps(require_gpu, monkeypatch, tile):
+    # every (iterations per pass, tile rows) the autotuner may pick, on a grid
+    # with several tiles in i and j (130 / (64 - 4T) and 96 / rows)
+    from les_halo_b200 import abi
+    ip, jp, kp = 130, 96, 40
+    _, a = _pair(ip, jp, kp, seed=2)
+    b = a.copy()
+    monkeypatch.setenv("LES_SOR_TILE", tile)
+    g1, g2 = GpuLes(a), GpuLes(b)
+    abi.check(abi.lib().les_ctx_set_sor_path(g2.ctx, 1))
+    for g in (g1, g2):
+        g.warmup(1)
+        g.step(1, 3)
+    T, ty = _sor_tile(g1)
+    assert (T, ty) == tuple(int(x) for x in tile.split(","))
+    assert_bitexact(g1.download(ALL), g2.download(ALL), ip, jp, kp, ALL)
+    assert g1.metrics()["sor_iters"] == g2.metrics()["sor_iters"]
+    g1.close()
+    g2.close()
+
+
+def _sor_tile(gpu):
+    import ctypes as C
+    from les_halo_b200 import abi
+    T, ty = C.c_int(), C.c_int()
+    abi.check(abi.lib().les_ctx_sor_tile(gpu.ctx, C.byref(T), C.byref(ty)))
+    return T.value, ty.value
