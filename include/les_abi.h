@@ -277,6 +277,21 @@ les_status les_boundp1_(const int *km, const int *jm, float *p, const int *im);
 /* boundp.f95:18 */
 les_status les_boundp2_(const int *jm, const int *im, float *p, const int *km);
 
+/* ---- press.f95:49-81 without allocating (no counterpart in the reference) --
+ * bondfg, rhs, rhsav and rhs -= rhsav, as les_press_ computes them, on
+ * arrays the caller already holds on the device (same Fortran layouts and
+ * argument order as les_press_; scalars by value), enqueued on `stream`
+ * (a cudaStream_t or NULL); rhsav (a device float, may be NULL) receives
+ * the average.  Allocates no device memory: the per-block partial sums sit
+ * in a 256 KiB static __device__ array, so ceil(im/32) * ceil(jm/8) must be
+ * at most 5456 (e.g. im = jm = 1024 needs 4096); larger grids are rejected
+ * with LES_ERR_DIMS before any device work.  The first call on each device
+ * looks up the scratch address; make it outside any stream capture.  Calls
+ * that overlap in time on one device share the scratch and race. */
+les_status les_press_rhs_noalloc(int km, int jm, int im, float *rhs, const float *u,
+                                 const float *dx1, const float *v, const float *dy1,
+                                 const float *w, const float *dzn, float *f, float *g, float *h,
+                                 float dt, float *rhsav, void *stream);
 
 #ifdef __cplusplus
 }

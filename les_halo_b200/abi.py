@@ -101,6 +101,7 @@ _SIGS = {
     "les_synth_grid": (C.c_int, [C.POINTER(LesSynthCfg)] + [_P] * 9),
     "les_synth_terrain": (C.c_float, [C.POINTER(LesSynthCfg), _P]),
     "les_synth_inflow": (C.c_int, [C.POINTER(LesSynthCfg), _P, _P, _P]),
+    "les_press_rhs_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int] + [_P] * 10 + [C.c_float, _P, _P]),
 }
 
 # Per-routine entries: every argument is a pointer (Fortran by-reference).
