@@ -46,7 +46,8 @@ struct Scal {
     unsigned int uout_pos;  // max of positive u(im,j,k) as float bits
     unsigned int uout_neg;  // max of -u(im,j,k) for negative u, float bits
     float uout, rhsav, pav, sor;
-    int sor_iters, converged, n, pad;
+    int sor_iters, converged, n;
+    unsigned int ticket;  // blocks of the running SOR pass that have finished (0 between launches)
     int pbuf;  // SOR result buffer: 0 = p, 1 = the second p buffer
     int redo;  // iterations to redo after a pass that converged part-way
     float probe[4];

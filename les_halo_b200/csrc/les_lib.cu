@@ -136,6 +136,12 @@ TableLayout table_layout(int ip, int jp, int kp) {
 
 }  // namespace
 
+// Shape of a temporal-blocked SOR pass: iterations per pass, tile rows,
+// region rows per warp, k chunks.
+struct TbShape {
+    int T = 0, ty = 0, rpw = 1, nch = 1;
+};
+
 struct les_ctx {
     les_params prm{};
     Geo geo{};
@@ -172,8 +178,7 @@ struct les_ctx {
     const float *cn1_box = nullptr;  // caller's cn1 (per-routine press only)
     // temporal-blocked SOR (les_sor_tb.cuh)
     float *d_p2 = nullptr;           // second p buffer
-    int tb_T = 0, tb_ty = 0, tb_gx = 0, tb_gy = 0;  // tile chosen by the autotuner
-    size_t tb_smem = 0;
+    TbShape tb;  // SOR pass shape chosen by the autotuner (tb.T == 0: not yet)
     bool cn1_by_k = false;           // uniform dx, dy: cn1 from a per-k table
     bool p_ghosts_ok = false;        // p's ghosts hold what boundp1/boundp2 give
     bool force_exact_sor = false;    // testing: always the per-colour path
@@ -182,7 +187,7 @@ struct les_ctx {
 namespace {
 
 float *field_ptr(les_ctx *c, int f) { return c->d_fields + (size_t)f * c->box_elems; }
-les_status launch_sor_tb(les_ctx *c, int T, int ty, bool cn1k, int niter, int mode);
+les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, bool tuning = false);
 
 // Host copies of the 1-D tables -> device; builds cnA/B/C, smc, wind.
 // Tables not given stay zero (the per-routine entries pass only theirs).
@@ -381,16 +386,14 @@ les_status enqueue_press(les_ctx *c, bool exact) {
             LAUNCH(c, k_final_sor, dim3(1), dim3(1024), c->d_part, 2 * np, c->prm.pjuge, c->d_scal);
         }
     } else {
-        const int nblk = c->tb_gx * c->tb_gy;
         for (int done = 0, pass = 0; done < c->prm.nmaxp; ++pass) {
-            const int nit = std::min(c->tb_T, c->prm.nmaxp - done);
+            const int nit = std::min(c->tb.T, c->prm.nmaxp - done);
             if (pass == 0) MARK(c, EV_SOR1_START);
-            les_status st = launch_sor_tb(c, c->tb_T, c->tb_ty, c->cn1_by_k, nit, 0);
+            les_status st = launch_sor_tb(c, c->tb, nit, 0, c->prm.pjuge);
             if (st != LES_OK) return st;
             if (pass == 0) MARK(c, EV_SOR1_END);
-            LAUNCH(c, k_final_tb, dim3(1), dim3(1024), c->d_part, nblk, nit, c->prm.pjuge, c->d_scal);
-            if ((st = launch_sor_tb(c, c->tb_T, c->tb_ty, c->cn1_by_k, nit, 1)) != LES_OK) return st;
-            LAUNCH(c, k_finish_redo, dim3(1), dim3(1), c->d_scal);
+            // a pass of one iteration cannot stop part-way: no redo launch
+            if (nit > 1 && (st = launch_sor_tb(c, c->tb, nit, 1, c->prm.pjuge)) != LES_OK) return st;
             done += nit;
         }
     }
@@ -432,126 +435,169 @@ les_status check_params(const les_params *p) {
     return LES_OK;
 }
 
-// Launch one temporal-blocked SOR pass (T iterations per pass, tile rows ty).
-les_status launch_sor_tb(les_ctx *c, int T, int ty, bool cn1k, int niter, int mode) {
-    const dim3 grid(cdiv(c->prm.ip, tb_tx(T)), cdiv(c->prm.jp, ty));
-    const size_t sm = tb_smem(T, ty);
-    const float *tab = c->geo.cnC ? c->d_tables + c->tl.cn1k : nullptr;
+// Launch one temporal-blocked SOR pass (mode 0) or its redo (mode 1).
+// tuning: read and write only the second p buffer (scratch between steps),
+// so timing passes leave the model state alone.
+les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, bool tuning) {
+    const int kc = cdiv(c->prm.kp, sh.nch);
+    const dim3 grid(cdiv(c->prm.ip, tb_tx(sh.T)), cdiv(c->prm.jp, sh.ty), cdiv(c->prm.kp, kc));
+    const dim3 block(32 * tb_warps(sh.T, sh.ty, sh.rpw));
+    const size_t sm = tb_smem(sh.T, sh.ty);
+    TbArgs a;
+    a.pb0 = tuning ? c->d_p2 : c->F.p;
+    a.pb1 = c->d_p2;
+    a.rhs = c->F.rhs;
+    a.cn1k = c->d_tables + c->tl.cn1k;
+    a.ty = sh.ty;
+    a.kc = kc;
+    a.niter = niter;
+    a.mode = mode;
+    a.pjuge = pjuge;
+    a.part = c->d_part;
+    a.sc = c->d_scal;
     const Geo &g = c->geo;
-#define TBL(TT, KT)                                                                                      \
-    LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, dim3(kTbNT), sm, g, c->F.p, c->d_p2, c->F.rhs, tab, ty, niter, \
-                mode, c->d_part, c->d_scal)
-    switch (T * 2 + (cn1k ? 1 : 0)) {
-        case 2: TBL(1, false); break;
-        case 3: TBL(1, true); break;
-        case 4: TBL(2, false); break;
-        case 5: TBL(2, true); break;
-        case 6: TBL(3, false); break;
-        case 7: TBL(3, true); break;
-        default: return fail(LES_ERR_BAD_ARG, "SOR pass depth %d", T);
+#define TBL(TT, KT, RP) LAUNCH_SMEM(c, (k_sor_tb<TT, KT, RP>), grid, block, sm, g, a)
+    switch ((sh.T * 2 + (c->cn1_by_k ? 1 : 0)) * 2 + (sh.rpw - 1)) {
+        case 4: TBL(1, false, 1); break;
+        case 5: TBL(1, false, 2); break;
+        case 6: TBL(1, true, 1); break;
+        case 7: TBL(1, true, 2); break;
+        case 8: TBL(2, false, 1); break;
+        case 9: TBL(2, false, 2); break;
+        case 10: TBL(2, true, 1); break;
+        case 11: TBL(2, true, 2); break;
+        case 12: TBL(3, false, 1); break;
+        case 13: TBL(3, false, 2); break;
+        case 14: TBL(3, true, 1); break;
+        case 15: TBL(3, true, 2); break;
+        default: return fail(LES_ERR_BAD_ARG, "SOR pass shape %d,%d,%d", sh.T, sh.ty, sh.rpw);
     }
 #undef TBL
     return LES_OK;
 }
 
+// Largest dynamic shared memory of each pass kernel: the opt-in limit minus
+// the kernel's static buffers.
+int g_tb_dyn_max = 0;
 les_status set_tb_smem_attrs() {
-    // dynamic shared memory allowed on top of the kernel's static buffers
     int dev = 0, optin = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const int mx = optin - 1024;
-#define TBA(TT, KT)                                                                                  \
-    CK(cudaFuncSetAttribute(k_sor_tb<TT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    TBA(1, false) TBA(1, true) TBA(2, false) TBA(2, true) TBA(3, false) TBA(3, true)
+    int lim = optin;
+#define TBA(TT, KT, RP)                                                                            \
+    {                                                                                              \
+        cudaFuncAttributes fa;                                                                     \
+        CK(cudaFuncGetAttributes(&fa, k_sor_tb<TT, KT, RP>));                                      \
+        const int mx = optin - (int)fa.sharedSizeBytes;                                            \
+        CK(cudaFuncSetAttribute(k_sor_tb<TT, KT, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+        lim = std::min(lim, mx);                                                                   \
+    }
+    TBA(1, false, 1) TBA(1, false, 2) TBA(1, true, 1) TBA(1, true, 2)
+    TBA(2, false, 1) TBA(2, false, 2) TBA(2, true, 1) TBA(2, true, 2)
+    TBA(3, false, 1) TBA(3, false, 2) TBA(3, true, 1) TBA(3, true, 2)
 #undef TBA
+    g_tb_dyn_max = lim;
     return LES_OK;
 }
 
-// Process-wide cache of autotuned SOR tiles: (ip, jp, kp, SMs) -> (T, ty).
+// Process-wide cache of autotuned SOR pass shapes: (ip, jp, kp, SMs) -> shape.
 struct TuneKey {
     int ip, jp, kp, nsm;
     bool operator<(const TuneKey &o) const {
         return std::tie(ip, jp, kp, nsm) < std::tie(o.ip, o.jp, o.kp, o.nsm);
     }
 };
-std::map<TuneKey, std::pair<int, int>> g_tune;
+std::map<TuneKey, TbShape> g_tune;
 std::mutex g_tune_mu;
 
-// Autotuner: time each candidate (T, ty) on this context's buffers with CUDA
-// events (two passes after one warm-up pass) and keep the fastest time per
-// SOR iteration.  Runs once per grid shape and device; LES_SOR_TILE=T,ty
-// overrides it.  Results persist in the file named by LES_TUNE_CACHE.
+// A shape this context can launch: it fits the kernel limits, the shared
+// memory and the partial-sum array.
+bool tb_shape_ok(const les_ctx *c, const TbShape &sh) {
+    if (!tb_fits(sh.T, sh.ty, sh.rpw) || sh.nch < 1 || sh.nch > kTbMaxChunks) return false;
+    if (tb_smem(sh.T, sh.ty) > (size_t)g_tb_dyn_max) return false;
+    const int kc = cdiv(c->prm.kp, sh.nch);
+    const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(sh.T)) * cdiv(c->prm.jp, sh.ty) * cdiv(c->prm.kp, kc);
+    return nblk * kTbTMax <= c->npart;
+}
+
+// Autotuner: time each candidate shape on this context's rhs and scratch p
+// buffer with CUDA events (two passes after one warm-up pass, the stop test
+// disabled; the passes run in place, so the values are meaningless) and
+// keep the fastest time per SOR iteration.  Runs once per grid and device;
+// LES_SOR_TILE=T,ty[,rows per warp[,k chunks]] overrides it.  Results persist
+// in the file named by LES_TUNE_CACHE.
 les_status autotune_sor(les_ctx *c) {
     int dev = 0, nsm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const TuneKey key{c->prm.ip, c->prm.jp, c->prm.kp, nsm};
-    int bestT = 0, bestTy = 0;
+    TbShape best;
     if (const char *ov = std::getenv("LES_SOR_TILE")) {
-        std::sscanf(ov, "%d,%d", &bestT, &bestTy);
+        std::sscanf(ov, "%d,%d,%d,%d", &best.T, &best.ty, &best.rpw, &best.nch);
     } else {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(key);
-        if (it != g_tune.end()) {
-            bestT = it->second.first;
-            bestTy = it->second.second;
-        }
+        if (it != g_tune.end()) best = it->second;
     }
     const char *cache = std::getenv("LES_TUNE_CACHE");
-    if (!bestT && cache) {
+    if (!best.T && cache) {
         if (FILE *fp = std::fopen(cache, "r")) {
-            int a, b, cc, d, t, y;
-            while (std::fscanf(fp, "%d %d %d %d %d %d", &a, &b, &cc, &d, &t, &y) == 6)
-                if (a == key.ip && b == key.jp && cc == key.kp && d == key.nsm) bestT = t, bestTy = y;
+            int a, b, cc, d;
+            TbShape sh;
+            while (std::fscanf(fp, "%d %d %d %d %d %d %d %d", &a, &b, &cc, &d, &sh.T, &sh.ty, &sh.rpw, &sh.nch) == 8)
+                if (a == key.ip && b == key.jp && cc == key.kp && d == key.nsm) best = sh;
             std::fclose(fp);
         }
     }
-    if (!bestT) {
+    if (!best.T) {
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
-        double best = 0.0;
-        const int tys[] = {8, 12, 16, 20, 24, 28, 32, 40, 48, 56};
+        double best_t = 0.0;
+        const int rh1[] = {8, 12, 16, 20, 24, 28, 32}, rh2[] = {8, 12, 16, 20, 24, 28, 32};
         for (int T = 1; T <= kTbTMax; ++T)
-            for (int ty : tys) {
-                if (!tb_fits(T, ty) || tb_smem(T, ty) > 226 * 1024) continue;
-                const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(T)) * cdiv(c->prm.jp, ty);
-                if (nblk * kTbTMax > c->npart) continue;
-                CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
-                les_status st = launch_sor_tb(c, T, ty, c->cn1_by_k, T, 0);
-                if (st != LES_OK) return st;
-                CK(cudaEventRecord(e0, c->stream));
-                for (int r = 0; r < 2; ++r)
-                    if ((st = launch_sor_tb(c, T, ty, c->cn1_by_k, T, 0)) != LES_OK) return st;
-                CK(cudaEventRecord(e1, c->stream));
-                CK(cudaEventSynchronize(e1));
-                float ms = 0.0f;
-                CK(cudaEventElapsedTime(&ms, e0, e1));
-                const double per_iter = ms / (2.0 * T);
-                if (!bestT || per_iter < best) best = per_iter, bestT = T, bestTy = ty;
-            }
+            for (int rpw = 1; rpw <= 2; ++rpw)
+                for (int ri = 0; ri < 7; ++ri)
+                    for (int nch = 1; nch <= 4; nch *= 2) {
+                        TbShape sh;
+                        sh.T = T;
+                        sh.rpw = rpw;
+                        sh.ty = (rpw == 1 ? rh1[ri] : rh2[ri]) - 2 * tb_ring(T);
+                        sh.nch = nch;
+                        if (sh.ty < 4 || (nch > 1 && cdiv(c->prm.kp, nch) < 8) || !tb_shape_ok(c, sh)) continue;
+                        CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
+                        les_status st = launch_sor_tb(c, sh, T, 0, -1.0f, true);
+                        if (st != LES_OK) return st;
+                        CK(cudaEventRecord(e0, c->stream));
+                        for (int r = 0; r < 2; ++r)
+                            if ((st = launch_sor_tb(c, sh, T, 0, -1.0f, true)) != LES_OK) return st;
+                        CK(cudaEventRecord(e1, c->stream));
+                        CK(cudaEventSynchronize(e1));
+                        float ms = 0.0f;
+                        CK(cudaEventElapsedTime(&ms, e0, e1));
+                        const double per_iter = ms / (2.0 * T);
+                        if (!best.T || per_iter < best_t) best_t = per_iter, best = sh;
+                    }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        if (!bestT) return fail(LES_ERR_DIMS, "no SOR tile shape fits");
+        if (!best.T) return fail(LES_ERR_DIMS, "no SOR pass shape fits");
         if (cache)
             if (FILE *fp = std::fopen(cache, "a")) {
-                std::fprintf(fp, "%d %d %d %d %d %d\n", key.ip, key.jp, key.kp, key.nsm, bestT, bestTy);
+                std::fprintf(fp, "%d %d %d %d %d %d %d %d\n", key.ip, key.jp, key.kp, key.nsm, best.T, best.ty,
+                             best.rpw, best.nch);
                 std::fclose(fp);
             }
     }
+    if (!tb_shape_ok(c, best))
+        return fail(LES_ERR_BAD_ARG, "SOR pass shape %d,%d,%d,%d out of range", best.T, best.ty, best.rpw,
+                    best.nch);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tune[key] = {bestT, bestTy};
+        g_tune[key] = best;
     }
-    if (bestT < 1 || bestT > kTbTMax || !tb_fits(bestT, bestTy) || tb_smem(bestT, bestTy) > 226 * 1024)
-        return fail(LES_ERR_BAD_ARG, "SOR tile %d,%d out of range", bestT, bestTy);
-    c->tb_T = bestT;
-    c->tb_ty = bestTy;
-    c->tb_smem = tb_smem(bestT, bestTy);
-    c->tb_gx = cdiv(c->prm.ip, tb_tx(bestT));
-    c->tb_gy = cdiv(c->prm.jp, bestTy);
+    c->tb = best;
     return LES_OK;
 }
 
@@ -669,7 +715,8 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
             cudaFuncSetAttribute(k_mom2<false, false>, A, ms) != cudaSuccess)
             return cleanup(fail(LES_ERR_CUDA, "shared memory attribute"));
     }
-    c->npart = std::max(c->npart, kTbTMax * cdiv(ip, tb_tx(kTbTMax)) * cdiv(jp, 8));
+    // the largest SOR pass grid: narrowest tiles, 4-row tiles, most k chunks
+    c->npart = std::max(c->npart, kTbTMax * cdiv(ip, tb_tx(kTbTMax)) * cdiv(jp, 4) * kTbMaxChunks);
     if (cudaMalloc(&c->d_part, sizeof(FixPart) * c->npart) != cudaSuccess)
         return cleanup(fail(LES_ERR_NOMEM, "partials"));
     if (cudaMalloc(&c->d_p2, sizeof(float) * c->box_elems) != cudaSuccess)
@@ -845,15 +892,25 @@ les_status les_ctx_warmup(les_ctx *c, int n) {
 
 les_status les_ctx_sor_tile(les_ctx *c, int *T, int *ty) {
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
-    if (T) *T = c->tb_T;
-    if (ty) *ty = c->tb_ty;
+    if (T) *T = c->tb.T;
+    if (ty) *ty = c->tb.ty;
+    return ok();
+}
+
+les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *rpw, int *nch) {
+    if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    if (T) *T = c->tb.T;
+    if (ty) *ty = c->tb.ty;
+    if (tx) *tx = c->tb.T ? tb_tx(c->tb.T) : 0;
+    if (rpw) *rpw = c->tb.rpw;
+    if (nch) *nch = c->tb.nch;
     return ok();
 }
 
 float les_ctx_sor_iters_per_launch(les_ctx *c) {
     if (!c) return 0.0f;
     const bool exact = c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok;
-    return exact ? 0.5f : (float)(c->tb_T ? c->tb_T : 2);
+    return exact ? 0.5f : (float)(c->tb.T ? c->tb.T : 2);
 }
 
 les_status les_ctx_set_sor_path(les_ctx *c, int exact) {
@@ -878,7 +935,7 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
         const int n = n0 + s;
         const bool exact = c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok;
         const int gi = ((n == 1 && c->prm.ical == 0) ? 1 : 0) + (exact ? 2 : 0);
-        if (!exact && c->tb_T == 0) {
+        if (!exact && c->tb.T == 0) {
             les_status st = autotune_sor(c);
             if (st != LES_OK) return st;
         }

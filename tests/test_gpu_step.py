@@ -93,10 +93,12 @@ def test_multi_step_call_and_metrics(require_gpu):
     gpu.close()
 
 
+@pytest.mark.parametrize("shape", ["3,8,1,1", "2,8,2,2"])
 @pytest.mark.parametrize("pjuge", [2.0e4, 6.0e3, 2.0e3, 7.0e2])
-def test_sor_stops_midway_through_a_pass(require_gpu, pjuge):
-    # thresholds chosen so the SOR stops at different iteration counts,
-    # odd ones included (the multi-iteration pass is then redone)
+def test_sor_stops_midway_through_a_pass(require_gpu, monkeypatch, pjuge, shape):
+    # thresholds chosen so the SOR stops at different iteration counts, also
+    # part-way through a pass of 2 or 3 iterations (which is then redone)
+    monkeypatch.setenv("LES_SOR_TILE", shape)
     ip, jp, kp = 20, 16, 10
     ref, dev = _pair(ip, jp, kp, seed=4)
     for c in (ref, dev):
@@ -153,31 +155,32 @@ def test_upload_with_inconsistent_p_ghosts(require_gpu):
     gpu.close()
 
 
-@pytest.mark.parametrize("tile", ["1,8", "1,44", "2,20", "3,12", "3,24"])
-def test_each_sor_tile_equals_per_colour_sweeps(require_gpu, monkeypatch, tile):
-    # every (iterations per pass, tile rows) the autotuner may pick, on a grid
-    # with several tiles in i and j (130 / (64 - 4T) and 96 / rows)
+@pytest.mark.parametrize("shape", ["1,8,1,1", "1,28,1,2", "1,12,2,4", "2,20,1,1", "2,8,2,3",
+                                   "3,12,1,2", "3,20,2,1"])
+def test_each_sor_pass_shape_equals_per_colour_sweeps(require_gpu, monkeypatch, shape):
+    # shapes (iterations per pass, tile rows, rows per warp, k chunks) the
+    # autotuner may pick, on a grid with several tiles in i, j and k
     from les_halo_b200 import abi
     ip, jp, kp = 130, 96, 40
     _, a = _pair(ip, jp, kp, seed=2)
     b = a.copy()
-    monkeypatch.setenv("LES_SOR_TILE", tile)
+    monkeypatch.setenv("LES_SOR_TILE", shape)
     g1, g2 = GpuLes(a), GpuLes(b)
     abi.check(abi.lib().les_ctx_set_sor_path(g2.ctx, 1))
     for g in (g1, g2):
         g.warmup(1)
         g.step(1, 3)
-    T, ty = _sor_tile(g1)
-    assert (T, ty) == tuple(int(x) for x in tile.split(","))
+    T, ty, _, rpw, nch = _sor_shape(g1)
+    assert (T, ty, rpw, nch) == tuple(int(x) for x in shape.split(","))
     assert_bitexact(g1.download(ALL), g2.download(ALL), ip, jp, kp, ALL)
     assert g1.metrics()["sor_iters"] == g2.metrics()["sor_iters"]
     g1.close()
     g2.close()
 
 
-def _sor_tile(gpu):
+def _sor_shape(gpu):
     import ctypes as C
     from les_halo_b200 import abi
-    T, ty = C.c_int(), C.c_int()
-    abi.check(abi.lib().les_ctx_sor_tile(gpu.ctx, C.byref(T), C.byref(ty)))
-    return T.value, ty.value
+    v = [C.c_int() for _ in range(5)]
+    abi.check(abi.lib().les_ctx_sor_shape(gpu.ctx, *[C.byref(x) for x in v]))
+    return tuple(x.value for x in v)
