@@ -278,9 +278,9 @@ def run_ours(args):
     sor_launch_ms = float(np.mean(phases[:, 5])) if not args.profile else float("nan")
     peak, peak_kind = _peaks()
     ipl = float(L.les_ctx_sor_iters_per_launch(gpu.ctx))
-    sh = [C.c_int() for _ in range(5)]
+    sh = [C.c_int() for _ in range(4)]
     abi.check(L.les_ctx_sor_shape(gpu.ctx, *[C.byref(x) for x in sh]))
-    tT, tY, tX, tR, tK = (x.value for x in sh)
+    tT, tY, tX, tK = (x.value for x in sh)
     achieved = SOR_BYTES_PER_CELL_PER_ITER * ipl * cells / (sor_launch_ms / 1e3) / 1e9
     step_gbs = STEP_BYTES_PER_CELL * cells / (ms_step / 1e3) / 1e9
     traffic = None
@@ -300,8 +300,7 @@ def run_ours(args):
                                    "heights <=120 m, dt=0.05, SOR 50 sweeps/step)",
                        "grid": [case.ip, case.jp, case.kp], "sor_iters": int(m["sor_iters"]),
                        "parallelism": f"replicas x{ws}",
-                       "sor_tile": {"iters_per_pass": tT, "rows": tY, "cols": tX, "rows_per_warp": tR,
-                                    "k_chunks": tK},
+                       "sor_tile": {"iters_per_pass": tT, "rows": tY, "cols": tX, "k_chunks": tK},
                        "l2": "inputs larger than L2 (19 state fields, 3.5 GB)"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "k_sor_tb" if ipl > 1 else "k_sor_colour",

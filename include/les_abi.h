@@ -149,9 +149,9 @@ float les_ctx_sor_iters_per_launch(les_ctx *ctx);
 /* Iterations per pass and tile rows the autotuner chose for the
  * multi-iteration SOR (0, 0 before the first step that uses it). */
 les_status les_ctx_sor_tile(les_ctx *ctx, int *iters_per_pass, int *tile_rows);
-/* The full pass shape: tile columns, region rows per warp and k chunks too. */
+/* The full pass shape: tile columns and k chunks too. */
 les_status les_ctx_sor_shape(les_ctx *ctx, int *iters_per_pass, int *tile_rows, int *tile_cols,
-                             int *rows_per_warp, int *k_chunks);
+                             int *k_chunks);
 les_status les_ctx_phase_times(les_ctx *ctx, int slot, float *ms, int n);
 
 /* Device state access for callers that keep fields on the GPU.  The field

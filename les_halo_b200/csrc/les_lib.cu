@@ -137,9 +137,9 @@ TableLayout table_layout(int ip, int jp, int kp) {
 }  // namespace
 
 // Shape of a temporal-blocked SOR pass: iterations per pass, tile rows,
-// region rows per warp, k chunks.
+// k chunks.
 struct TbShape {
-    int T = 0, ty = 0, rpw = 1, nch = 1;
+    int T = 0, ty = 0, nch = 1;
 };
 
 struct les_ctx {
@@ -441,7 +441,7 @@ les_status check_params(const les_params *p) {
 les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, bool tuning) {
     const int kc = cdiv(c->prm.kp, sh.nch);
     const dim3 grid(cdiv(c->prm.ip, tb_tx(sh.T)), cdiv(c->prm.jp, sh.ty), cdiv(c->prm.kp, kc));
-    const dim3 block(32 * tb_warps(sh.T, sh.ty, sh.rpw));
+    const dim3 block(32 * tb_warps(sh.T, sh.ty));
     const size_t sm = tb_smem(sh.T, sh.ty);
     TbArgs a;
     a.pb0 = tuning ? c->d_p2 : c->F.p;
@@ -456,21 +456,15 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     a.part = c->d_part;
     a.sc = c->d_scal;
     const Geo &g = c->geo;
-#define TBL(TT, KT, RP) LAUNCH_SMEM(c, (k_sor_tb<TT, KT, RP>), grid, block, sm, g, a)
-    switch ((sh.T * 2 + (c->cn1_by_k ? 1 : 0)) * 2 + (sh.rpw - 1)) {
-        case 4: TBL(1, false, 1); break;
-        case 5: TBL(1, false, 2); break;
-        case 6: TBL(1, true, 1); break;
-        case 7: TBL(1, true, 2); break;
-        case 8: TBL(2, false, 1); break;
-        case 9: TBL(2, false, 2); break;
-        case 10: TBL(2, true, 1); break;
-        case 11: TBL(2, true, 2); break;
-        case 12: TBL(3, false, 1); break;
-        case 13: TBL(3, false, 2); break;
-        case 14: TBL(3, true, 1); break;
-        case 15: TBL(3, true, 2); break;
-        default: return fail(LES_ERR_BAD_ARG, "SOR pass shape %d,%d,%d", sh.T, sh.ty, sh.rpw);
+#define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a)
+    switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
+        case 2: TBL(1, false); break;
+        case 3: TBL(1, true); break;
+        case 4: TBL(2, false); break;
+        case 5: TBL(2, true); break;
+        case 6: TBL(3, false); break;
+        case 7: TBL(3, true); break;
+        default: return fail(LES_ERR_BAD_ARG, "SOR pass shape %d,%d", sh.T, sh.ty);
     }
 #undef TBL
     return LES_OK;
@@ -484,17 +478,15 @@ les_status set_tb_smem_attrs() {
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     int lim = optin;
-#define TBA(TT, KT, RP)                                                                            \
+#define TBA(TT, KT)                                                                                \
     {                                                                                              \
         cudaFuncAttributes fa;                                                                     \
-        CK(cudaFuncGetAttributes(&fa, k_sor_tb<TT, KT, RP>));                                      \
+        CK(cudaFuncGetAttributes(&fa, k_sor_tb<TT, KT>));                                          \
         const int mx = optin - (int)fa.sharedSizeBytes;                                            \
-        CK(cudaFuncSetAttribute(k_sor_tb<TT, KT, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+        CK(cudaFuncSetAttribute(k_sor_tb<TT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
         lim = std::min(lim, mx);                                                                   \
     }
-    TBA(1, false, 1) TBA(1, false, 2) TBA(1, true, 1) TBA(1, true, 2)
-    TBA(2, false, 1) TBA(2, false, 2) TBA(2, true, 1) TBA(2, true, 2)
-    TBA(3, false, 1) TBA(3, false, 2) TBA(3, true, 1) TBA(3, true, 2)
+    TBA(1, false) TBA(1, true) TBA(2, false) TBA(2, true) TBA(3, false) TBA(3, true)
 #undef TBA
     g_tb_dyn_max = lim;
     return LES_OK;
@@ -513,7 +505,7 @@ std::mutex g_tune_mu;
 // A shape this context can launch: it fits the kernel limits, the shared
 // memory and the partial-sum array.
 bool tb_shape_ok(const les_ctx *c, const TbShape &sh) {
-    if (!tb_fits(sh.T, sh.ty, sh.rpw) || sh.nch < 1 || sh.nch > kTbMaxChunks) return false;
+    if (!tb_fits(sh.T, sh.ty) || sh.nch < 1 || sh.nch > kTbMaxChunks) return false;
     if (tb_smem(sh.T, sh.ty) > (size_t)g_tb_dyn_max) return false;
     const int kc = cdiv(c->prm.kp, sh.nch);
     const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(sh.T)) * cdiv(c->prm.jp, sh.ty) * cdiv(c->prm.kp, kc);
@@ -524,7 +516,7 @@ bool tb_shape_ok(const les_ctx *c, const TbShape &sh) {
 // buffer with CUDA events (two passes after one warm-up pass, the stop test
 // disabled; the passes run in place, so the values are meaningless) and
 // keep the fastest time per SOR iteration.  Runs once per grid and device;
-// LES_SOR_TILE=T,ty[,rows per warp[,k chunks]] overrides it.  Results persist
+// LES_SOR_TILE=T,ty[,k chunks] overrides it.  Results persist
 // in the file named by LES_TUNE_CACHE.
 les_status autotune_sor(les_ctx *c) {
     int dev = 0, nsm = 0;
@@ -533,7 +525,7 @@ les_status autotune_sor(les_ctx *c) {
     const TuneKey key{c->prm.ip, c->prm.jp, c->prm.kp, nsm};
     TbShape best;
     if (const char *ov = std::getenv("LES_SOR_TILE")) {
-        std::sscanf(ov, "%d,%d,%d,%d", &best.T, &best.ty, &best.rpw, &best.nch);
+        std::sscanf(ov, "%d,%d,%d", &best.T, &best.ty, &best.nch);
     } else {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(key);
@@ -544,7 +536,7 @@ les_status autotune_sor(les_ctx *c) {
         if (FILE *fp = std::fopen(cache, "r")) {
             int a, b, cc, d;
             TbShape sh;
-            while (std::fscanf(fp, "%d %d %d %d %d %d %d %d", &a, &b, &cc, &d, &sh.T, &sh.ty, &sh.rpw, &sh.nch) == 8)
+            while (std::fscanf(fp, "%d %d %d %d %d %d %d", &a, &b, &cc, &d, &sh.T, &sh.ty, &sh.nch) == 7)
                 if (a == key.ip && b == key.jp && cc == key.kp && d == key.nsm) best = sh;
             std::fclose(fp);
         }
@@ -554,15 +546,13 @@ les_status autotune_sor(les_ctx *c) {
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         double best_t = 0.0;
-        const int rh1[] = {8, 12, 16, 20, 24, 28, 32}, rh2[] = {8, 12, 16, 20, 24, 28, 32};
+        const int rhs_[] = {8, 12, 16, 20, 24, 28, 32};
         for (int T = 1; T <= kTbTMax; ++T)
-            for (int rpw = 1; rpw <= 2; ++rpw)
-                for (int ri = 0; ri < 7; ++ri)
-                    for (int nch = 1; nch <= 4; nch *= 2) {
+            for (int ri = 0; ri < 7; ++ri)
+                for (int nch = 1; nch <= 4; nch *= 2) {
                         TbShape sh;
                         sh.T = T;
-                        sh.rpw = rpw;
-                        sh.ty = (rpw == 1 ? rh1[ri] : rh2[ri]) - 2 * tb_ring(T);
+                        sh.ty = rhs_[ri] - 2 * tb_ring(T);
                         sh.nch = nch;
                         if (sh.ty < 4 || (nch > 1 && cdiv(c->prm.kp, nch) < 8) || !tb_shape_ok(c, sh)) continue;
                         CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
@@ -585,14 +575,13 @@ les_status autotune_sor(les_ctx *c) {
         if (!best.T) return fail(LES_ERR_DIMS, "no SOR pass shape fits");
         if (cache)
             if (FILE *fp = std::fopen(cache, "a")) {
-                std::fprintf(fp, "%d %d %d %d %d %d %d %d\n", key.ip, key.jp, key.kp, key.nsm, best.T, best.ty,
-                             best.rpw, best.nch);
+                std::fprintf(fp, "%d %d %d %d %d %d %d\n", key.ip, key.jp, key.kp, key.nsm, best.T, best.ty,
+                             best.nch);
                 std::fclose(fp);
             }
     }
     if (!tb_shape_ok(c, best))
-        return fail(LES_ERR_BAD_ARG, "SOR pass shape %d,%d,%d,%d out of range", best.T, best.ty, best.rpw,
-                    best.nch);
+        return fail(LES_ERR_BAD_ARG, "SOR pass shape %d,%d,%d out of range", best.T, best.ty, best.nch);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune[key] = best;
@@ -897,12 +886,11 @@ les_status les_ctx_sor_tile(les_ctx *c, int *T, int *ty) {
     return ok();
 }
 
-les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *rpw, int *nch) {
+les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *nch) {
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     if (T) *T = c->tb.T;
     if (ty) *ty = c->tb.ty;
     if (tx) *tx = c->tb.T ? tb_tx(c->tb.T) : 0;
-    if (rpw) *rpw = c->tb.rpw;
     if (nch) *nch = c->tb.nch;
     return ok();
 }

@@ -11,19 +11,20 @@
 // the interior with i/k mirror and j periodic neighbours, and a CTA can run
 // several half-sweeps per pass (a skewed wavefront along k, temporal
 // blocking):
-//   - a CTA owns a (64 - 4T) x ty tile of (i,j) columns, a chunk of k, and
+//   - a CTA owns a (128 - 4T) x ty tile of (i,j) columns, a chunk of k, and
 //     a ring of R = 2T cells (and planes) around them; half-sweep s updates
 //     the region shrunk by s+1 on every side, so after 2T half-sweeps the
 //     tile holds exact values;
 //   - planes march upward: at step tau half-sweep s works on plane tau-s,
 //     in order s = 0,1,.., so each plane sees its neighbours at the right
 //     level;
-//   - a warp owns whole region rows (64 columns), lane l the column pair
-//     2l, 2l+1, whose values on the last 2T+2 planes stay in registers: the
-//     k neighbours and the own x neighbour come from registers, the other x
-//     neighbour from the adjacent lane (one shuffle), the j neighbours from
-//     a shared copy of the plane (parity-split rows: x -> (x&1)*32 + x/2, so
-//     a colour's cells and their j neighbours are bank-conflict free);
+//   - a warp owns one region row (128 columns), lane l the columns 4l..4l+3,
+//     whose values on the last 2T+2 planes stay in registers; a half-sweep
+//     updates two of them (one colour), taking the k neighbours and three
+//     of the four x neighbours from registers, the fourth from the adjacent
+//     lane (one shuffle), and the j neighbours from a shared copy of the
+//     plane (rows stored as x -> (x%4)*32 + x/4, so these reads are
+//     bank-conflict free);
 //   - within a step every half-sweep works on its own plane and reads only
 //     the other colour, written in earlier steps: one barrier per step;
 //   - planes are staged with cp.async kTbDepth steps ahead of their use;
@@ -35,32 +36,36 @@
 // redone from its input buffer with exactly the iterations the reference
 // executes.
 #pragma once
+#include <type_traits>
+
 #include "les_dev.cuh"
 
 namespace les {
 namespace {  // kernels get internal linkage: each .cu has its own copy
 
-constexpr int kTbRW = 64;     // region row: 64 columns, lane l owns 2l and 2l+1
-constexpr int kTbTMax = 3;    // iterations per pass
-constexpr int kTbDepth = 2;   // planes requested ahead of the one a step needs
-constexpr int kTbMaxRH = 64;  // region rows
+constexpr int kTbCW = 4;              // columns per lane
+constexpr int kTbRW = 32 * kTbCW;     // region row: 128 columns
+constexpr int kTbTMax = 3;            // iterations per pass
+constexpr int kTbDepth = 2;           // planes requested ahead of the one a step needs
+constexpr int kTbMaxRH = 32;          // region rows, one warp each
 constexpr int kTbMaxChunks = 8;
 
 __host__ __device__ constexpr int tb_ring(int T) { return 2 * T; }
-// tile columns: the 64-column region minus a ring on each side
+// tile columns: the region minus a ring on each side
 __host__ __device__ constexpr int tb_tx(int T) { return kTbRW - 2 * tb_ring(T); }
 // shared plane slots (p and rhs each): 2T planes in work, the incoming one,
 // kTbDepth in flight and one of slack so a request never hits a plane a
 // slower warp may still read
 __host__ __device__ constexpr int tb_ns(int T) { return 2 * T + 2 + kTbDepth; }
 __host__ __device__ inline int tb_rh(int T, int ty) { return ty + 2 * tb_ring(T); }
-__host__ __device__ inline int tb_warps(int T, int ty, int rpw) { return (tb_rh(T, ty) + rpw - 1) / rpw; }
+__host__ __device__ inline int tb_warps(int T, int ty) { return tb_rh(T, ty); }
 __host__ __device__ inline size_t tb_smem(int T, int ty) {
     return sizeof(float) * 2 * (size_t)kTbRW * tb_rh(T, ty) * tb_ns(T);
 }
-__host__ __device__ inline bool tb_fits(int T, int ty, int rpw) {
-    return T >= 1 && T <= kTbTMax && ty >= 1 && (rpw == 1 || rpw == 2) && tb_rh(T, ty) <= kTbMaxRH &&
-           tb_warps(T, ty, rpw) <= (rpw == 1 ? 32 : 16);  // the kernels' launch bounds
+// rows (= warps) within the kernels' launch bounds: 32 for one iteration per
+// pass, 24 for more (their longer register windows need more registers)
+__host__ __device__ inline bool tb_fits(int T, int ty) {
+    return T >= 1 && T <= kTbTMax && ty >= 1 && tb_rh(T, ty) <= (T == 1 ? kTbMaxRH : 24);
 }
 
 struct TbArgs {
@@ -162,157 +167,123 @@ __device__ void tb_finish_pass(const FixPart *part, int nblocks, int nit, float 
 // One pass of niter <= T iterations (mode 0), or the redo of scal->redo
 // iterations after a pass that converged part-way (mode 1).
 // CN1K: cn1 depends on k only (uniform dx and dy), read from cn1k[k].
-// RPW: region rows per warp (blockDim.x = 32 * tb_warps(T, ty, RPW); two
-// rows per warp trade warps for registers, so at most 512 threads).
-template <int T, bool CN1K, int RPW>
-__global__ void __launch_bounds__(RPW == 1 ? 1024 : 512) k_sor_tb(Geo g, TbArgs a) {
+// blockDim.x = 32 * tb_rh(T, ty): warp y owns region row y.
+template <int T, bool CN1K>
+__global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a) {
     extern __shared__ float smem[];
     Scal *sc = a.sc;
     const bool redo = (a.mode == 1);
     if (!redo && sc->converged) return;
     const int nit = redo ? sc->redo : a.niter;
     if (nit <= 0) return;
-    constexpr int R = tb_ring(T), TX = tb_tx(T), NS = tb_ns(T), D = kTbDepth, W = 2 * T + 2;
+    constexpr int R = tb_ring(T), TX = tb_tx(T), NS = tb_ns(T), D = kTbDepth, W = 2 * T + 2, RW = kTbRW;
     const int nhs = 2 * nit;
-    const int ty = a.ty, RH = ty + 2 * R, RA = kTbRW * RH;
+    const int ty = a.ty, RH = ty + 2 * R, RA = RW * RH;
     float *P = smem;          // NS plane slots of p
     float *Bs = P + NS * RA;  // NS plane slots of rhs
     const float *pin = sc->pbuf ? a.pb1 : a.pb0;
     float *pout = sc->pbuf ? a.pb0 : a.pb1;
     const float rhsav = sc->rhsav, omega = g.omega;
     const int im = g.im, jm = g.jm, km = g.km;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, y = threadIdx.x >> 5;  // warp y owns region row y
     const int ir0 = 1 + blockIdx.x * TX - R, jr0 = 1 + blockIdx.y * ty - R;
     const int k0 = 1 + blockIdx.z * a.kc, k1 = min(km, k0 + a.kc - 1);
     const int kb = max(1, k0 - R), ke = min(km, k1 + R);
     const long long pstride = (long long)g.si * g.sj;
-    const int dA = (lane & 1) * 32 + (lane >> 1);  // parity-split slot of column `lane`
 
-    // owned rows: region row, box offset of (ir0, j, k=0), j coefficients
-    int ry[RPW], roff[RPW];
-    bool rok[RPW];
-    float c3l[RPW], c3s[RPW], cB[RPW];
+    const int jw = ((jr0 + y - 1) % jm + jm) % jm + 1;  // periodic j (jm even)
+    const int roff = IX(g, ir0, jw, 0);                 // box offset of (ir0, jw, k=0)
+    const float c3l = g.cn3l[jw], c3s = g.cn3s[jw], cB = CN1K ? 0.0f : g.cnB[jw];
+    const bool ytile = (y >= R && y < R + ty && jr0 + y <= jm);
+    // the lane's columns x = 4l + c
+    float c2l[kTbCW], c2s[kTbCW], cA[kTbCW];
+    int fl[kTbCW];  // bit 0: 1 <= i <= im, 1: i == 1, 2: i == im, 3: x inside the tile
 #pragma unroll
-    for (int r = 0; r < RPW; ++r) {
-        ry[r] = warp + nw * r;
-        rok[r] = ry[r] < RH;
-        const int jw = ((jr0 + ry[r] - 1) % jm + jm) % jm + 1;  // periodic j (jm even)
-        roff[r] = IX(g, ir0, jw, 0);
-        c3l[r] = rok[r] ? g.cn3l[jw] : 0.0f;
-        c3s[r] = rok[r] ? g.cn3s[jw] : 0.0f;
-        cB[r] = (!CN1K && rok[r]) ? g.cnB[jw] : 0.0f;
+    for (int c = 0; c < kTbCW; ++c) {
+        const int x = kTbCW * lane + c, i = ir0 + x;
+        const bool ok = (i >= 1 && i <= im);
+        c2l[c] = ok ? g.cn2l[i] : 0.0f;
+        c2s[c] = ok ? g.cn2s[i] : 0.0f;
+        cA[c] = (!CN1K && ok) ? g.cnA[i] : 0.0f;
+        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0) | ((x >= R && x < R + TX) ? 8 : 0);
     }
-    // the lane's two columns (x = 2l + c)
-    float c2l0, c2l1, c2s0, c2s1, cA0, cA1;
-    int fl0, fl1;  // bit 0: 1 <= i <= im, 1: i == 1, 2: i == im, 3: x inside the tile
-    {
-        auto col = [&](int c, float &cl, float &cs, float &ca, int &fl) {
-            const int x = c + 2 * lane, i = ir0 + x;
-            const bool ok = (i >= 1 && i <= im);
-            cl = ok ? g.cn2l[i] : 0.0f;
-            cs = ok ? g.cn2s[i] : 0.0f;
-            ca = (!CN1K && ok) ? g.cnA[i] : 0.0f;
-            fl = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0) | ((x >= R && x < R + TX) ? 8 : 0);
-        };
-        col(0, c2l0, c2s0, cA0, fl0);
-        col(1, c2l1, c2s1, cA1, fl1);
-    }
-    // register window: w0/w1[r][m] = column 0/1 of owned row r on plane tau+1-m
-    float w0[RPW][W], w1[RPW][W];
+    // register window: w[c][m] = column c on plane tau+1-m
+    float w[kTbCW][W];
 #pragma unroll
-    for (int r = 0; r < RPW; ++r)
+    for (int c = 0; c < kTbCW; ++c)
 #pragma unroll
-        for (int m = 0; m < W; ++m) w0[r][m] = w1[r][m] = 0.0f;
+        for (int m = 0; m < W; ++m) w[c][m] = 0.0f;
     // reltmp^2 sums of iterations 0, 1, 2 of the pass
     unsigned long long h0 = 0, l0 = 0, h1 = 0, l1 = 0, h2 = 0, l2 = 0;
     int bad = 0;
 
-    auto request = [&](int k) {
+    // plane k of this warp's row: lane copies global columns lane + 32*cc
+    // (128-byte coalesced) to their shared positions
+    const int d0 = y * RW + (lane & 3) * 32 + (lane >> 2);
+    auto request = [&](int k, int slot) {
         if (k <= ke) {
-            float *Pp = P + (k % NS) * RA;
-            float *Bp = Bs + (k % NS) * RA;
-            const long long ko = pstride * k;
+            const long long src = roff + pstride * k + lane;
+            float *Pp = P + slot * RA + d0;
+            float *Bp = Bs + slot * RA + d0;
 #pragma unroll
-            for (int r = 0; r < RPW; ++r)
-                if (rok[r]) {
-                    const long long src = roff[r] + ko + lane;
-                    const int d = ry[r] * kTbRW + dA;
-                    tb_cp_async4(Pp + d, pin + src);
-                    tb_cp_async4(Pp + d + 16, pin + src + 32);
-                    tb_cp_async4(Bp + d, a.rhs + src);
-                    tb_cp_async4(Bp + d + 16, a.rhs + src + 32);
-                }
+            for (int cc = 0; cc < kTbCW; ++cc) {
+                tb_cp_async4(Pp + 8 * cc, pin + src + 32 * cc);
+                tb_cp_async4(Bp + 8 * cc, a.rhs + src + 32 * cc);
+            }
         }
         tb_cp_commit();
     };
 
 #pragma unroll
-    for (int k = 0; k < D; ++k) request(kb + k);
+    for (int k = 0; k < D; ++k) request(kb + k, (kb + k) % NS);
+    int st1 = kb % NS;  // slot of plane tau+1
     const int tau_end = k1 + 2 * T - 1;  // plane k1 is stored at this step
     for (int tau = kb - 1; tau <= tau_end; ++tau) {
-        request(tau + 1 + D);
+        request(tau + 1 + D, st1 + D >= NS ? st1 + D - NS : st1 + D);
         tb_cp_wait<D>();  // plane tau+1 has landed (this thread's copies)
         __syncthreads();  // ... and everyone's
-        const float *Pn = P + ((tau + 1) % NS) * RA;
 #pragma unroll
-        for (int r = 0; r < RPW; ++r) {
+        for (int c = 0; c < kTbCW; ++c) {
 #pragma unroll
-            for (int m = W - 1; m > 0; --m) {
-                w0[r][m] = w0[r][m - 1];
-                w1[r][m] = w1[r][m - 1];
-            }
-            if (rok[r] && tau + 1 <= ke) {
-                w0[r][0] = Pn[ry[r] * kTbRW + lane];
-                w1[r][0] = Pn[ry[r] * kTbRW + 32 + lane];
-            }
+            for (int m = W - 1; m > 0; --m) w[c][m] = w[c][m - 1];
+            if (tau + 1 <= ke) w[c][0] = P[st1 * RA + y * RW + c * 32 + lane];
         }
 #pragma unroll
         for (int s = 0; s < 2 * T; ++s) {
             const int q = tau - s;
             const int qlo = (kb == 1) ? 1 : kb + s + 1, qhi = (ke == km) ? km : ke - s - 1;
-            if (s < nhs && q >= qlo && q <= qhi) {
-                const int nrd = s & 1;
-                float *Pq = P + (q % NS) * RA;
-                const float *Bq = Bs + (q % NS) * RA;
+            const int lo = s + 1;
+            if (s < nhs && q >= qlo && q <= qhi && y >= lo && y < RH - lo) {
+                int sq = st1 - 1 - s;
+                if (sq < 0) sq += NS;
+                float *Pq = P + sq * RA;
+                const float *Bq = Bs + sq * RA;
                 const float c4l = g.cn4l[q], c4s = g.cn4s[q];
                 const float cnq = CN1K ? a.cn1k[q] : 0.0f;
                 const float cC = CN1K ? 0.0f : g.cnC[q];
                 const bool top = (q == km), bottom = (q == 1);
-                const int lo = s + 1;
-                const bool qtile = (q >= k0 && q <= k1);
-#pragma unroll
-                for (int r = 0; r < RPW; ++r) {
-                    const int y = ry[r];
-                    if (!rok[r] || y < lo || y >= RH - lo) continue;
-                    const int par = (jr0 + y + q + nrd + 1 - ir0) & 1;  // column of the colour in my pair
-                    // x neighbour held by the adjacent lane: column 1 of lane-1
-                    // (par 0, west) or column 0 of lane+1 (par 1, east)
-                    const float vsh = par ? w0[r][s + 1] : w1[r][s + 1];
-                    const float nb = __shfl_sync(0xffffffffu, vsh, lane + (par ? 1 : -1));
-                    const int x = par + 2 * lane;
-                    const int fl = par ? fl1 : fl0;
-                    if (x < lo || x >= kTbRW - lo || !(fl & 1)) continue;
-                    const float pc = par ? w1[r][s + 1] : w0[r][s + 1];
-                    const float own = par ? w0[r][s + 1] : w1[r][s + 1];
-                    const float pe = (fl & 4) ? pc : (par ? nb : own);
-                    const float pw = (fl & 2) ? pc : (par ? own : nb);
-                    const int o = y * kTbRW + par * 32 + lane;
-                    const float pn = Pq[o + kTbRW];
-                    const float ps = Pq[o - kTbRW];
-                    const float pu = top ? pc : (par ? w1[r][s] : w0[r][s]);
-                    const float pd = bottom ? pc : (par ? w1[r][s + 2] : w0[r][s + 2]);
-                    const float cn1 = CN1K ? cnq : 1.0f / ((par ? cA1 : cA0) + cB[r] + cC);
-                    const float reltmp =
-                        omega * (cn1 * ((par ? c2l1 : c2l0) * pe + (par ? c2s1 : c2s0) * pw + c3l[r] * pn +
-                                        c3s[r] * ps + c4l * pu + c4s * pd - (Bq[o] - rhsav)) -
-                                 pc);
+                const bool acc = !redo && ytile && q >= k0 && q <= k1;
+                // update column C (of this half-sweep's colour) given its x neighbours
+                auto upd = [&](auto Cc, float west, float east) {
+                    constexpr int C = decltype(Cc)::value;
+                    const int x = kTbCW * lane + C;
+                    if (x < lo || x >= RW - lo || !(fl[C] & 1)) return;
+                    const float pc = w[C][s + 1];
+                    const float pe = (fl[C] & 4) ? pc : east;
+                    const float pw = (fl[C] & 2) ? pc : west;
+                    const int o = y * RW + C * 32 + lane;
+                    const float pn = Pq[o + RW];
+                    const float ps = Pq[o - RW];
+                    const float pu = top ? pc : w[C][s];
+                    const float pd = bottom ? pc : w[C][s + 2];
+                    const float cn1 = CN1K ? cnq : 1.0f / (cA[C] + cB + cC);
+                    const float reltmp = omega * (cn1 * (c2l[C] * pe + c2s[C] * pw + c3l * pn + c3s * ps + c4l * pu +
+                                                         c4s * pd - (Bq[o] - rhsav)) -
+                                                  pc);
                     const float nv = pc + reltmp;
                     Pq[o] = nv;
-                    if (par)
-                        w1[r][s + 1] = nv;
-                    else
-                        w0[r][s + 1] = nv;
-                    if (!redo && qtile && (fl & 8) && y >= R && y < R + ty && jr0 + y <= jm) {
+                    w[C][s + 1] = nv;
+                    if (acc && (fl[C] & 8)) {
                         if (s < 2)
                             fix_add_nonneg(reltmp * reltmp, h0, l0, bad);
                         else if (s < 4)
@@ -320,27 +291,37 @@ __global__ void __launch_bounds__(RPW == 1 ? 1024 : 512) k_sor_tb(Geo g, TbArgs 
                         else
                             fix_add_nonneg(reltmp * reltmp, h2, l2, bad);
                     }
+                };
+                // x parity of this colour's cells on the row
+                if (((jr0 + y + q + (s & 1) + 1 - ir0) & 1) == 0) {
+                    // cells 4l, 4l+2; the west neighbour of 4l is column 3 of lane-1
+                    const float nb = __shfl_sync(0xffffffffu, w[3][s + 1], lane - 1);
+                    upd(std::integral_constant<int, 0>(), nb, w[1][s + 1]);
+                    upd(std::integral_constant<int, 2>(), w[1][s + 1], w[3][s + 1]);
+                } else {
+                    // cells 4l+1, 4l+3; the east neighbour of 4l+3 is column 0 of lane+1
+                    const float nb = __shfl_sync(0xffffffffu, w[0][s + 1], lane + 1);
+                    upd(std::integral_constant<int, 1>(), w[0][s + 1], w[2][s + 1]);
+                    upd(std::integral_constant<int, 3>(), w[2][s + 1], nb);
                 }
             }
         }
-        // plane tau+1-2T is final: store the tile part of the owned rows
+        // plane tau+1-2T is final: store the tile part of the row
         const int qs = tau + 1 - 2 * T;
-        if (qs >= k0 && qs <= k1) {
-            const long long ko = pstride * qs;
+        if (ytile && qs >= k0 && qs <= k1) {
+            float *dst = pout + (roff + pstride * qs + kTbCW * lane);
 #pragma unroll
-            for (int r = 0; r < RPW; ++r) {
-                const int y = ry[r];
-                if (!rok[r] || y < R || y >= R + ty || jr0 + y > jm) continue;
-                float *dst = pout + (roff[r] + ko + 2 * lane);
-                const bool s0 = (fl0 & 9) == 9, s1 = (fl1 & 9) == 9;
-                if (s0 && s1)  // (ir0 + 2l) + 31 is even: 8-byte aligned
-                    *reinterpret_cast<float2 *>(dst) = make_float2(w0[r][2 * T], w1[r][2 * T]);
+            for (int h = 0; h < kTbCW; h += 2) {
+                const bool s0 = (fl[h] & 9) == 9, s1 = (fl[h + 1] & 9) == 9;
+                if (s0 && s1)  // (ir0 + 4l + h) + 31 is even: 8-byte aligned
+                    *reinterpret_cast<float2 *>(dst + h) = make_float2(w[h][2 * T], w[h + 1][2 * T]);
                 else if (s0)
-                    dst[0] = w0[r][2 * T];
+                    dst[h] = w[h][2 * T];
                 else if (s1)
-                    dst[1] = w1[r][2 * T];
+                    dst[h + 1] = w[h + 1][2 * T];
             }
         }
+        st1 = (st1 + 1 == NS) ? 0 : st1 + 1;
     }
     tb_cp_wait<0>();  // only empty groups can be left
 
