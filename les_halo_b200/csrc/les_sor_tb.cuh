@@ -51,8 +51,11 @@ constexpr int kTbMaxRH = 32;          // region rows, one warp each
 constexpr int kTbMaxChunks = 8;
 
 __host__ __device__ constexpr int tb_ring(int T) { return 2 * T; }
+// ring in x: 2T rounded up to 4 columns, so every row of the region starts
+// on a 16-byte boundary (whole float4 per lane)
+__host__ __device__ constexpr int tb_ringx(int T) { return (2 * T + 3) / 4 * 4; }
 // tile columns: the region minus a ring on each side
-__host__ __device__ constexpr int tb_tx(int T) { return kTbRW - 2 * tb_ring(T); }
+__host__ __device__ constexpr int tb_tx(int T) { return kTbRW - 2 * tb_ringx(T); }
 // shared plane slots (p and rhs each): 2T planes in work, the incoming one,
 // kTbDepth in flight and one of slack so a request never hits a plane a
 // slower warp may still read
@@ -127,9 +130,9 @@ __device__ __forceinline__ void block_fix_sum_any(i128 v, int bad, FixPart *out)
     }
 }
 
-__device__ __forceinline__ void tb_cp_async4(float *dst, const float *src) {
+__device__ __forceinline__ void tb_cp_async16(float *dst, const float *src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void tb_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -170,29 +173,31 @@ __device__ void tb_finish_pass(const FixPart *part, int nblocks, int nit, float 
 // blockDim.x = 32 * tb_rh(T, ty): warp y owns region row y.
 template <int T, bool CN1K>
 __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a) {
-    extern __shared__ float smem[];
+    extern __shared__ float4 smem4[];
     Scal *sc = a.sc;
     const bool redo = (a.mode == 1);
     if (!redo && sc->converged) return;
     const int nit = redo ? sc->redo : a.niter;
     if (nit <= 0) return;
-    constexpr int R = tb_ring(T), TX = tb_tx(T), NS = tb_ns(T), D = kTbDepth, W = 2 * T + 2, RW = kTbRW;
+    constexpr int R = tb_ring(T), RX = tb_ringx(T), TX = tb_tx(T), NS = tb_ns(T), D = kTbDepth, W = 2 * T + 2;
+    constexpr int RW4 = kTbRW / 4;  // float4 per region row
     const int nhs = 2 * nit;
-    const int ty = a.ty, RH = ty + 2 * R, RA = RW * RH;
-    float *P = smem;          // NS plane slots of p
-    float *Bs = P + NS * RA;  // NS plane slots of rhs
+    const int ty = a.ty, RH = ty + 2 * R, RA4 = RW4 * RH;
+    float4 *P = smem4;          // NS plane slots of p
+    float4 *Bs = P + NS * RA4;  // NS plane slots of rhs
     const float *pin = sc->pbuf ? a.pb1 : a.pb0;
     float *pout = sc->pbuf ? a.pb0 : a.pb1;
     const float rhsav = sc->rhsav, omega = g.omega;
     const int im = g.im, jm = g.jm, km = g.km;
     const int lane = threadIdx.x & 31, y = threadIdx.x >> 5;  // warp y owns region row y
-    const int ir0 = 1 + blockIdx.x * TX - R, jr0 = 1 + blockIdx.y * ty - R;
+    const int ir0 = 1 + blockIdx.x * TX - RX, jr0 = 1 + blockIdx.y * ty - R;
     const int k0 = 1 + blockIdx.z * a.kc, k1 = min(km, k0 + a.kc - 1);
     const int kb = max(1, k0 - R), ke = min(km, k1 + R);
     const long long pstride = (long long)g.si * g.sj;
 
     const int jw = ((jr0 + y - 1) % jm + jm) % jm + 1;  // periodic j (jm even)
-    const int roff = IX(g, ir0, jw, 0);                 // box offset of (ir0, jw, k=0)
+    // box offset of (ir0 + 4*lane, jw, k=0); (ir0 + 31) is a multiple of 4
+    const long long coff = IX(g, ir0, jw, 0) + kTbCW * lane;
     const float c3l = g.cn3l[jw], c3s = g.cn3s[jw], cB = CN1K ? 0.0f : g.cnB[jw];
     const bool ytile = (y >= R && y < R + ty && jr0 + y <= jm);
     // the lane's columns x = 4l + c
@@ -205,8 +210,10 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
         c2l[c] = ok ? g.cn2l[i] : 0.0f;
         c2s[c] = ok ? g.cn2s[i] : 0.0f;
         cA[c] = (!CN1K && ok) ? g.cnA[i] : 0.0f;
-        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0) | ((x >= R && x < R + TX) ? 8 : 0);
+        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0) | ((x >= RX && x < RX + TX) ? 8 : 0);
     }
+    // the tile's columns come in whole lanes (RX and TX are multiples of 4)
+    const bool lane_tile = (fl[0] & 8) != 0;
     // register window: w[c][m] = column c on plane tau+1-m
     float w[kTbCW][W];
 #pragma unroll
@@ -217,19 +224,13 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
     unsigned long long h0 = 0, l0 = 0, h1 = 0, l1 = 0, h2 = 0, l2 = 0;
     int bad = 0;
 
-    // plane k of this warp's row: lane copies global columns lane + 32*cc
-    // (128-byte coalesced) to their shared positions
-    const int d0 = y * RW + (lane & 3) * 32 + (lane >> 2);
+    // plane k of this warp's row: one 16-byte copy per lane and array
+    const int d0 = y * RW4 + lane;
     auto request = [&](int k, int slot) {
         if (k <= ke) {
-            const long long src = roff + pstride * k + lane;
-            float *Pp = P + slot * RA + d0;
-            float *Bp = Bs + slot * RA + d0;
-#pragma unroll
-            for (int cc = 0; cc < kTbCW; ++cc) {
-                tb_cp_async4(Pp + 8 * cc, pin + src + 32 * cc);
-                tb_cp_async4(Bp + 8 * cc, a.rhs + src + 32 * cc);
-            }
+            const long long src = coff + pstride * k;
+            tb_cp_async16(reinterpret_cast<float *>(P + slot * RA4 + d0), pin + src);
+            tb_cp_async16(reinterpret_cast<float *>(Bs + slot * RA4 + d0), a.rhs + src);
         }
         tb_cp_commit();
     };
@@ -243,10 +244,15 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
         tb_cp_wait<D>();  // plane tau+1 has landed (this thread's copies)
         __syncthreads();  // ... and everyone's
 #pragma unroll
-        for (int c = 0; c < kTbCW; ++c) {
+        for (int c = 0; c < kTbCW; ++c)
 #pragma unroll
             for (int m = W - 1; m > 0; --m) w[c][m] = w[c][m - 1];
-            if (tau + 1 <= ke) w[c][0] = P[st1 * RA + y * RW + c * 32 + lane];
+        if (tau + 1 <= ke) {
+            const float4 v = P[st1 * RA4 + d0];
+            w[0][0] = v.x;
+            w[1][0] = v.y;
+            w[2][0] = v.z;
+            w[3][0] = v.w;
         }
 #pragma unroll
         for (int s = 0; s < 2 * T; ++s) {
@@ -256,34 +262,31 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
             if (s < nhs && q >= qlo && q <= qhi && y >= lo && y < RH - lo) {
                 int sq = st1 - 1 - s;
                 if (sq < 0) sq += NS;
-                float *Pq = P + sq * RA;
-                const float *Bq = Bs + sq * RA;
+                float4 *Pq = P + sq * RA4 + d0;
+                const float4 nn = Pq[RW4], ss = Pq[-RW4], bb = Bs[sq * RA4 + d0];
+                const float pn4[kTbCW] = {nn.x, nn.y, nn.z, nn.w}, ps4[kTbCW] = {ss.x, ss.y, ss.z, ss.w};
+                const float b4[kTbCW] = {bb.x, bb.y, bb.z, bb.w};
                 const float c4l = g.cn4l[q], c4s = g.cn4s[q];
                 const float cnq = CN1K ? a.cn1k[q] : 0.0f;
                 const float cC = CN1K ? 0.0f : g.cnC[q];
                 const bool top = (q == km), bottom = (q == 1);
-                const bool acc = !redo && ytile && q >= k0 && q <= k1;
+                const bool acc = !redo && ytile && lane_tile && q >= k0 && q <= k1;
                 // update column C (of this half-sweep's colour) given its x neighbours
                 auto upd = [&](auto Cc, float west, float east) {
                     constexpr int C = decltype(Cc)::value;
                     const int x = kTbCW * lane + C;
-                    if (x < lo || x >= RW - lo || !(fl[C] & 1)) return;
+                    if (x < lo || x >= kTbRW - lo || !(fl[C] & 1)) return;
                     const float pc = w[C][s + 1];
                     const float pe = (fl[C] & 4) ? pc : east;
                     const float pw = (fl[C] & 2) ? pc : west;
-                    const int o = y * RW + C * 32 + lane;
-                    const float pn = Pq[o + RW];
-                    const float ps = Pq[o - RW];
                     const float pu = top ? pc : w[C][s];
                     const float pd = bottom ? pc : w[C][s + 2];
                     const float cn1 = CN1K ? cnq : 1.0f / (cA[C] + cB + cC);
-                    const float reltmp = omega * (cn1 * (c2l[C] * pe + c2s[C] * pw + c3l * pn + c3s * ps + c4l * pu +
-                                                         c4s * pd - (Bq[o] - rhsav)) -
+                    const float reltmp = omega * (cn1 * (c2l[C] * pe + c2s[C] * pw + c3l * pn4[C] + c3s * ps4[C] +
+                                                         c4l * pu + c4s * pd - (b4[C] - rhsav)) -
                                                   pc);
-                    const float nv = pc + reltmp;
-                    Pq[o] = nv;
-                    w[C][s + 1] = nv;
-                    if (acc && (fl[C] & 8)) {
+                    w[C][s + 1] = pc + reltmp;
+                    if (acc) {
                         if (s < 2)
                             fix_add_nonneg(reltmp * reltmp, h0, l0, bad);
                         else if (s < 4)
@@ -304,21 +307,21 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
                     upd(std::integral_constant<int, 1>(), w[0][s + 1], w[2][s + 1]);
                     upd(std::integral_constant<int, 3>(), w[2][s + 1], nb);
                 }
+                // publish the row's four columns (the other colour's two are
+                // unchanged, so concurrent readers of those see the same bits)
+                *Pq = make_float4(w[0][s + 1], w[1][s + 1], w[2][s + 1], w[3][s + 1]);
             }
         }
         // plane tau+1-2T is final: store the tile part of the row
         const int qs = tau + 1 - 2 * T;
-        if (ytile && qs >= k0 && qs <= k1) {
-            float *dst = pout + (roff + pstride * qs + kTbCW * lane);
+        if (ytile && lane_tile && qs >= k0 && qs <= k1) {
+            float *dst = pout + (coff + pstride * qs);
+            if ((fl[3] & 1))  // all four columns inside the grid: one 16-byte store
+                *reinterpret_cast<float4 *>(dst) = make_float4(w[0][2 * T], w[1][2 * T], w[2][2 * T], w[3][2 * T]);
+            else {
 #pragma unroll
-            for (int h = 0; h < kTbCW; h += 2) {
-                const bool s0 = (fl[h] & 9) == 9, s1 = (fl[h + 1] & 9) == 9;
-                if (s0 && s1)  // (ir0 + 4l + h) + 31 is even: 8-byte aligned
-                    *reinterpret_cast<float2 *>(dst + h) = make_float2(w[h][2 * T], w[h + 1][2 * T]);
-                else if (s0)
-                    dst[h] = w[h][2 * T];
-                else if (s1)
-                    dst[h + 1] = w[h + 1][2 * T];
+                for (int c = 0; c < kTbCW; ++c)
+                    if (fl[c] & 1) dst[c] = w[c][2 * T];
             }
         }
         st1 = (st1 + 1 == NS) ? 0 : st1 + 1;
