@@ -40,6 +40,25 @@ struct UVWBand {
     }
 };
 
+// The band for an interior tile: every position of the ring and its +-1
+// neighbours lies inside the band without moving by jm, and the plane slots
+// around the plane being filled (kc) are looked up once.
+struct UVWBandFast {
+    const float *sl[4];  // slots of planes kc-1 .. kc+2
+    int ib2, jb2, kc;
+    __device__ __forceinline__ UVWBandFast(const float *base, int ib2_, int jb2_, int kc_)
+        : ib2(ib2_), jb2(jb2_), kc(kc_) {
+#pragma unroll
+        for (int d = 0; d < 4; ++d) sl[d] = base + ((kc + d) % kBS) * 3 * kBA;  // plane kc-1+d
+    }
+    __device__ __forceinline__ float at(int f, int i, int j, int k) const {
+        return sl[k - kc + 1][f * kBA + (j - jb2) * kBW + (i - ib2)];
+    }
+    __device__ __forceinline__ float U(const Geo &, int i, int j, int k) const { return at(0, i, j, k); }
+    __device__ __forceinline__ float V(const Geo &, int i, int j, int k) const { return at(1, i, j, k); }
+    __device__ __forceinline__ float W(const Geo &, int i, int j, int k) const { return at(2, i, j, k); }
+};
+
 __device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc));
@@ -143,6 +162,71 @@ __device__ __forceinline__ void vel2_pair(const Geo &g, const Q &q, int n, int i
     }
 }
 
+// vel2_pair for a position with 1 <= i <= im and 1 <= j <= jm: only the k
+// ranges of vel2.f95:48-123 remain (kr bit 0: 1..km, 1: 1..km+1, 2: 1..km-1).
+template <class Q>
+__device__ __forceinline__ void vel2_pair_in(const Geo &g, const Q &q, int n, int i, int j, int k, int kr, float &d,
+                                             float &c) {
+    d = 0.0f;
+    c = 0.0f;
+    switch (n) {
+        case 1:
+            if (kr & 1) {
+                d = diu1_raw(g, q, i, j, k);
+                c = nou1_raw(g, q, i, j, k) * d;
+            }
+            break;
+        case 2:
+            if (kr & 1) {
+                d = diu2_raw(g, q, i, j, k);
+                c = nou2_raw(g, q, i, j, k) * d;
+            }
+            break;
+        case 3:
+            if (kr & 2) {
+                d = diu3_raw(g, q, i, j, k);
+                c = nou3_raw(g, q, i, j, k) * d;
+            }
+            break;
+        case 4:
+            if (kr & 1) {
+                d = diu4_raw(g, q, i, j, k);
+                c = (nou4_raw(g, q, i, j, k) - 0.0f) * d;
+            }
+            break;
+        case 5:
+            if (kr & 1) {
+                d = diu5_raw(g, q, i, j, k);
+                c = nou5_raw(g, q, i, j, k) * d;
+            }
+            break;
+        case 6:
+            if (kr & 2) {
+                d = diu6_raw(g, q, i, j, k);
+                c = nou6_raw(g, q, i, j, k) * d;
+            }
+            break;
+        case 7:
+            if (kr & 4) {
+                d = diu7_raw(g, q, i, j, k);
+                c = (nou7_raw(g, q, i, j, k) - 0.0f) * d;
+            }
+            break;
+        case 8:
+            if (kr & 4) {
+                d = diu8_raw(g, q, i, j, k);
+                c = nou8_raw(g, q, i, j, k) * d;
+            }
+            break;
+        default:  // 9
+            if (kr & 1) {
+                d = diu9_raw(g, q, i, j, k);
+                c = nou9_raw(g, q, i, j, k) * d;
+            }
+            break;
+    }
+}
+
 // Shared-memory view: plane slots cur (k), nxt (k+1) and prv78 (diu7, diu8
 // of k-1), for the cell policies of les_step.cuh.
 struct TileView {
@@ -208,9 +292,11 @@ __device__ __forceinline__ void velfg_tile(const Geo &g, const TileView &t, int 
 
 // Fill plane slot `dst` with the 18 values of plane k over the ring; copy
 // the diu7/diu8 the slot held (plane k-2) into prv7/prv8 first if asked.
-template <bool DIU_ONLY, class Q>
+// INTERIOR: the whole ring lies in 1..im x 1..jm (see vel2_pair_in).
+template <bool DIU_ONLY, bool INTERIOR, class Q>
 __device__ __forceinline__ void tile_plane(const Geo &g, const Q &q, float *dst, float *prv7, float *prv8, int ib,
                                            int jb, int k, bool save_prev) {
+    const int kr = (k >= 1 && k <= g.km ? 1 : 0) | (k >= 1 && k <= g.km + 1 ? 2 : 0) | (k >= 1 && k <= g.km - 1 ? 4 : 0);
     for (int p = threadIdx.x; p < kMPOS; p += kMNT) {
         const int i = ib + p % kMEX, j = jb + p / kMEX;
         if (save_prev) {
@@ -220,7 +306,10 @@ __device__ __forceinline__ void tile_plane(const Geo &g, const Q &q, float *dst,
 #pragma unroll
         for (int n = 1; n <= 9; ++n) {
             float d, c;
-            vel2_pair(g, q, n, i, j, k, d, c);
+            if (INTERIOR)
+                vel2_pair_in(g, q, n, i, j, k, kr, d, c);
+            else
+                vel2_pair(g, q, n, i, j, k, d, c);
             dst[(V_D1 + n - 1) * kMPOS + p] = d;
             if (!DIU_ONLY) dst[(V_C1 + n - 1) * kMPOS + p] = c;
         }
@@ -235,11 +324,12 @@ __host__ __device__ constexpr size_t mom_smem(bool diu_only) {
 
 // Shared prologue/march of both momentum kernels: stage u,v,w planes, fill
 // the face-value ring plane by plane, call `cell` for every tile cell.
-template <bool DIU_ONLY, bool BAND, class CellFn>
+template <bool DIU_ONLY, bool BAND, bool INTERIOR, class CellFn>
 __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn cell) {
     extern __shared__ float sh[];
     constexpr int NVU = DIU_ONLY ? 9 : NV;
-    float *slot[2] = {sh, sh + NVU * kMPOS};
+    float *const s0 = sh, *const s1 = sh + NVU * kMPOS;  // the two face-value plane slots
+    auto slot = [&](int x) { return x ? s1 : s0; };
     float *prv7 = sh + 2 * NVU * kMPOS, *prv8 = prv7 + kMPOS;
     float *band = prv8 + kMPOS;
     const int i0 = 1 + blockIdx.x * kMX, j0 = 1 + blockIdx.y * kMY;
@@ -247,10 +337,12 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
     const UVW qg{F.u, F.v, F.w};
     const UVWBand qb{band, i0 - 2, j0 - 2};
     auto fill = [&](float *dst, int k, bool save) {
-        if (BAND)
-            tile_plane<DIU_ONLY>(g, qb, dst, prv7, prv8, ib, jb, k, save);
+        if (BAND && INTERIOR)
+            tile_plane<DIU_ONLY, true>(g, UVWBandFast(band, i0 - 2, j0 - 2, k), dst, prv7, prv8, ib, jb, k, save);
+        else if (BAND)
+            tile_plane<DIU_ONLY, false>(g, qb, dst, prv7, prv8, ib, jb, k, save);
         else
-            tile_plane<DIU_ONLY>(g, qg, dst, prv7, prv8, ib, jb, k, save);
+            tile_plane<DIU_ONLY, false>(g, qg, dst, prv7, prv8, ib, jb, k, save);
     };
     if (BAND) {  // planes -1..1 and 0..2 fill the first two face planes; 3 is needed at k=1
         for (int k = -1; k <= 3; ++k) band_load(g, F, band, i0 - 2, j0 - 2, k);
@@ -258,8 +350,8 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
         cp_async_wait<0>();
         __syncthreads();
     }
-    fill(slot[0], 0, false);
-    fill(slot[1], 1, false);
+    fill(s0, 0, false);
+    fill(s1, 1, false);
     __syncthreads();
     for (int k = 1; k <= g.km; ++k) {
         if (BAND) {  // plane k+3 streams in while plane k+1 is filled from k..k+2
@@ -267,21 +359,30 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
             cp_async_commit();
         }
         // slot (k+1)&1 holds plane k-1: keep its diu7/diu8, then plane k+1
-        fill(slot[(k + 1) & 1], k + 1, true);
+        fill(slot((k + 1) & 1), k + 1, true);
         __syncthreads();
-        const TileView t{slot[k & 1], slot[(k + 1) & 1], prv7, prv8, ib, jb, k};
+        const TileView t{slot(k & 1), slot((k + 1) & 1), prv7, prv8, ib, jb, k};
         cell(t, k);
         if (BAND) cp_async_wait<0>();
         __syncthreads();
     }
 }
 
+// This CTA's tile ring (i0-1 .. i0+32, j0-1 .. j0+8) inside 1..im x 1..jm,
+// with the band in use (see UVWBandFast).
+template <bool BAND>
+__device__ __forceinline__ bool tile_interior_b(const Geo &g) {
+    const int ib = blockIdx.x * kMX, jb = blockIdx.y * kMY;  // i0-1, j0-1
+    return BAND && ib >= 1 && ib + kMEX - 1 <= g.im && jb >= 1 && jb + kMEY - 1 <= g.jm;
+}
+#define tile_interior(g) tile_interior_b<BAND>(g)
+
 // velFG + feedbf + sgs viscosity (les.f95:132-152) for a 32 x 8 tile, all k.
 template <bool BAND>
 __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
     const bool mine = (i <= g.im && j <= g.jm);
-    mom_march<false, BAND>(g, F, [&](const TileView &t, int k) {
+    auto cell = [&](const TileView &t, int k) {
         if (!mine) return;
         const int c = IX(g, i, j, k);
         float fv, gv, hv = F.h[c];
@@ -292,7 +393,11 @@ __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
         F.g[c] = gv + fy;
         F.h[c] = hv + fz;
         F.sm[c] = sgs_sm(g, t, i, j, k);
-    });
+    };
+    if (tile_interior(g))
+        mom_march<false, BAND, true>(g, F, cell);
+    else
+        mom_march<false, BAND, false>(g, F, cell);
 }
 
 // les.f95:170-274 viscous terms (+ adam.f95:32-46) for a 32 x 8 tile, all k.
@@ -300,7 +405,7 @@ template <bool ADAM, bool BAND>
 __global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
     const bool mine = (i <= g.im && j <= g.jm);
-    mom_march<true, BAND>(g, F, [&](const TileView &t, int k) {
+    auto cell = [&](const TileView &t, int k) {
         if (!mine) return;
         float vfu, vfv, vfw;
         visc_cell(g, t, F.sm, i, j, k, vfu, vfv, vfw);
@@ -318,7 +423,11 @@ __global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
             F.g[c] = gv;
             F.h[c] = hv;
         }
-    });
+    };
+    if (tile_interior(g))
+        mom_march<true, BAND, true>(g, F, cell);
+    else
+        mom_march<true, BAND, false>(g, F, cell);
 }
 
 }  // namespace
