@@ -67,21 +67,44 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// Issue the copies of plane k (k in -1..kp+2) of u, v, w into its slot.  A
-// band row is 36 floats starting at an even box offset (ib2 + 31 = 32*bx +
-// 30), copied as 18 pairs; columns past the box row end read the next row
-// (still inside the allocation) and are never used.
-__device__ __forceinline__ void band_load(const Geo &g, const Fields &F, float *base, int ib2, int jb2, int k) {
-    float *slot = base + ((k + 1) % kBS) * 3 * kBA;
-    const int npair = kBW / 2;
-    for (int e = threadIdx.x; e < 3 * kBH * npair; e += kMNT) {
-        const int f = e / (kBH * npair), rem = e % (kBH * npair);
-        const int b = rem / npair, pr = rem % npair;
-        const int j = ((jb2 + b - 1) % g.jm + g.jm) % g.jm + 1;
-        const float *src = (f == 0 ? F.u : (f == 1 ? F.v : F.w)) + IX(g, ib2 + 2 * pr, j, k);
-        cp_async8(slot + f * kBA + b * kBW + 2 * pr, src);
+// The band copies of one thread: plane k of u, v, w moves as 3 x 12 rows of
+// 18 float pairs (a row is 36 floats starting at an even box offset:
+// ib2 + 31 = 32*bx + 30).  Thread t issues pairs t, t+256, t+512 (< 648);
+// the source address at k = 0 and the slot offset are fixed for the whole
+// march, so a plane costs one pointer step per copy.  Columns past the box
+// row end read the next row (still inside the allocation) and are never used.
+struct BandCopies {
+    static constexpr int kPairs = 3 * kBH * (kBW / 2), kPer = (kPairs + kMNT - 1) / kMNT;
+    const float *src[kPer];  // plane-0 source of each copy (nullptr: none)
+    int dst[kPer];           // float offset inside a plane slot
+    long long pstride;
+    __device__ __forceinline__ BandCopies() : pstride(0) {}
+    __device__ __forceinline__ BandCopies(const Geo &g, const Fields &F, int ib2, int jb2) {
+        constexpr int npair = kBW / 2;
+        pstride = (long long)g.si * g.sj;
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) {
+            const int e = threadIdx.x + r * kMNT;
+            if (e < kPairs) {
+                const int f = e / (kBH * npair), rem = e % (kBH * npair);
+                const int b = rem / npair, pr = rem % npair;
+                const int j = ((jb2 + b - 1) % g.jm + g.jm) % g.jm + 1;  // periodic j
+                src[r] = (f == 0 ? F.u : (f == 1 ? F.v : F.w)) + IX(g, ib2 + 2 * pr, j, 0);
+                dst[r] = f * kBA + b * kBW + 2 * pr;
+            } else {
+                src[r] = nullptr;
+                dst[r] = 0;
+            }
+        }
     }
-}
+    // Issue the copies of plane k (k in -1..kp+2) into its slot.
+    __device__ __forceinline__ void load(float *base, int k) const {
+        float *slot = base + ((k + 1) % kBS) * 3 * kBA;
+#pragma unroll
+        for (int r = 0; r < kPer; ++r)
+            if (src[r]) cp_async8(slot + dst[r], src[r] + pstride * k);
+    }
+};
 
 // diu_n and cov_n at (i,j,k) (n = 1..9), as the arrays hold them after vel2.
 template <class Q>
@@ -344,8 +367,9 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
         else
             tile_plane<DIU_ONLY, false>(g, qg, dst, prv7, prv8, ib, jb, k, save);
     };
+    const BandCopies bc = BAND ? BandCopies(g, F, i0 - 2, j0 - 2) : BandCopies();
     if (BAND) {  // planes -1..1 and 0..2 fill the first two face planes; 3 is needed at k=1
-        for (int k = -1; k <= 3; ++k) band_load(g, F, band, i0 - 2, j0 - 2, k);
+        for (int k = -1; k <= 3; ++k) bc.load(band, k);
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
@@ -355,7 +379,7 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
     __syncthreads();
     for (int k = 1; k <= g.km; ++k) {
         if (BAND) {  // plane k+3 streams in while plane k+1 is filled from k..k+2
-            if (k + 3 <= g.km + 2) band_load(g, F, band, i0 - 2, j0 - 2, k + 3);
+            if (k + 3 <= g.km + 2) bc.load(band, k + 3);
             cp_async_commit();
         }
         // slot (k+1)&1 holds plane k-1: keep its diu7/diu8, then plane k+1
