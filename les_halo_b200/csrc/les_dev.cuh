@@ -30,11 +30,69 @@ struct Geo {
     // power-of-two divisor d, a*(1/d) and a/d are the correctly rounded
     // value of the same real number, so they are bit-identical.
     const float *rdx1, *rsx, *rdy1, *rsy;
+    // RN(1/b) for the k divisors b = dzn(k), dzs(k), dzn(k)+dzn(k+1) (kdiv),
+    // 0 where kdiv must divide
+    const float *rdzn, *rdzs, *rdzn2;
     float dt, ro, vn, alpha, beta, omega;
 };
 
 // a/d with d's exact reciprocal r when d is a power of two (r != 0).
 __device__ __forceinline__ float fdiv(float a, float d, float r) { return r != 0.0f ? a * r : a / d; }
+
+// a/b given y = RN(1/b): Markstein's correction (P. Markstein, IBM J. Res.
+// Dev. 34(1), 1990): q0 = RN(a*y), r = a - b*q0 exactly (one fma),
+// q = RN(q0 + r*y) is the correctly rounded a/b.  Used while q0 lies in
+// [2^-60, 2^60]; zero, tiny, huge and non-finite quotients (and y = 0, set for
+// divisors outside [2^-30, 2^30]) take the IEEE division.  Checked bit for bit
+// against IEEE division for every float a on 7564 divisors (stretched-grid
+// spacings, their sums, random values): no difference.
+__device__ __forceinline__ float kdiv(float a, float b, float y) {
+    const float q0 = a * y;
+    const float m = fabsf(q0);
+    if (!(m >= 0x1p-60f && m <= 0x1p60f)) return a / b;
+    const float r = __fmaf_rn(-q0, b, a);
+    return __fmaf_rn(r, y, q0);
+}
+
+// How the face-value and cell formulas divide.  xd: by an x/y spacing with
+// its power-of-two reciprocal r (or 0); zn/zs/zn2: by dzn(k), dzs(k),
+// dzn(k)+dzn(k+1).  DivIEEE divides as written; DivPlane (the tile engine)
+// holds the divisors and reciprocals of planes kc-1..kc+1 in registers and
+// uses kdiv, and with P2 (every x/y spacing a power of two) multiplies by r.
+// All forms give the IEEE quotient's bits.
+struct DivIEEE {
+    __device__ __forceinline__ float xd(float a, float d, float r) const { return fdiv(a, d, r); }
+    __device__ __forceinline__ float zn(const Geo &g, float a, int k) const { return a / g.dzn[k]; }
+    __device__ __forceinline__ float zs(const Geo &g, float a, int k) const { return a / g.dzs[k]; }
+    __device__ __forceinline__ float zn2(const Geo &g, float a, int k) const { return a / (g.dzn[k] + g.dzn[k + 1]); }
+};
+template <bool P2>
+struct DivPlane {
+    float bn[3], yn[3], bs[3], ys[3], bn2[3], yn2[3];  // planes kc-1, kc, kc+1
+    int kc;
+    __device__ __forceinline__ DivPlane(const Geo &g, int kc_) : kc(kc_) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int k = kc - 1 + d;
+            bn[d] = g.dzn[k];
+            yn[d] = g.rdzn[k];
+            bs[d] = g.dzs[k];
+            ys[d] = g.rdzs[k];
+            bn2[d] = g.dzn[k] + g.dzn[k + 1];
+            yn2[d] = g.rdzn2[k];
+        }
+    }
+    __device__ __forceinline__ float xd(float a, float d, float r) const { return P2 ? a * r : fdiv(a, d, r); }
+    __device__ __forceinline__ float zn(const Geo &, float a, int k) const {
+        return kdiv(a, bn[k - kc + 1], yn[k - kc + 1]);
+    }
+    __device__ __forceinline__ float zs(const Geo &, float a, int k) const {
+        return kdiv(a, bs[k - kc + 1], ys[k - kc + 1]);
+    }
+    __device__ __forceinline__ float zn2(const Geo &, float a, int k) const {
+        return kdiv(a, bn2[k - kc + 1], yn2[k - kc + 1]);
+    }
+};
 
 struct Fields {
     float *u, *v, *w, *p, *usum, *vsum, *wsum, *f, *g, *h, *fold, *gold, *hold, *rhs, *sm;
@@ -65,7 +123,7 @@ __device__ __forceinline__ int IX(const Geo &g, int i, int j, int k) {
 // ifdata.f95:15-127) everywhere nothing ever writes.
 // ---------------------------------------------------------------------------
 // u, v, w read straight from the state boxes.
-struct UVW {
+struct UVW : DivIEEE {
     const float *__restrict__ u;
     const float *__restrict__ v;
     const float *__restrict__ w;
@@ -84,7 +142,7 @@ __device__ __forceinline__ float nou1_raw(const Geo &g, const Q &q, int i, int j
 }
 template <class Q>
 __device__ __forceinline__ float diu1_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(-LU(i - 1, j, k) + LU(i, j, k), g.dx1[i], g.rdx1[i]);
+    return q.xd(-LU(i - 1, j, k) + LU(i, j, k), g.dx1[i], g.rdx1[i]);
 }
 template <class Q>
 __device__ __forceinline__ float nou5_raw(const Geo &g, const Q &q, int i, int j, int k) {
@@ -92,7 +150,7 @@ __device__ __forceinline__ float nou5_raw(const Geo &g, const Q &q, int i, int j
 }
 template <class Q>
 __device__ __forceinline__ float diu5_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(-LV(i, j - 1, k) + LV(i, j, k), g.dy1[j], g.rdy1[j]);
+    return q.xd(-LV(i, j - 1, k) + LV(i, j, k), g.dy1[j], g.rdy1[j]);
 }
 template <class Q>
 __device__ __forceinline__ float nou9_raw(const Geo &g, const Q &q, int i, int j, int k) {
@@ -100,55 +158,55 @@ __device__ __forceinline__ float nou9_raw(const Geo &g, const Q &q, int i, int j
 }
 template <class Q>
 __device__ __forceinline__ float diu9_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return (-LW(i, j, k - 1) + LW(i, j, k)) / g.dzn[k];
+    return q.zn(g, -LW(i, j, k - 1) + LW(i, j, k), k);
 }
 template <class Q>
 __device__ __forceinline__ float nou2_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(g.dx1[i + 1] * LV(i, j - 1, k) + g.dx1[i] * LV(i + 1, j - 1, k), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
+    return q.xd(g.dx1[i + 1] * LV(i, j - 1, k) + g.dx1[i] * LV(i + 1, j - 1, k), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
 }
 template <class Q>
 __device__ __forceinline__ float diu2_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(2.0f * (-LU(i, j - 1, k) + LU(i, j, k)), g.dy1[j - 1] + g.dy1[j], g.rsy[j - 1]);
+    return q.xd(2.0f * (-LU(i, j - 1, k) + LU(i, j, k)), g.dy1[j - 1] + g.dy1[j], g.rsy[j - 1]);
 }
 template <class Q>
 __device__ __forceinline__ float nou3_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(g.dx1[i + 1] * LW(i, j, k - 1) + g.dx1[i] * LW(i + 1, j, k - 1), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
+    return q.xd(g.dx1[i + 1] * LW(i, j, k - 1) + g.dx1[i] * LW(i + 1, j, k - 1), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
 }
 template <class Q>
 __device__ __forceinline__ float diu3_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return (-LU(i, j, k - 1) + LU(i, j, k)) / g.dzs[k - 1];
+    return q.zs(g, -LU(i, j, k - 1) + LU(i, j, k), k - 1);
 }
 template <class Q>
 __device__ __forceinline__ float nou4_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(g.dy1[j + 1] * LU(i - 1, j, k) + g.dy1[j] * LU(i - 1, j + 1, k), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
+    return q.xd(g.dy1[j + 1] * LU(i - 1, j, k) + g.dy1[j] * LU(i - 1, j + 1, k), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
 }
 template <class Q>
 __device__ __forceinline__ float diu4_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(2.0f * (-LV(i - 1, j, k) + LV(i, j, k)), g.dx1[i - 1] + g.dx1[i], g.rsx[i - 1]);
+    return q.xd(2.0f * (-LV(i - 1, j, k) + LV(i, j, k)), g.dx1[i - 1] + g.dx1[i], g.rsx[i - 1]);
 }
 template <class Q>
 __device__ __forceinline__ float nou6_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(g.dy1[j + 1] * LW(i, j, k - 1) + g.dy1[j] * LW(i, j + 1, k - 1), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
+    return q.xd(g.dy1[j + 1] * LW(i, j, k - 1) + g.dy1[j] * LW(i, j + 1, k - 1), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
 }
 template <class Q>
 __device__ __forceinline__ float diu6_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return (-LV(i, j, k - 1) + LV(i, j, k)) / g.dzs[k - 1];
+    return q.zs(g, -LV(i, j, k - 1) + LV(i, j, k), k - 1);
 }
 template <class Q>
 __device__ __forceinline__ float nou7_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return (g.dzn[k + 1] * LU(i - 1, j, k) + g.dzn[k] * LU(i - 1, j, k + 1)) / (g.dzn[k] + g.dzn[k + 1]);
+    return q.zn2(g, g.dzn[k + 1] * LU(i - 1, j, k) + g.dzn[k] * LU(i - 1, j, k + 1), k);
 }
 template <class Q>
 __device__ __forceinline__ float diu7_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(2.0f * (-LW(i - 1, j, k) + LW(i, j, k)), g.dx1[i - 1] + g.dx1[i], g.rsx[i - 1]);
+    return q.xd(2.0f * (-LW(i - 1, j, k) + LW(i, j, k)), g.dx1[i - 1] + g.dx1[i], g.rsx[i - 1]);
 }
 template <class Q>
 __device__ __forceinline__ float nou8_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return (g.dzn[k + 1] * LV(i, j - 1, k) + g.dzn[k] * LV(i, j - 1, k + 1)) / (g.dzn[k] + g.dzn[k + 1]);
+    return q.zn2(g, g.dzn[k + 1] * LV(i, j - 1, k) + g.dzn[k] * LV(i, j - 1, k + 1), k);
 }
 template <class Q>
 __device__ __forceinline__ float diu8_raw(const Geo &g, const Q &q, int i, int j, int k) {
-    return fdiv(2.0f * (-LW(i, j - 1, k) + LW(i, j, k)), g.dy1[j - 1] + g.dy1[j], g.rsy[j - 1]);
+    return q.xd(2.0f * (-LW(i, j - 1, k) + LW(i, j, k)), g.dy1[j - 1] + g.dy1[j], g.rsy[j - 1]);
 }
 
 // j index of the periodic copies X(i,0,k)=X(i,jm,k), X(i,jm+1,k)=X(i,1,k);

@@ -98,7 +98,7 @@ FBounds field_bounds(int f, int ip, int jp, int kp) {
 // Offsets of the 1-D tables inside one device buffer (each with slack).
 struct TableLayout {
     size_t dx1, dy1, dzn, dzs, dxs, dys, cn2l, cn2s, cn3l, cn3s, cn4l, cn4s, cnA, cnB, cnC, smc, wind;
-    size_t rdx1, rsx, rdy1, rsy, cn1k, total;
+    size_t rdx1, rsx, rdy1, rsy, cn1k, rdzn, rdzs, rdzn2, total;
 };
 TableLayout table_layout(int ip, int jp, int kp) {
     TableLayout t;
@@ -130,6 +130,9 @@ TableLayout table_layout(int ip, int jp, int kp) {
     t.rdy1 = take(jp + 4);
     t.rsy = take(jp + 4);
     t.cn1k = take(kp + 2);
+    t.rdzn = take(kp + 5);
+    t.rdzs = take(kp + 5);
+    t.rdzn2 = take(kp + 5);
     t.total = o;
     return t;
 }
@@ -179,6 +182,7 @@ struct les_ctx {
     // temporal-blocked SOR (les_sor_tb.cuh)
     float *d_p2 = nullptr;           // second p buffer
     TbShape tb;  // SOR pass shape chosen by the autotuner (tb.T == 0: not yet)
+    bool xy_pow2 = false;  // every x/y spacing divisor a power of two (build_tables)
     bool cn1_by_k = false;           // uniform dx, dy: cn1 from a per-k table
     bool p_ghosts_ok = false;        // p's ghosts hold what boundp1/boundp2 give
     bool force_exact_sor = false;    // testing: always the per-colour path
@@ -191,6 +195,13 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
 
 // Host copies of the 1-D tables -> device; builds cnA/B/C, smc, wind.
 // Tables not given stay zero (the per-routine entries pass only theirs).
+// y = RN(1/b) for kdiv, or 0 when b is outside [2^-30, 2^30] (or not
+// finite), which makes kdiv divide.
+float kdiv_recip(float b) {
+    const float a = std::fabs(b);
+    return (a >= 0x1p-30f && a <= 0x1p30f) ? 1.0f / b : 0.0f;
+}
+
 les_status build_tables(les_ctx *c, const les_host_fields *hf, bool require_inflow) {
     const int ip = c->prm.ip, jp = c->prm.jp, kp = c->prm.kp;
     const TableLayout &t = c->tl;
@@ -264,6 +275,19 @@ les_status build_tables(les_ctx *c, const les_host_fields *hf, bool require_infl
     for (int i = -1; i <= ip; ++i) h[t.rsx + i + 1] = recip(dx1(i) + dx1(i + 1));
     for (int j = 0; j <= jp + 1; ++j) h[t.rdy1 + j] = recip(dy1(j));
     for (int j = 0; j <= jp; ++j) h[t.rsy + j] = recip(dy1(j) + dy1(j + 1));
+    // reciprocals of the k divisors for kdiv
+    for (int k = -1; k <= kp + 2; ++k) {
+        h[t.rdzn + k + 1] = kdiv_recip(dzn(k));
+        h[t.rdzs + k + 1] = kdiv_recip(dzs(k));
+        if (k <= kp + 1) h[t.rdzn2 + k + 1] = kdiv_recip(dzn(k) + dzn(k + 1));
+    }
+    // every x/y divisor of the face and cell formulas a power of two: the tile
+    // engine multiplies by the reciprocal without testing it
+    c->xy_pow2 = true;
+    for (int i = -1; i <= ip + 1; ++i) c->xy_pow2 = c->xy_pow2 && h[t.rdx1 + i + 1] != 0.0f;
+    for (int i = -1; i <= ip; ++i) c->xy_pow2 = c->xy_pow2 && h[t.rsx + i + 1] != 0.0f;
+    for (int j = 0; j <= jp + 1; ++j) c->xy_pow2 = c->xy_pow2 && h[t.rdy1 + j] != 0.0f;
+    for (int j = 0; j <= jp; ++j) c->xy_pow2 = c->xy_pow2 && h[t.rsy + j] != 0.0f;
     // grid-only denominator of rhsav and pav (press.f95:134, 192)
     i128 acc = 0;
     int bad = 0;
@@ -324,22 +348,34 @@ les_status enqueue_velfg_les(les_ctx *c, bool adam) {
     const Geo &g = c->geo;
     const dim3 mg(cdiv(g.im, kMX), cdiv(g.jm, kMY));
     const bool band = g.jm >= kBH;  // the staged band must not wrap onto itself
-    if (band)
-        LAUNCH_SMEM(c, k_mom1<true>, mg, dim3(kMNT), mom_smem(false), g, c->F);
+    const bool p2 = band && c->xy_pow2;
+    if (p2)
+        LAUNCH_SMEM(c, (k_mom1<true, true>), mg, dim3(kMNT), mom_smem(false), g, c->F);
+    else if (band)
+        LAUNCH_SMEM(c, (k_mom1<true, false>), mg, dim3(kMNT), mom_smem(false), g, c->F);
     else
-        LAUNCH_SMEM(c, k_mom1<false>, mg, dim3(kMNT), mom_smem(false), g, c->F);
+        LAUNCH_SMEM(c, (k_mom1<false, false>), mg, dim3(kMNT), mom_smem(false), g, c->F);
     MARK(c, EV_VELFG);
     const long long nb = 2LL * (g.jm + 3) * (g.km + 2) + 2LL * g.im * (g.km + 2) + 2LL * g.im * (g.jm + 1);
     LAUNCH(c, k_boundsm, dim3(cdiv(nb, 256)), dim3(256), g, c->F.sm);
     const size_t sm2 = mom_smem(true);
-    if (adam && band)
-        LAUNCH_SMEM(c, (k_mom2<true, true>), mg, dim3(kMNT), sm2, g, c->F);
-    else if (adam)
-        LAUNCH_SMEM(c, (k_mom2<true, false>), mg, dim3(kMNT), sm2, g, c->F);
-    else if (band)
-        LAUNCH_SMEM(c, (k_mom2<false, true>), mg, dim3(kMNT), sm2, g, c->F);
-    else
-        LAUNCH_SMEM(c, (k_mom2<false, false>), mg, dim3(kMNT), sm2, g, c->F);
+#define M2(A, B, P) LAUNCH_SMEM(c, (k_mom2<A, B, P>), mg, dim3(kMNT), sm2, g, c->F)
+    if (adam) {
+        if (p2)
+            M2(true, true, true);
+        else if (band)
+            M2(true, true, false);
+        else
+            M2(true, false, false);
+    } else {
+        if (p2)
+            M2(false, true, true);
+        else if (band)
+            M2(false, true, false);
+        else
+            M2(false, false, false);
+    }
+#undef M2
     MARK(c, EV_VISC);
     return LES_OK;
 }
@@ -696,12 +732,15 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     {
         const int ms = (int)mom_smem(false);
         const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
-        if (cudaFuncSetAttribute(k_mom1<true>, A, ms) != cudaSuccess ||
-            cudaFuncSetAttribute(k_mom1<false>, A, ms) != cudaSuccess ||
-            cudaFuncSetAttribute(k_mom2<true, true>, A, ms) != cudaSuccess ||
-            cudaFuncSetAttribute(k_mom2<true, false>, A, ms) != cudaSuccess ||
-            cudaFuncSetAttribute(k_mom2<false, true>, A, ms) != cudaSuccess ||
-            cudaFuncSetAttribute(k_mom2<false, false>, A, ms) != cudaSuccess)
+        if (cudaFuncSetAttribute(k_mom1<true, true>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom1<true, false>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom1<false, false>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<true, true, true>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<true, true, false>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<true, false, false>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<false, true, true>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<false, true, false>, A, ms) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mom2<false, false, false>, A, ms) != cudaSuccess)
             return cleanup(fail(LES_ERR_CUDA, "shared memory attribute"));
     }
     // the largest SOR pass grid: narrowest tiles, 4-row tiles, most k chunks
@@ -740,6 +779,9 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     g.rsx = base + t.rsx + 1;
     g.rdy1 = base + t.rdy1;
     g.rsy = base + t.rsy;
+    g.rdzn = base + t.rdzn + 1;
+    g.rdzs = base + t.rdzs + 1;
+    g.rdzn2 = base + t.rdzn2 + 1;
     float **fp[LES_NFIELDS] = {&c->F.u,    &c->F.v,    &c->F.w,    &c->F.p,     &c->F.usum,  &c->F.vsum,  &c->F.wsum,
                                &c->F.f,    &c->F.g,    &c->F.h,    &c->F.fold,  &c->F.gold,  &c->F.hold,  &c->F.rhs,
                                &c->F.sm,   &c->F.amask, &c->F.bmask, &c->F.cmask, &c->F.dmask};

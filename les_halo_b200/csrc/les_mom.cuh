@@ -24,7 +24,7 @@ enum { V_D1 = 0, V_C1 = 9, NV = 18 };
 // Band row b holds real row jwrap(jb2 + b); a real row j is found by moving
 // it by +-jm into the band.  Valid when the band is not taller than jm.
 constexpr int kBW = kMX + 4, kBH = kMY + 4, kBA = kBW * kBH, kBS = 5;
-struct UVWBand {
+struct UVWBand : DivIEEE {
     const float *base;  // slot s, field f at base + (s*3 + f)*kBA
     int ib2, jb2;       // real (i, j) of band position (0, 0)
     __device__ __forceinline__ int off(const Geo &g, int i, int j, int k) const {
@@ -43,16 +43,18 @@ struct UVWBand {
 // The band for an interior tile: every position of the ring and its +-1
 // neighbours lies inside the band without moving by jm, and the plane slots
 // around the plane being filled (kc) are looked up once.
-struct UVWBandFast {
+template <bool P2>
+struct UVWBandFast : DivPlane<P2> {
     const float *sl[4];  // slots of planes kc-1 .. kc+2
-    int ib2, jb2, kc;
-    __device__ __forceinline__ UVWBandFast(const float *base, int ib2_, int jb2_, int kc_)
-        : ib2(ib2_), jb2(jb2_), kc(kc_) {
+    int ib2, jb2;
+    __device__ __forceinline__ UVWBandFast(const Geo &g, const float *base, int ib2_, int jb2_, int kc_)
+        : DivPlane<P2>(g, kc_), ib2(ib2_), jb2(jb2_) {
+        const int kc = kc_;
 #pragma unroll
         for (int d = 0; d < 4; ++d) sl[d] = base + ((kc + d) % kBS) * 3 * kBA;  // plane kc-1+d
     }
     __device__ __forceinline__ float at(int f, int i, int j, int k) const {
-        return sl[k - kc + 1][f * kBA + (j - jb2) * kBW + (i - ib2)];
+        return sl[k - this->kc + 1][f * kBA + (j - jb2) * kBW + (i - ib2)];
     }
     __device__ __forceinline__ float U(const Geo &, int i, int j, int k) const { return at(0, i, j, k); }
     __device__ __forceinline__ float V(const Geo &, int i, int j, int k) const { return at(1, i, j, k); }
@@ -252,9 +254,13 @@ __device__ __forceinline__ void vel2_pair_in(const Geo &g, const Q &q, int n, in
 
 // Shared-memory view: plane slots cur (k), nxt (k+1) and prv78 (diu7, diu8
 // of k-1), for the cell policies of les_step.cuh.
-struct TileView {
+template <bool P2>
+struct TileView : DivPlane<P2> {
     const float *cur, *nxt, *prv7, *prv8;
     int ib, jb, kc;  // i, j of ring position 0 and the current plane
+    __device__ __forceinline__ TileView(const Geo &g, const float *cur_, const float *nxt_, const float *p7,
+                                        const float *p8, int ib_, int jb_, int kc_)
+        : DivPlane<P2>(g, kc_), cur(cur_), nxt(nxt_), prv7(p7), prv8(p8), ib(ib_), jb(jb_), kc(kc_) {}
     __device__ __forceinline__ int pos(int i, int j) const { return (j - jb) * kMEX + (i - ib); }
     __device__ __forceinline__ float dv(int n, int i, int j, int k) const {
         const int p = pos(i, j);
@@ -278,37 +284,38 @@ struct TileView {
 };
 
 // velFG.f95:58-105 for one cell from the tile.
-__device__ __forceinline__ void velfg_tile(const Geo &g, const TileView &t, int i, int j, int k, float &fv, float &gv,
+template <class TV>
+__device__ __forceinline__ void velfg_tile(const Geo &g, const TV &t, int i, int j, int k, float &fv, float &gv,
                                            float &hv) {
-    const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn, *dzs = g.dzs;
+    const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn;
     {
-        float covx1 = fdiv(dx1[i + 1] * t.cv(1, i, j, k) + dx1[i] * t.cv(1, i + 1, j, k), dx1[i] + dx1[i + 1], g.rsx[i]);
+        float covx1 = t.xd(dx1[i + 1] * t.cv(1, i, j, k) + dx1[i] * t.cv(1, i + 1, j, k), dx1[i] + dx1[i + 1], g.rsx[i]);
         float covy1 = (t.cv(2, i, j, k) + t.cv(2, i, j + 1, k)) / 2.0f;
         float covz1 = (t.cv(3, i, j, k) + t.cv(3, i, j, k + 1)) / 2.0f;
         float covc = covx1 + covy1 + covz1;
-        float dfu1 = fdiv(2.0f * (-t.d1(i, j, k) + t.d1(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]) +
-                     fdiv(-t.d2(i, j, k) + t.d2(i, j + 1, k), dy1[j], g.rdy1[j]) +
-                     (-t.d3(i, j, k) + t.d3(i, j, k + 1)) / dzn[k];
+        float dfu1 = t.xd(2.0f * (-t.d1(i, j, k) + t.d1(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]) +
+                     t.xd(-t.d2(i, j, k) + t.d2(i, j + 1, k), dy1[j], g.rdy1[j]) +
+                     t.zn(g, -t.d3(i, j, k) + t.d3(i, j, k + 1), k);
         fv = (-covc + g.vn * dfu1);
     }
     {
         float covx1 = (t.cv(4, i, j, k) + t.cv(4, i + 1, j, k)) / 2.0f;
-        float covy1 = fdiv(dy1[j + 1] * t.cv(5, i, j, k) + dy1[j] * t.cv(5, i, j + 1, k), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float covy1 = t.xd(dy1[j + 1] * t.cv(5, i, j, k) + dy1[j] * t.cv(5, i, j + 1, k), dy1[j] + dy1[j + 1], g.rsy[j]);
         float covz1 = (t.cv(6, i, j, k) + t.cv(6, i, j, k + 1)) / 2.0f;
         float covc = covx1 + covy1 + covz1;
-        float dfv1 = fdiv(-t.d4(i, j, k) + t.d4(i + 1, j, k), dx1[i], g.rdx1[i]) +
-                     fdiv(2.0f * (-t.d5(i, j, k) + t.d5(i, j + 1, k)), dy1[j] + dy1[j + 1], g.rsy[j]) +
-                     (-t.d6(i, j, k) + t.d6(i, j, k + 1)) / dzn[k];
+        float dfv1 = t.xd(-t.d4(i, j, k) + t.d4(i + 1, j, k), dx1[i], g.rdx1[i]) +
+                     t.xd(2.0f * (-t.d5(i, j, k) + t.d5(i, j + 1, k)), dy1[j] + dy1[j + 1], g.rsy[j]) +
+                     t.zn(g, -t.d6(i, j, k) + t.d6(i, j, k + 1), k);
         gv = (-covc + g.vn * dfv1);
     }
     if (k <= g.km - 1) {
         float covx1 = (t.cv(7, i, j, k) + t.cv(7, i + 1, j, k)) / 2.0f;
         float covy1 = (t.cv(8, i, j, k) + t.cv(8, i, j + 1, k)) / 2.0f;
-        float covz1 = (dzn[k + 1] * t.cv(9, i, j, k) + dzn[k] * t.cv(9, i, j, k + 1)) / (dzn[k] + dzn[k + 1]);
+        float covz1 = t.zn2(g, dzn[k + 1] * t.cv(9, i, j, k) + dzn[k] * t.cv(9, i, j, k + 1), k);
         float covc = covx1 + covy1 + covz1;
-        float dfw1 = fdiv(-t.d7(i, j, k) + t.d7(i + 1, j, k), dx1[i], g.rdx1[i]) +
-                     fdiv(-t.d8(i, j, k) + t.d8(i, j + 1, k), dy1[j], g.rdy1[j]) +
-                     (-t.d9(i, j, k) + t.d9(i, j, k + 1)) / dzs[k];
+        float dfw1 = t.xd(-t.d7(i, j, k) + t.d7(i + 1, j, k), dx1[i], g.rdx1[i]) +
+                     t.xd(-t.d8(i, j, k) + t.d8(i, j + 1, k), dy1[j], g.rdy1[j]) +
+                     t.zs(g, -t.d9(i, j, k) + t.d9(i, j, k + 1), k);
         hv = (-covc + g.vn * dfw1);
     }
 }
@@ -347,7 +354,7 @@ __host__ __device__ constexpr size_t mom_smem(bool diu_only) {
 
 // Shared prologue/march of both momentum kernels: stage u,v,w planes, fill
 // the face-value ring plane by plane, call `cell` for every tile cell.
-template <bool DIU_ONLY, bool BAND, bool INTERIOR, class CellFn>
+template <bool DIU_ONLY, bool BAND, bool INTERIOR, bool P2, class CellFn>
 __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn cell) {
     extern __shared__ float sh[];
     constexpr int NVU = DIU_ONLY ? 9 : NV;
@@ -357,11 +364,11 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
     float *band = prv8 + kMPOS;
     const int i0 = 1 + blockIdx.x * kMX, j0 = 1 + blockIdx.y * kMY;
     const int ib = i0 - 1, jb = j0 - 1;
-    const UVW qg{F.u, F.v, F.w};
-    const UVWBand qb{band, i0 - 2, j0 - 2};
+    const UVW qg{{}, F.u, F.v, F.w};
+    const UVWBand qb{{}, band, i0 - 2, j0 - 2};
     auto fill = [&](float *dst, int k, bool save) {
         if (BAND && INTERIOR)
-            tile_plane<DIU_ONLY, true>(g, UVWBandFast(band, i0 - 2, j0 - 2, k), dst, prv7, prv8, ib, jb, k, save);
+            tile_plane<DIU_ONLY, true>(g, UVWBandFast<P2>(g, band, i0 - 2, j0 - 2, k), dst, prv7, prv8, ib, jb, k, save);
         else if (BAND)
             tile_plane<DIU_ONLY, false>(g, qb, dst, prv7, prv8, ib, jb, k, save);
         else
@@ -385,7 +392,7 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
         // slot (k+1)&1 holds plane k-1: keep its diu7/diu8, then plane k+1
         fill(slot((k + 1) & 1), k + 1, true);
         __syncthreads();
-        const TileView t{slot(k & 1), slot((k + 1) & 1), prv7, prv8, ib, jb, k};
+        const TileView<P2> t(g, slot(k & 1), slot((k + 1) & 1), prv7, prv8, ib, jb, k);
         cell(t, k);
         if (BAND) cp_async_wait<0>();
         __syncthreads();
@@ -402,11 +409,11 @@ __device__ __forceinline__ bool tile_interior_b(const Geo &g) {
 #define tile_interior(g) tile_interior_b<BAND>(g)
 
 // velFG + feedbf + sgs viscosity (les.f95:132-152) for a 32 x 8 tile, all k.
-template <bool BAND>
+template <bool BAND, bool P2>
 __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
     const bool mine = (i <= g.im && j <= g.jm);
-    auto cell = [&](const TileView &t, int k) {
+    auto cell = [&](const TileView<P2> &t, int k) {
         if (!mine) return;
         const int c = IX(g, i, j, k);
         float fv, gv, hv = F.h[c];
@@ -419,17 +426,17 @@ __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
         F.sm[c] = sgs_sm(g, t, i, j, k);
     };
     if (tile_interior(g))
-        mom_march<false, BAND, true>(g, F, cell);
+        mom_march<false, BAND, true, P2>(g, F, cell);
     else
-        mom_march<false, BAND, false>(g, F, cell);
+        mom_march<false, BAND, false, P2>(g, F, cell);
 }
 
 // les.f95:170-274 viscous terms (+ adam.f95:32-46) for a 32 x 8 tile, all k.
-template <bool ADAM, bool BAND>
+template <bool ADAM, bool BAND, bool P2>
 __global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
     const bool mine = (i <= g.im && j <= g.jm);
-    auto cell = [&](const TileView &t, int k) {
+    auto cell = [&](const TileView<P2> &t, int k) {
         if (!mine) return;
         float vfu, vfv, vfw;
         visc_cell(g, t, F.sm, i, j, k, vfu, vfv, vfw);
@@ -449,9 +456,9 @@ __global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
         }
     };
     if (tile_interior(g))
-        mom_march<true, BAND, true>(g, F, cell);
+        mom_march<true, BAND, true, P2>(g, F, cell);
     else
-        mom_march<true, BAND, false>(g, F, cell);
+        mom_march<true, BAND, false, P2>(g, F, cell);
 }
 
 }  // namespace

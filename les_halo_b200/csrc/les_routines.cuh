@@ -15,7 +15,7 @@ __global__ void __launch_bounds__(128) k_velfg_only(Geo g, Fields F, float *dfu,
     const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int k = 1 + blockIdx.z;
     if (i > g.im || j > g.jm) return;
-    const UVW q{F.u, F.v, F.w};
+    const UVW q{{}, F.u, F.v, F.w};
     const int c = IX(g, i, j, k);
     float fv, gv, hv = 0.0f, d1, d2, d3 = 0.0f;
     velfg_cell(g, q, i, j, k, fv, gv, hv, d1, d2, d3);

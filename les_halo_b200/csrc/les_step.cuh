@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256) k_uvw_ghosts(Geo g, Fields F) {
 // Sources of the nine strain-rate arrays diu1..9 read by les.f95: computed
 // on the fly from u,v,w (the fused step), or the caller's arrays held in
 // box layout (the les per-routine entry, which receives diu as input).
-struct DiuOnFly {
+struct DiuOnFly : DivIEEE {
     Geo g;
     UVW q;
     __device__ __forceinline__ float d1(int i, int j, int k) const { return diu1_e(g, q, i, j, k); }
@@ -159,7 +159,7 @@ struct DiuOnFly {
     __device__ __forceinline__ float d8(int i, int j, int k) const { return diu8_e(g, q, i, j, k); }
     __device__ __forceinline__ float d9(int i, int j, int k) const { return diu9_e(g, q, i, j, k); }
 };
-struct DiuBoxes {
+struct DiuBoxes : DivIEEE {
     Geo g;
     const float *a[9];
     __device__ __forceinline__ float at(int n, int i, int j, int k) const { return __ldg(&a[n][IX(g, i, j, k)]); }
@@ -242,67 +242,67 @@ __device__ __forceinline__ void visc_cell(const Geo &g, const D &d, const float 
     {  // x-comp, les.f95:170-201
         float evsx2 = SM(i + 1, j, k);
         float evsx1 = SM(i, j, k);
-        float evsy2 = fdiv((dy1[j + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dy1[j] * (fdiv((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
-        float evsy1 = fdiv((dy1[j + 1] * (fdiv((dx1[i + 1] * SM(i, j - 1, k) + dx1[i] * SM(i + 1, j - 1, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dy1[j] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
-        float evsz2 = (dzn[k + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsz1 = (dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dzn[k - 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
-                      (dzn[k - 1] + dzn[k]);
+        float evsy2 = d.xd((dy1[j + 1] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dy1[j] * (d.xd((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsy1 = d.xd((dy1[j + 1] * (d.xd((dx1[i + 1] * SM(i, j - 1, k) + dx1[i] * SM(i + 1, j - 1, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dy1[j] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsz2 = d.zn2(g, (dzn[k + 1] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k] * (d.xd((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))),
+                      k);
+        float evsz1 = d.zn2(g, (dzn[k] * (d.xd((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k - 1] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))),
+                      k - 1);
         float visux2 = (evsx2) * 2.0f * d.d1(i + 1, j, k);
         float visux1 = (evsx1) * 2.0f * d.d1(i, j, k);
         float visuy2 = (evsy2) * (d.d2(i, j + 1, k) + d.d4(i + 1, j, k));
         float visuy1 = (evsy1) * (d.d2(i, j, k) + d.d4(i + 1, j - 1, k));
         float visuz2 = (evsz2) * (d.d3(i, j, k + 1) + d.d7(i + 1, j, k));
         float visuz1 = (evsz1) * (d.d3(i, j, k) + d.d7(i + 1, j, k - 1));
-        vfu = fdiv(visux2 - visux1, dx1[i], g.rdx1[i]) + fdiv(visuy2 - visuy1, dy1[j], g.rdy1[j]) + (visuz2 - visuz1) / dzn[k];
+        vfu = d.xd(visux2 - visux1, dx1[i], g.rdx1[i]) + d.xd(visuy2 - visuy1, dy1[j], g.rdy1[j]) + d.zn(g, visuz2 - visuz1, k);
     }
     {  // y-comp, les.f95:204-235
         float evsy2 = SM(i, j + 1, k);
         float evsy1 = SM(i, j, k);
-        float evsx2 = fdiv((dy1[j + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dy1[j] * (fdiv((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
-        float evsx1 = fdiv((dy1[j + 1] * (fdiv((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1])) +
-                       dy1[j] * (fdiv((dx1[i] * SM(i - 1, j + 1, k) + dx1[i - 1] * SM(i, j + 1, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1]))), dy1[j] + dy1[j + 1], g.rsy[j]);
-        float evsz2 = (dzn[k + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsz1 = (dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dzn[k - 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
-                      (dzn[k - 1] + dzn[k]);
+        float evsx2 = d.xd((dy1[j + 1] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dy1[j] * (d.xd((dx1[i + 1] * SM(i, j + 1, k) + dx1[i] * SM(i + 1, j + 1, k)), dx1[i] + dx1[i + 1], g.rsx[i]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsx1 = d.xd((dy1[j + 1] * (d.xd((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1])) +
+                       dy1[j] * (d.xd((dx1[i] * SM(i - 1, j + 1, k) + dx1[i - 1] * SM(i, j + 1, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1]))), dy1[j] + dy1[j + 1], g.rsy[j]);
+        float evsz2 = d.zn2(g, (dzn[k + 1] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k] * (d.xd((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))),
+                      k);
+        float evsz1 = d.zn2(g, (dzn[k] * (d.xd((dx1[i + 1] * SM(i, j, k - 1) + dx1[i] * SM(i + 1, j, k - 1)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k - 1] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i]))),
+                      k - 1);
         float visvx2 = (evsx2) * (d.d2(i, j + 1, k) + d.d4(i + 1, j, k));
         float visvx1 = (evsx1) * (d.d2(i - 1, j + 1, k) + d.d4(i, j, k));
         float visvy2 = (evsy2) * 2.0f * d.d5(i, j + 1, k);
         float visvy1 = (evsy1) * 2.0f * d.d5(i, j, k);
         float visvz2 = (evsz2) * (d.d6(i, j, k + 1) + d.d8(i, j + 1, k));
         float visvz1 = (evsz1) * (d.d6(i, j, k) + d.d8(i, j + 1, k - 1));
-        vfv = fdiv(visvx2 - visvx1, dx1[i], g.rdx1[i]) + fdiv(visvy2 - visvy1, dy1[j], g.rdy1[j]) + (visvz2 - visvz1) / dzn[k];
+        vfv = d.xd(visvx2 - visvx1, dx1[i], g.rdx1[i]) + d.xd(visvy2 - visvy1, dy1[j], g.rdy1[j]) + d.zn(g, visvz2 - visvz1, k);
     }
     {  // z-comp, les.f95:238-272
         float evsz2 = SM(i, j, k + 1);
         float evsz1 = SM(i, j, k);
-        float evsx2 = (dzn[k + 1] * (fdiv((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
-                       dzn[k] * (fdiv((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsx1 = (dzn[k + 1] * (fdiv((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1])) +
-                       dzn[k] * (fdiv((dx1[i] * SM(i - 1, j, k + 1) + dx1[i - 1] * SM(i, j, k + 1)), dx1[i - 1] + dx1[i], g.rsx[i - 1]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsy2 = (dzn[k + 1] * (fdiv((dy1[j + 1] * SM(i, j, k) + dy1[j] * SM(i, j + 1, k)), dy1[j] + dy1[j + 1], g.rsy[j])) +
-                       dzn[k] * (fdiv((dy1[j + 1] * SM(i, j, k + 1) + dy1[j] * SM(i, j + 1, k + 1)), dy1[j] + dy1[j + 1], g.rsy[j]))) /
-                      (dzn[k] + dzn[k + 1]);
-        float evsy1 = (dzn[k + 1] * (fdiv((dy1[j] * SM(i, j - 1, k) + dy1[j - 1] * SM(i, j, k)), dy1[j - 1] + dy1[j], g.rsy[j - 1])) +
-                       dzn[k] * (fdiv((dy1[j] * SM(i, j - 1, k + 1) + dy1[j - 1] * SM(i, j, k + 1)), dy1[j - 1] + dy1[j], g.rsy[j - 1]))) /
-                      (dzn[k] + dzn[k + 1]);
+        float evsx2 = d.zn2(g, (dzn[k + 1] * (d.xd((dx1[i + 1] * SM(i, j, k) + dx1[i] * SM(i + 1, j, k)), dx1[i] + dx1[i + 1], g.rsx[i])) +
+                       dzn[k] * (d.xd((dx1[i + 1] * SM(i, j, k + 1) + dx1[i] * SM(i + 1, j, k + 1)), dx1[i] + dx1[i + 1], g.rsx[i]))),
+                      k);
+        float evsx1 = d.zn2(g, (dzn[k + 1] * (d.xd((dx1[i] * SM(i - 1, j, k) + dx1[i - 1] * SM(i, j, k)), dx1[i - 1] + dx1[i], g.rsx[i - 1])) +
+                       dzn[k] * (d.xd((dx1[i] * SM(i - 1, j, k + 1) + dx1[i - 1] * SM(i, j, k + 1)), dx1[i - 1] + dx1[i], g.rsx[i - 1]))),
+                      k);
+        float evsy2 = d.zn2(g, (dzn[k + 1] * (d.xd((dy1[j + 1] * SM(i, j, k) + dy1[j] * SM(i, j + 1, k)), dy1[j] + dy1[j + 1], g.rsy[j])) +
+                       dzn[k] * (d.xd((dy1[j + 1] * SM(i, j, k + 1) + dy1[j] * SM(i, j + 1, k + 1)), dy1[j] + dy1[j + 1], g.rsy[j]))),
+                      k);
+        float evsy1 = d.zn2(g, (dzn[k + 1] * (d.xd((dy1[j] * SM(i, j - 1, k) + dy1[j - 1] * SM(i, j, k)), dy1[j - 1] + dy1[j], g.rsy[j - 1])) +
+                       dzn[k] * (d.xd((dy1[j] * SM(i, j - 1, k + 1) + dy1[j - 1] * SM(i, j, k + 1)), dy1[j - 1] + dy1[j], g.rsy[j - 1]))),
+                      k);
         float viswx2 = (evsx2) * (d.d3(i, j, k + 1) + d.d7(i + 1, j, k));
         float viswx1 = (evsx1) * (d.d3(i - 1, j, k + 1) + d.d7(i, j, k));
         float viswy2 = (evsy2) * (d.d6(i, j, k + 1) + d.d8(i, j + 1, k));
         float viswy1 = (evsy1) * (d.d6(i, j - 1, k + 1) + d.d8(i, j, k));
         float viswz2 = (evsz2) * 2.0f * d.d9(i, j, k + 1);
         float viswz1 = (evsz1) * 2.0f * d.d9(i, j, k);
-        vfw = fdiv(viswx2 - viswx1, dx1[i], g.rdx1[i]) + fdiv(viswy2 - viswy1, dy1[j], g.rdy1[j]) + (viswz2 - viswz1) / dzn[k];
+        vfw = d.xd(viswx2 - viswx1, dx1[i], g.rdx1[i]) + d.xd(viswy2 - viswy1, dy1[j], g.rdy1[j]) + d.zn(g, viswz2 - viswz1, k);
     }
 #undef SM
 }

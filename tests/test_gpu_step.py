@@ -46,6 +46,24 @@ def test_warmup_and_steps_bitexact(require_gpu, dims):
     gpu.close()
 
 
+@pytest.mark.parametrize("spacing", [(4.0, 4.0), (3.0, 5.0), (2.5, 4.0)])
+def test_interior_tiles_bitexact(require_gpu, spacing):
+    # a grid with interior 32 x 8 momentum tiles (their ring inside the
+    # domain): power-of-two x/y spacing takes the multiply-only division
+    # path, the others the tested one
+    ip, jp, kp = 100, 40, 20
+    dx, dy = spacing
+    ref, dev = _pair(ip, jp, kp, seed=11, dx=dx, dy=dy)
+    gpu = GpuLes(dev)
+    oracle.ifdata(ref, 1)
+    gpu.warmup(1)
+    _compare(gpu, ref)
+    oracle.run_steps(ref, 1, 3)
+    gpu.step(1, 3)
+    _compare(gpu, ref)
+    gpu.close()
+
+
 def test_power_law_inflow(require_gpu):
     ip, jp, kp = 12, 10, 80
     ref, dev = _pair(ip, jp, kp, seed=3, inflow="power")
