@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
     if (nit <= 0) return;
     constexpr int R = tb_ring(T), RX = tb_ringx(T), TX = tb_tx(T), NS = tb_ns(T), D = kTbDepth, W = 2 * T + 2;
     constexpr int RW4 = kTbRW / 4;  // float4 per region row
-    const int nhs = 2 * nit;
+    const int nhs = (T == 1) ? 2 : 2 * nit;  // a one-iteration pass is never a redo
     const int ty = a.ty, RH = ty + 2 * R, RA4 = RW4 * RH;
     float4 *P = smem4;          // NS plane slots of p
     float4 *Bs = P + NS * RA4;  // NS plane slots of rhs
@@ -214,6 +214,10 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
     }
     // the tile's columns come in whole lanes (RX and TX are multiples of 4)
     const bool lane_tile = (fl[0] & 8) != 0;
+    const bool acc_cells = !redo && ytile && lane_tile;  // this lane's updates enter the residual
+    // x parity of the colour updated at step tau: (pbase + tau) & 1 for every
+    // half-sweep (q = tau - s and nrd = s & 1 move together)
+    const int pbase = (jr0 + y + 1 - ir0) & 1;
     // register window: w[c][m] = column c on plane tau+1-m
     float w[kTbCW][W];
 #pragma unroll
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
 #pragma unroll
         for (int s = 0; s < 2 * T; ++s) {
             const int q = tau - s;
-            const int qlo = (kb == 1) ? 1 : kb + s + 1, qhi = (ke == km) ? km : ke - s - 1;
+            const int qlo = (kb == 1) ? 1 : kb + s + 1, qhi = (ke == km) ? km : ke - s - 1;  // hoisted by the compiler
             const int lo = s + 1;
             if (s < nhs && q >= qlo && q <= qhi && y >= lo && y < RH - lo) {
                 int sq = st1 - 1 - s;
@@ -270,7 +274,7 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
                 const float cnq = CN1K ? a.cn1k[q] : 0.0f;
                 const float cC = CN1K ? 0.0f : g.cnC[q];
                 const bool top = (q == km), bottom = (q == 1);
-                const bool acc = !redo && ytile && lane_tile && q >= k0 && q <= k1;
+                const bool acc = acc_cells && q >= k0 && q <= k1;
                 // update column C (of this half-sweep's colour) given its x neighbours
                 auto upd = [&](auto Cc, float west, float east) {
                     constexpr int C = decltype(Cc)::value;
@@ -296,7 +300,7 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
                     }
                 };
                 // x parity of this colour's cells on the row
-                if (((jr0 + y + q + (s & 1) + 1 - ir0) & 1) == 0) {
+                if (((pbase + tau) & 1) == 0) {
                     // cells 4l, 4l+2; the west neighbour of 4l is column 3 of lane-1
                     const float nb = __shfl_sync(0xffffffffu, w[3][s + 1], lane - 1);
                     upd(std::integral_constant<int, 0>(), nb, w[1][s + 1]);
