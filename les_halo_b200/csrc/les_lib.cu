@@ -334,9 +334,9 @@ dim3 cells_grid(const Geo &g, int i0) {  // i from i0, 32 x 4 blocks, z = k
 les_status enqueue_bondv1(les_ctx *c, int n, bool velnw) {
     const Geo &g = c->geo;
     if (velnw)
-        LAUNCH(c, k_velnw_inflow<true>, cells_grid(g, 0), dim3(32, 4), g, c->F, n, c->prm.ical);
+        LAUNCH(c, k_velnw_inflow<true>, cells_grid(g, 1), dim3(32, 4), g, c->F, n, c->prm.ical);
     else
-        LAUNCH(c, k_velnw_inflow<false>, cells_grid(g, 0), dim3(32, 4), g, c->F, n, c->prm.ical);
+        LAUNCH(c, k_velnw_inflow<false>, cells_grid(g, 1), dim3(32, 4), g, c->F, n, c->prm.ical);
     LAUNCH(c, k_uout_reduce, dim3(cdiv((long long)g.jm * g.km, 256 * 8)), dim3(256), g, c->F.u, c->d_scal);
     LAUNCH(c, k_outflow, dim3(cdiv((long long)g.jm * g.km, 256)), dim3(256), g, c->F, c->d_scal);
     const long long ng = 2LL * g.km * (g.im + 2) + 2LL * (g.jm + 2) * (g.im + 2) + 2LL * (g.jm + 3) * (g.im + 2);

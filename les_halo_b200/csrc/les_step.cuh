@@ -15,13 +15,8 @@ namespace {  // kernels get internal linkage: each .cu has its own copy
 // bondv1.f95:47-59 (ICAL=0).  Cells i in 0..im, j in 1..jm, k in 1..km.
 // VELNW=false gives the bondv1 part alone (ifdata.f95:258); INFLOW=false
 // gives velnw alone (velnw.f95, the per-routine entry).
-template <bool VELNW, bool INFLOW = true>
-__global__ void __launch_bounds__(128) k_velnw_inflow(Geo g, Fields F, int n, int ical) {
-    const int i = blockIdx.x * 32 + threadIdx.x;  // 0..
-    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = 1 + blockIdx.z;
-    if (i > g.im || j > g.jm) return;
-    if (!INFLOW && i == 0) return;
+template <bool VELNW, bool INFLOW>
+__device__ __forceinline__ void velnw_cell(const Geo &g, const Fields &F, int n, int ical, int i, int j, int k) {
     const int c = IX(g, i, j, k);
     const bool bc = INFLOW && ((i <= 1) || (n == 1 && ical == 0));
     if (bc) {
@@ -44,6 +39,18 @@ __global__ void __launch_bounds__(128) k_velnw_inflow(Geo g, Fields F, int n, in
         float pz = (-pc + F.p[IX(g, i, j, k + 1)]) / g.ro / g.dzs[k];
         F.w[c] = F.w[c] + g.dt * (F.h[c] - pz);
     }
+}
+
+// Warps cover i = 1..im from the start of a 128-byte line (box offset 32);
+// the i = 0 inflow column is done by lane 0 of the first block column.
+template <bool VELNW, bool INFLOW = true>
+__global__ void __launch_bounds__(128) k_velnw_inflow(Geo g, Fields F, int n, int ical) {
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 1 + blockIdx.z;
+    if (j > g.jm) return;
+    const int i = 1 + blockIdx.x * 32 + threadIdx.x;
+    if (i <= g.im) velnw_cell<VELNW, INFLOW>(g, F, n, ical, i, j, k);
+    if (INFLOW && blockIdx.x == 0 && threadIdx.x == 0) velnw_cell<VELNW, INFLOW>(g, F, n, ical, 0, j, k);
 }
 
 // bondv1.f95:67-74: aaa = max(0, u(im,:,:)), bbb = min(0, u(im,:,:)).
