@@ -720,10 +720,11 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
         return cleanup(fail(LES_ERR_NOMEM, "tables"));
     if (cudaMalloc(&c->d_scal, sizeof(Scal)) != cudaSuccess) return cleanup(fail(LES_ERR_NOMEM, "scalars"));
     cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream);
-    // reduction grid: 32x8 blocks over (i,j), k split so there are >= 4 blocks per SM
+    // reduction grid: 32x8 blocks over (i,j), k split into chunks of at most
+    // 8 planes (short per-thread loops keep many loads in flight)
     c->red_gx = cdiv(ip, kRedBX);
     c->red_gy = cdiv(jp, kRedBY);
-    int nk = cdiv(4 * 148, (long long)c->red_gx * c->red_gy);
+    int nk = std::max(cdiv(4 * 148, (long long)c->red_gx * c->red_gy), cdiv(kp, 8));
     nk = nk < 1 ? 1 : (nk > kp ? kp : nk);
     c->red_kchunk = cdiv(kp, nk);
     c->red_nk = cdiv(kp, c->red_kchunk);

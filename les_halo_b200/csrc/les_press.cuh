@@ -26,9 +26,17 @@ __global__ void __launch_bounds__(kRedNT) k_rhs(Geo g, Fields F, int kchunk, Fix
     if (i <= g.im && j <= g.jm) {
         const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn;
         for (int k = k0; k <= k1; ++k) {
+            // every load first (no store below writes a location any thread
+            // reads), then the bondfg ghost writes, then rhs
             const int c = IX(g, i, j, k);
             const float fc = F.f[c], gc = F.g[c];
             float hc = F.h[c];
+            const float fm = (i == 1) ? fc : F.f[IX(g, i - 1, j, k)];
+            const float gm = (j == 1) ? F.g[IX(g, i, g.jm, k)] : F.g[IX(g, i, j - 1, k)];
+            const float hm = (k == 1) ? 0.0f : F.h[IX(g, i, j, k - 1)];
+            const float um = F.u[IX(g, i - 1, j, k)], uc = F.u[c];
+            const float vm = F.v[IX(g, i, j - 1, k)], vc = F.v[c];
+            const float wm = F.w[IX(g, i, j, k - 1)], wc = F.w[c];
             // bondfg: f(0,j,k)=f(1,j,k); g(i,0,k)=g(i,jm,k); h(i,j,0)=h(i,j,km)=0
             if (i == 1) F.f[IX(g, 0, j, k)] = fc;
             if (j == g.jm) F.g[IX(g, i, 0, k)] = gc;
@@ -37,11 +45,7 @@ __global__ void __launch_bounds__(kRedNT) k_rhs(Geo g, Fields F, int kchunk, Fix
                 hc = 0.0f;
             }
             if (k == 1) F.h[IX(g, i, j, 0)] = 0.0f;
-            const float fm = (i == 1) ? fc : F.f[IX(g, i - 1, j, k)];
-            const float gm = (j == 1) ? F.g[IX(g, i, g.jm, k)] : F.g[IX(g, i, j - 1, k)];
-            const float hm = (k == 1) ? 0.0f : F.h[IX(g, i, j, k - 1)];
-            float r = (-F.u[IX(g, i - 1, j, k)] + F.u[c]) / dx1[i] + (-F.v[IX(g, i, j - 1, k)] + F.v[c]) / dy1[j] +
-                      (-F.w[IX(g, i, j, k - 1)] + F.w[c]) / dzn[k];
+            float r = (-um + uc) / dx1[i] + (-vm + vc) / dy1[j] + (-wm + wc) / dzn[k];
             r = (fc - fm) / dx1[i] + (gc - gm) / dy1[j] + (hc - hm) / dzn[k] + r / g.dt;
             F.rhs[c] = r;
             acc += fix_term(dx1[i] * dy1[j] * dzn[k] * r, bad);
@@ -257,20 +261,21 @@ __global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *p, const fl
     if (i > g.im || j > g.jm) return;
     const float *src = s->pbuf ? p1 : p;
     const float val = src[IX(g, i, j, k)] - s->pav;
-    int is[2], js[2], ks[2];
-    int ni = 0, nj = 0, nk = 0;
-    is[ni++] = i;
-    if (i == 1) is[ni++] = 0;
-    if (i == g.im) is[ni++] = g.im + 1;  // (im >= 2 so at most one extra)
-    js[nj++] = j;
-    if (j == g.jm) js[nj++] = 0;
-    if (j == 1) js[nj++] = g.jm + 1;
-    ks[nk++] = k;
-    if (k == 1) ks[nk++] = 0;
-    if (k == g.km) ks[nk++] = g.km + 1;
-    for (int a = 0; a < ni; ++a)
-        for (int b = 0; b < nj; ++b)
-            for (int c = 0; c < nk; ++c) p[IX(g, is[a], js[b], ks[c])] = val;
+    // the cell and its boundp1/boundp2 copies: at most one extra i, j and k
+    // (im, jm >= 2, km >= 3)
+    const int ie = (i == 1) ? 0 : (i == g.im ? g.im + 1 : -9);
+    const int je = (j == g.jm) ? 0 : (j == 1 ? g.jm + 1 : -9);
+    const int ke = (k == 1) ? 0 : (k == g.km ? g.km + 1 : -9);
+    auto put = [&](int kk) {
+        p[IX(g, i, j, kk)] = val;
+        if (ie != -9) p[IX(g, ie, j, kk)] = val;
+        if (je != -9) {
+            p[IX(g, i, je, kk)] = val;
+            if (ie != -9) p[IX(g, ie, je, kk)] = val;
+        }
+    };
+    put(k);
+    if (ke != -9) put(ke);
 }
 
 // Per-step scalars reset and the centre probe of press.f95:183-187.

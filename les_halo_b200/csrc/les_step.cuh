@@ -26,18 +26,24 @@ __device__ __forceinline__ void velnw_cell(const Geo &g, const Fields &F, int n,
         return;
     }
     if (!VELNW) return;
-    const float pc = F.p[c];
+    // every load before the first store (the compiler cannot move loads
+    // across stores to possibly aliasing fields)
+    const bool wz = (k <= g.km - 1);
+    const float pc = F.p[c], pe = F.p[IX(g, i + 1, j, k)], pn = F.p[IX(g, i, j + 1, k)];
+    const float pu = wz ? F.p[IX(g, i, j, k + 1)] : 0.0f;
+    const float uc = F.u[c], vc = F.v[c], wc = wz ? F.w[c] : 0.0f;
+    const float fc = F.f[c], gc = F.g[c], hc = wz ? F.h[c] : 0.0f;
     {
-        float pz = (-pc + F.p[IX(g, i + 1, j, k)]) / g.ro / g.dxs[i];
-        F.u[c] = F.u[c] + g.dt * (F.f[c] - pz);
+        float pz = (-pc + pe) / g.ro / g.dxs[i];
+        F.u[c] = uc + g.dt * (fc - pz);
     }
     {
-        float pz = (-pc + F.p[IX(g, i, j + 1, k)]) / g.ro / g.dys[j];
-        F.v[c] = F.v[c] + g.dt * (F.g[c] - pz);
+        float pz = (-pc + pn) / g.ro / g.dys[j];
+        F.v[c] = vc + g.dt * (gc - pz);
     }
-    if (k <= g.km - 1) {
-        float pz = (-pc + F.p[IX(g, i, j, k + 1)]) / g.ro / g.dzs[k];
-        F.w[c] = F.w[c] + g.dt * (F.h[c] - pz);
+    if (wz) {
+        float pz = (-pc + pu) / g.ro / g.dzs[k];
+        F.w[c] = wc + g.dt * (hc - pz);
     }
 }
 
