@@ -32,7 +32,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "time-step Mpts/s: plain vs FP64-refined press at ≤1e-5 err; adjoint/fwd cost"
 WORKLOAD = dict(ip=600, jp=600, kp=120, plan_area=0.35, h_max=120.0, dt=0.05, nmaxp=50, seed=1)
-SOR_BYTES_PER_CELL_PER_ITER = 12.0   # p read, rhs read, p write per SOR iteration (SURVEY 8d accounting)
+SOR_BYTES_PER_CELL_PER_ITER = 12.0   # algorithmic bytes of one SOR iteration: p read, rhs read, p write
 STEP_BYTES_PER_CELL = 204.0 + 12.0 * 50  # algorithmic bytes per cell per step at 50 SOR iterations
 
 
@@ -41,6 +41,20 @@ def _dist():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+def job_rates(ms_total, e2e_s, cells, steps, e2e_steps, ws, dist=None, device="cpu"):
+    """Max-over-ranks device and end-to-end times and the whole-job rates in
+    Mpts/s: every rank advances its own replica of `cells` cells, so the job
+    moves ws * cells per step in the slowest rank's time."""
+    import torch
+    t = torch.tensor([ms_total, e2e_s], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_total, e2e_s = float(t[0]), float(t[1])
+    value = ws * cells * steps / (ms_total / 1e3) / 1e6
+    e2e_val = ws * cells * e2e_steps / e2e_s / 1e6
+    return ms_total, e2e_s, value, e2e_val
 
 
 def _peaks():
@@ -268,13 +282,9 @@ def run_ours(args):
         abi.check(L.les_last_metrics(gpu.ctx, C.byref(mrec)))
     e2e_s = time.perf_counter() - t0
 
-    times = torch.tensor([ms_total, e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms_total, e2e_s = float(times[0]), float(times[1])
+    ms_total, e2e_s, value, e2e_val = job_rates(ms_total, e2e_s, cells, args.steps, e2e_steps, ws,
+                                                dist, "cuda")
     ms_step = ms_total / args.steps
-    value = ws * cells * args.steps / (ms_total / 1e3) / 1e6
-    e2e_val = ws * cells * e2e_steps / e2e_s / 1e6
 
     sor_launch_ms = float(np.mean(phases[:, 5])) if not args.profile else float("nan")
     peak, peak_kind = _peaks()
