@@ -215,6 +215,16 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
     // the tile's columns come in whole lanes (RX and TX are multiples of 4)
     const bool lane_tile = (fl[0] & 8) != 0;
     const bool acc_cells = !redo && ytile && lane_tile;  // this lane's updates enter the residual
+    // bit 4s+c: column c of this lane is updated by half-sweep s (inside the
+    // region shrunk by s+1 and inside 1..im)
+    unsigned vmask = 0u;
+#pragma unroll
+    for (int s = 0; s < 2 * T; ++s)
+#pragma unroll
+        for (int c = 0; c < kTbCW; ++c) {
+            const int x = kTbCW * lane + c;
+            if (x >= s + 1 && x < kTbRW - s - 1 && (fl[c] & 1)) vmask |= 1u << (kTbCW * s + c);
+        }
     // x parity of the colour updated at step tau: (pbase + tau) & 1 for every
     // half-sweep (q = tau - s and nrd = s & 1 move together)
     const int pbase = (jr0 + y + 1 - ir0) & 1;
@@ -278,8 +288,9 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
                 // update column C (of this half-sweep's colour) given its x neighbours
                 auto upd = [&](auto Cc, float west, float east) {
                     constexpr int C = decltype(Cc)::value;
-                    const int x = kTbCW * lane + C;
-                    if (x < lo || x >= kTbRW - lo || !(fl[C] & 1)) return;
+                    // computed on every lane; kept where the cell is in the
+                    // half-sweep's region (no divergent branch)
+                    const bool ok = (vmask >> (kTbCW * s + C)) & 1u;
                     const float pc = w[C][s + 1];
                     const float pe = (fl[C] & 4) ? pc : east;
                     const float pw = (fl[C] & 2) ? pc : west;
@@ -289,8 +300,8 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
                     const float reltmp = omega * (cn1 * (c2l[C] * pe + c2s[C] * pw + c3l * pn4[C] + c3s * ps4[C] +
                                                          c4l * pu + c4s * pd - (b4[C] - rhsav)) -
                                                   pc);
-                    w[C][s + 1] = pc + reltmp;
-                    if (acc) {
+                    w[C][s + 1] = ok ? pc + reltmp : pc;
+                    if (acc && ok) {
                         if (s < 2)
                             fix_add_nonneg(reltmp * reltmp, h0, l0, bad);
                         else if (s < 4)
