@@ -82,12 +82,14 @@ struct TbArgs {
 };
 
 // Exact Q63.64 term (les_fix.h) of a non-negative float below 2^62: the
-// integer part and the fraction scaled by 2^64, both exact in FP64; a term
-// below 1 needs only the fraction.
+// integer part and the fraction scaled by 2^64, both exact in FP64.  A term
+// below 1 is the fraction alone, and x * 2^64 is then exact in FP32 (a
+// power-of-two scaling inside the normal range), so one truncating
+// conversion gives it.
 __device__ __forceinline__ void fix_add_nonneg(float x, unsigned long long &hi, unsigned long long &lo, int &bad) {
     unsigned long long fr, ip;
     if (x < 1.0f) {
-        fr = __double2ull_rz((double)x * 18446744073709551616.0);
+        fr = __float2ull_rz(x * 18446744073709551616.0f);
         ip = 0ull;
     } else if (x < 4.611686018427388e18f) {
         const double d = (double)x;
