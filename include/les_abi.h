@@ -285,8 +285,12 @@ les_status les_boundp2_(const int *jm, const int *im, float *p, const int *km);
  * arrays the caller already holds on the device (same Fortran layouts and
  * argument order as les_press_; scalars by value), enqueued on `stream`
  * (a cudaStream_t or NULL); rhsav (a device float, may be NULL) receives
- * the average.  Allocates no device memory: the per-block partial sums sit
- * in a 256 KiB static __device__ array, so ceil(im/32) * ceil(jm/8) must be
+ * the average.  For hosts that cannot allocate device memory in their time
+ * loop: one whose memory pool already holds the free device memory (a
+ * cudaMalloc would fail), or one that keeps other streams busy (cudaFree
+ * synchronises the whole device).  Allocates no device memory: the
+ * per-block partial sums sit in a 256 KiB static __device__ array that every
+ * GPU loading the library holds until exit, so ceil(im/32) * ceil(jm/8) must be
  * at most 5456 (e.g. im = jm = 1024 needs 4096); larger grids are rejected
  * with LES_ERR_DIMS before any device work.  The first call on each device
  * looks up the scratch address; make it outside any stream capture.  Calls

@@ -2,8 +2,12 @@
 // subtraction) on arrays the caller already holds on the device, allocating
 // no device memory.
 //
-// The exact global sums need per-block partials.  They live in one
-// file-scope static __device__ array (kScratchBytes); the host looks up its
+// It serves hosts that cannot allocate in their time loop: a host whose
+// memory pool already holds the free device memory (cudaMalloc fails there)
+// or one that overlaps work on other streams (cudaFree synchronises the
+// device).  The exact global sums need per-block partials.  They live in one
+// file-scope static __device__ array (kScratchBytes, held by every GPU that
+// loads the library until the process exits); the host looks up its
 // address once per device with cudaGetSymbolAddress and never calls
 // cudaMalloc, cudaFree or a library routine that allocates.  Layout of the
 // scratch:

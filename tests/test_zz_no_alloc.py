@@ -47,9 +47,11 @@ def _oracle_rhsav(ip, jp, kp, dt, base):
     args = [FL.ptr(a[n]) for n in NAMES]
     out = C.c_float()
     fn = L.oracle_press
+    i, f, p = C.c_int, C.c_float, C.c_void_p
+    # the full signature: pointers must not go through ctypes' default int
+    fn.argtypes = [i, i, i] + [p] * 10 + [f] + [p] * 8 + [i, i, p, p, p]
     fn.restype = C.c_int
-    fn(C.c_int(kp), C.c_int(jp), C.c_int(ip), *args[:10], C.c_float(dt), *args[10:], C.c_int(4),
-       C.c_int(10), None, C.byref(out), None)
+    fn(kp, jp, ip, *args[:10], dt, *args[10:], 4, 10, None, C.byref(out), None)
     return out.value
 
 
