@@ -348,14 +348,88 @@ __device__ __forceinline__ void tile_plane(const Geo &g, const Q &q, float *dst,
 
 // shared memory: two face-value planes (18 or 9 values), diu7/diu8 of the
 // plane below, and the u,v,w band slots
+// (the viscosity kernel adds its sm planes and edge values, kViscArrays
+// position arrays)
+constexpr int kViscArrays = 11;
 __host__ __device__ constexpr size_t mom_smem(bool diu_only) {
-    return sizeof(float) * (2 * (diu_only ? 9 : NV) * kMPOS + 2 * kMPOS + kBS * 3 * kBA);
+    return sizeof(float) *
+           (2 * (diu_only ? 9 : NV) * kMPOS + 2 * kMPOS + kBS * 3 * kBA + (diu_only ? kViscArrays * kMPOS : 0));
+}
+
+// Shared-memory view of the viscosity edge values around plane k for
+// visc_tile, one value per ring position.  With A = the x-weighted sm
+// average at (i+1/2, j) and B = the y-weighted one at (i, j+1/2) of a plane
+// (les.f95:170-272): exy = y-average of A, fxy = the same weights on A at
+// j-1 and j (les.f95's evsy1 of the u equation), exz = z-average of A
+// between k and k+1 (exz0: between k-1 and k), eyz = z-average of B.
+struct ViscView {
+    const float *s0, *s1;  // sm on planes k, k+1
+    const float *exy, *fxy, *exz0, *exz1, *eyz;
+};
+
+// les.f95:170-274 viscous flux divergence at one cell, the edge values read
+// from the tile (same expressions as visc_cell, evaluated once per position).
+template <class TV>
+__device__ __forceinline__ void visc_tile(const Geo &g, const TV &d, const ViscView &v, int i, int j, int k, float &vfu,
+                                          float &vfv, float &vfw) {
+    const float *dx1 = g.dx1, *dy1 = g.dy1;
+    const int p = d.pos(i, j);
+    {  // x-comp, les.f95:170-201
+        float evsx2 = v.s0[p + 1];
+        float evsx1 = v.s0[p];
+        float evsy2 = v.exy[p];
+        float evsy1 = v.fxy[p];
+        float evsz2 = v.exz1[p];
+        float evsz1 = v.exz0[p];
+        float visux2 = (evsx2) * 2.0f * d.d1(i + 1, j, k);
+        float visux1 = (evsx1) * 2.0f * d.d1(i, j, k);
+        float visuy2 = (evsy2) * (d.d2(i, j + 1, k) + d.d4(i + 1, j, k));
+        float visuy1 = (evsy1) * (d.d2(i, j, k) + d.d4(i + 1, j - 1, k));
+        float visuz2 = (evsz2) * (d.d3(i, j, k + 1) + d.d7(i + 1, j, k));
+        float visuz1 = (evsz1) * (d.d3(i, j, k) + d.d7(i + 1, j, k - 1));
+        vfu = d.xd(visux2 - visux1, dx1[i], g.rdx1[i]) + d.xd(visuy2 - visuy1, dy1[j], g.rdy1[j]) +
+              d.zn(g, visuz2 - visuz1, k);
+    }
+    {  // y-comp, les.f95:204-235
+        float evsy2 = v.s0[p + kMEX];
+        float evsy1 = v.s0[p];
+        float evsx2 = v.exy[p];
+        float evsx1 = v.exy[p - 1];
+        float evsz2 = v.exz1[p];
+        float evsz1 = v.exz0[p];
+        float visvx2 = (evsx2) * (d.d2(i, j + 1, k) + d.d4(i + 1, j, k));
+        float visvx1 = (evsx1) * (d.d2(i - 1, j + 1, k) + d.d4(i, j, k));
+        float visvy2 = (evsy2) * 2.0f * d.d5(i, j + 1, k);
+        float visvy1 = (evsy1) * 2.0f * d.d5(i, j, k);
+        float visvz2 = (evsz2) * (d.d6(i, j, k + 1) + d.d8(i, j + 1, k));
+        float visvz1 = (evsz1) * (d.d6(i, j, k) + d.d8(i, j + 1, k - 1));
+        vfv = d.xd(visvx2 - visvx1, dx1[i], g.rdx1[i]) + d.xd(visvy2 - visvy1, dy1[j], g.rdy1[j]) +
+              d.zn(g, visvz2 - visvz1, k);
+    }
+    {  // z-comp, les.f95:238-272
+        float evsz2 = v.s1[p];
+        float evsz1 = v.s0[p];
+        float evsx2 = v.exz1[p];
+        float evsx1 = v.exz1[p - 1];
+        float evsy2 = v.eyz[p];
+        float evsy1 = v.eyz[p - kMEX];
+        float viswx2 = (evsx2) * (d.d3(i, j, k + 1) + d.d7(i + 1, j, k));
+        float viswx1 = (evsx1) * (d.d3(i - 1, j, k + 1) + d.d7(i, j, k));
+        float viswy2 = (evsy2) * (d.d6(i, j, k + 1) + d.d8(i, j + 1, k));
+        float viswy1 = (evsy1) * (d.d6(i, j - 1, k + 1) + d.d8(i, j, k));
+        float viswz2 = (evsz2) * 2.0f * d.d9(i, j, k + 1);
+        float viswz1 = (evsz1) * 2.0f * d.d9(i, j, k);
+        vfw = d.xd(viswx2 - viswx1, dx1[i], g.rdx1[i]) + d.xd(viswy2 - viswy1, dy1[j], g.rdy1[j]) +
+              d.zn(g, viswz2 - viswz1, k);
+    }
 }
 
 // Shared prologue/march of both momentum kernels: stage u,v,w planes, fill
 // the face-value ring plane by plane, call `cell` for every tile cell.
-template <bool DIU_ONLY, bool BAND, bool INTERIOR, bool P2, class CellFn>
-__device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn cell) {
+// `pre(k)` runs at the top of plane k's iteration: the cell's global inputs
+// loaded there arrive while the plane's face values are being filled.
+template <bool DIU_ONLY, bool BAND, bool INTERIOR, bool P2, class PreFn, class CellFn>
+__device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn pre, CellFn cell) {
     extern __shared__ float sh[];
     constexpr int NVU = DIU_ONLY ? 9 : NV;
     float *const s0 = sh, *const s1 = sh + NVU * kMPOS;  // the two face-value plane slots
@@ -381,19 +455,77 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, CellFn 
         cp_async_wait<0>();
         __syncthreads();
     }
+    // viscosity edge values (DIU_ONLY: the viscosity kernel): sm planes and
+    // A, B, exz by plane parity, exy, fxy, eyz of the current plane.  Reads
+    // at p+-1 and p+-kMEX past a position array's ends land in neighbouring
+    // arrays and only feed positions no cell uses.
+    float *vS = band + kBS * 3 * kBA, *vA = vS + 2 * kMPOS, *vB = vA + 2 * kMPOS, *vXZ = vB + 2 * kMPOS;
+    float *vXY = vXZ + 2 * kMPOS, *vFXY = vXY + kMPOS, *vYZ = vFXY + kMPOS;
+    auto stage_sm = [&](int kk) {  // sm of plane kk into slot kk&1
+        float *dst = vS + (kk & 1) * kMPOS;
+        for (int p = threadIdx.x; p < kMPOS; p += kMNT) dst[p] = F.sm[IX(g, ib + p % kMEX, jb + p / kMEX, kk)];
+    };
+    // A and B of plane kk from its staged sm (les.f95:179-185 inner terms)
+    auto plane_ab = [&](const DivPlane<P2> &dv, int kk, bool with_b) {
+        const float *S = vS + (kk & 1) * kMPOS;
+        float *A = vA + (kk & 1) * kMPOS, *B = vB + (kk & 1) * kMPOS;
+        for (int p = threadIdx.x; p < kMPOS; p += kMNT) {
+            const int i = ib + p % kMEX, j = jb + p / kMEX;
+            A[p] = dv.xd((g.dx1[i + 1] * S[p] + g.dx1[i] * S[p + 1]), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
+            if (with_b)
+                B[p] = dv.xd((g.dy1[j + 1] * S[p] + g.dy1[j] * S[p + kMEX]), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
+        }
+    };
+    if (DIU_ONLY) {
+        stage_sm(0);
+        stage_sm(1);
+        __syncthreads();
+        const DivPlane<P2> d0(g, 0), d1(g, 1);
+        plane_ab(d0, 0, false);
+        plane_ab(d1, 1, true);
+        __syncthreads();
+        const float *A0 = vA, *A1 = vA + kMPOS;
+        for (int p = threadIdx.x; p < kMPOS; p += kMNT)
+            vXZ[p] = d0.zn2(g, g.dzn[1] * A0[p] + g.dzn[0] * A1[p], 0);
+    }
     fill(s0, 0, false);
     fill(s1, 1, false);
     __syncthreads();
     for (int k = 1; k <= g.km; ++k) {
+        pre(k);
         if (BAND) {  // plane k+3 streams in while plane k+1 is filled from k..k+2
             if (k + 3 <= g.km + 2) bc.load(band, k + 3);
             cp_async_commit();
         }
         // slot (k+1)&1 holds plane k-1: keep its diu7/diu8, then plane k+1
         fill(slot((k + 1) & 1), k + 1, true);
+        if (DIU_ONLY) stage_sm(k + 1);
         __syncthreads();
         const TileView<P2> t(g, slot(k & 1), slot((k + 1) & 1), prv7, prv8, ib, jb, k);
-        cell(t, k);
+        ViscView vv{};
+        if (DIU_ONLY) {
+            // A, B of plane k+1; exz, eyz between k and k+1; exy, fxy of k
+            const float *S1 = vS + ((k + 1) & 1) * kMPOS;
+            const float *A0 = vA + (k & 1) * kMPOS, *B0 = vB + (k & 1) * kMPOS;
+            float *A1 = vA + ((k + 1) & 1) * kMPOS, *B1 = vB + ((k + 1) & 1) * kMPOS;
+            float *XZ = vXZ + (k & 1) * kMPOS;
+            for (int p = threadIdx.x; p < kMPOS; p += kMNT) {
+                const int i = ib + p % kMEX, j = jb + p / kMEX;
+                const float a1 =
+                    t.xd((g.dx1[i + 1] * S1[p] + g.dx1[i] * S1[p + 1]), g.dx1[i] + g.dx1[i + 1], g.rsx[i]);
+                const float b1 =
+                    t.xd((g.dy1[j + 1] * S1[p] + g.dy1[j] * S1[p + kMEX]), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
+                A1[p] = a1;
+                B1[p] = b1;
+                XZ[p] = t.zn2(g, (g.dzn[k + 1] * (A0[p]) + g.dzn[k] * (a1)), k);
+                vYZ[p] = t.zn2(g, (g.dzn[k + 1] * (B0[p]) + g.dzn[k] * (b1)), k);
+                vXY[p] = t.xd((g.dy1[j + 1] * (A0[p]) + g.dy1[j] * (A0[p + kMEX])), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
+                vFXY[p] = t.xd((g.dy1[j + 1] * (A0[p - kMEX]) + g.dy1[j] * (A0[p])), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
+            }
+            __syncthreads();
+            vv = ViscView{vS + (k & 1) * kMPOS, S1, vXY, vFXY, vXZ + ((k + 1) & 1) * kMPOS, XZ, vYZ};
+        }
+        cell(t, k, vv);
         if (BAND) cp_async_wait<0>();
         __syncthreads();
     }
@@ -413,22 +545,46 @@ template <bool BAND, bool P2>
 __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
     const bool mine = (i <= g.im && j <= g.jm);
-    auto cell = [&](const TileView<P2> &t, int k) {
+    // the cell's own inputs of plane k (feedbf.f95:38-66, velFG's h), loaded
+    // ahead by pre(k); only this thread writes them
+    float h0 = 0, u0 = 0, v0 = 0, w0 = 0, us0 = 0, vs0 = 0, ws0 = 0, bm0 = 0, cm0 = 0, dm0 = 0;
+    auto pre = [&](int k) {
         if (!mine) return;
         const int c = IX(g, i, j, k);
-        float fv, gv, hv = F.h[c];
+        h0 = F.h[c];
+        u0 = __ldg(&F.u[c]);
+        v0 = __ldg(&F.v[c]);
+        w0 = __ldg(&F.w[c]);
+        us0 = F.usum[c];
+        vs0 = F.vsum[c];
+        ws0 = F.wsum[c];
+        bm0 = __ldg(&F.bmask[c]);
+        cm0 = __ldg(&F.cmask[c]);
+        dm0 = __ldg(&F.dmask[c]);
+    };
+    auto cell = [&](const TileView<P2> &t, int k, const ViscView &) {
+        if (!mine) return;
+        const int c = IX(g, i, j, k);
+        float fv, gv, hv = h0;
         velfg_tile(g, t, i, j, k, fv, gv, hv);
-        float fx, fy, fz;
-        feedbf_cell(g, F, c, __ldg(&F.u[c]), __ldg(&F.v[c]), __ldg(&F.w[c]), fx, fy, fz);
-        F.f[c] = fv + fx;
-        F.g[c] = gv + fy;
-        F.h[c] = hv + fz;
+        // feedbf.f95:38-66 (feedbf_cell with the inputs already loaded)
+        const float us = (us0 + u0) * bm0;
+        const float vs = (vs0 + v0) * cm0;
+        const float ws = (ws0 + w0) * dm0;
+        F.usum[c] = us;
+        F.vsum[c] = vs;
+        F.wsum[c] = ws;
+        float f1x = g.alpha * us * g.dt, f1y = g.alpha * vs * g.dt, f1z = g.alpha * ws * g.dt;
+        float f2x = g.beta * u0 * bm0, f2y = g.beta * v0 * cm0, f2z = g.beta * w0 * dm0;
+        F.f[c] = fv + (f1x + f2x);
+        F.g[c] = gv + (f1y + f2y);
+        F.h[c] = hv + (f1z + f2z);
         F.sm[c] = sgs_sm(g, t, i, j, k);
     };
     if (tile_interior(g))
-        mom_march<false, BAND, true, P2>(g, F, cell);
+        mom_march<false, BAND, true, P2>(g, F, pre, cell);
     else
-        mom_march<false, BAND, false, P2>(g, F, cell);
+        mom_march<false, BAND, false, P2>(g, F, pre, cell);
 }
 
 // les.f95:170-274 viscous terms (+ adam.f95:32-46) for a 32 x 8 tile, all k.
@@ -436,16 +592,31 @@ template <bool ADAM, bool BAND, bool P2>
 __global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
     const bool mine = (i <= g.im && j <= g.jm);
-    auto cell = [&](const TileView<P2> &t, int k) {
+    // the cell's f, g, h (and fold, gold, hold) of plane k, loaded ahead by
+    // pre(k); only this thread writes them
+    float f0 = 0, g0 = 0, hh0 = 0, fo0 = 0, go0 = 0, ho0 = 0;
+    auto pre = [&](int k) {
+        if (!mine) return;
+        const int c = IX(g, i, j, k);
+        f0 = F.f[c];
+        g0 = F.g[c];
+        hh0 = F.h[c];
+        if (ADAM) {
+            fo0 = F.fold[c];
+            go0 = F.gold[c];
+            ho0 = F.hold[c];
+        }
+    };
+    auto cell = [&](const TileView<P2> &t, int k, const ViscView &vv) {
         if (!mine) return;
         float vfu, vfv, vfw;
-        visc_cell(g, t, F.sm, i, j, k, vfu, vfv, vfw);
+        visc_tile(g, t, vv, i, j, k, vfu, vfv, vfw);
         const int c = IX(g, i, j, k);
-        const float fv = F.f[c] + vfu, gv = F.g[c] + vfv, hv = F.h[c] + vfw;
+        const float fv = f0 + vfu, gv = g0 + vfv, hv = hh0 + vfw;
         if (ADAM) {
-            F.f[c] = 1.5f * fv - 0.5f * F.fold[c];
-            F.g[c] = 1.5f * gv - 0.5f * F.gold[c];
-            F.h[c] = 1.5f * hv - 0.5f * F.hold[c];
+            F.f[c] = 1.5f * fv - 0.5f * fo0;
+            F.g[c] = 1.5f * gv - 0.5f * go0;
+            F.h[c] = 1.5f * hv - 0.5f * ho0;
             F.fold[c] = fv;
             F.gold[c] = gv;
             F.hold[c] = hv;
@@ -456,9 +627,9 @@ __global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
         }
     };
     if (tile_interior(g))
-        mom_march<true, BAND, true, P2>(g, F, cell);
+        mom_march<true, BAND, true, P2>(g, F, pre, cell);
     else
-        mom_march<true, BAND, false, P2>(g, F, cell);
+        mom_march<true, BAND, false, P2>(g, F, pre, cell);
 }
 
 }  // namespace
