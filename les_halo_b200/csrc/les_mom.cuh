@@ -65,6 +65,10 @@ __device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc));
 }
+__device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -350,7 +354,7 @@ __device__ __forceinline__ void tile_plane(const Geo &g, const Q &q, float *dst,
 // plane below, and the u,v,w band slots
 // (the viscosity kernel adds its sm planes and edge values, kViscArrays
 // position arrays)
-constexpr int kViscArrays = 11;
+constexpr int kViscArrays = 12;
 __host__ __device__ constexpr size_t mom_smem(bool diu_only) {
     return sizeof(float) *
            (2 * (diu_only ? 9 : NV) * kMPOS + 2 * kMPOS + kBS * 3 * kBA + (diu_only ? kViscArrays * kMPOS : 0));
@@ -455,19 +459,22 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
         cp_async_wait<0>();
         __syncthreads();
     }
-    // viscosity edge values (DIU_ONLY: the viscosity kernel): sm planes and
-    // A, B, exz by plane parity, exy, fxy, eyz of the current plane.  Reads
-    // at p+-1 and p+-kMEX past a position array's ends land in neighbouring
-    // arrays and only feed positions no cell uses.
-    float *vS = band + kBS * 3 * kBA, *vA = vS + 2 * kMPOS, *vB = vA + 2 * kMPOS, *vXZ = vB + 2 * kMPOS;
+    // viscosity edge values (DIU_ONLY: the viscosity kernel): sm planes by
+    // plane mod 3 (one arriving by cp.async while two are in use), A, B, exz
+    // by plane parity, exy, fxy, eyz of the current plane.  Reads at p+-1 and
+    // p+-kMEX past a position array's ends land in neighbouring arrays and
+    // only feed positions no cell uses.
+    float *vS = band + kBS * 3 * kBA, *vA = vS + 3 * kMPOS, *vB = vA + 2 * kMPOS, *vXZ = vB + 2 * kMPOS;
     float *vXY = vXZ + 2 * kMPOS, *vFXY = vXY + kMPOS, *vYZ = vFXY + kMPOS;
-    auto stage_sm = [&](int kk) {  // sm of plane kk into slot kk&1
-        float *dst = vS + (kk & 1) * kMPOS;
-        for (int p = threadIdx.x; p < kMPOS; p += kMNT) dst[p] = F.sm[IX(g, ib + p % kMEX, jb + p / kMEX, kk)];
+    auto sm_slot = [&](int kk) { return vS + (kk % 3) * kMPOS; };
+    auto stage_sm = [&](int kk) {  // issue the copies of sm plane kk into its slot
+        float *dst = sm_slot(kk);
+        for (int p = threadIdx.x; p < kMPOS; p += kMNT)
+            cp_async4(dst + p, F.sm + IX(g, ib + p % kMEX, jb + p / kMEX, kk));
     };
     // A and B of plane kk from its staged sm (les.f95:179-185 inner terms)
     auto plane_ab = [&](const DivPlane<P2> &dv, int kk, bool with_b) {
-        const float *S = vS + (kk & 1) * kMPOS;
+        const float *S = sm_slot(kk);
         float *A = vA + (kk & 1) * kMPOS, *B = vB + (kk & 1) * kMPOS;
         for (int p = threadIdx.x; p < kMPOS; p += kMNT) {
             const int i = ib + p % kMEX, j = jb + p / kMEX;
@@ -479,6 +486,9 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
     if (DIU_ONLY) {
         stage_sm(0);
         stage_sm(1);
+        stage_sm(2);
+        cp_async_commit();
+        cp_async_wait<0>();
         __syncthreads();
         const DivPlane<P2> d0(g, 0), d1(g, 1);
         plane_ab(d0, 0, false);
@@ -499,13 +509,14 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
         }
         // slot (k+1)&1 holds plane k-1: keep its diu7/diu8, then plane k+1
         fill(slot((k + 1) & 1), k + 1, true);
-        if (DIU_ONLY) stage_sm(k + 1);
+        if (DIU_ONLY && k + 2 <= g.km + 1) stage_sm(k + 2);  // waited for with the band copies
+        if (DIU_ONLY) cp_async_commit();
         __syncthreads();
         const TileView<P2> t(g, slot(k & 1), slot((k + 1) & 1), prv7, prv8, ib, jb, k);
         ViscView vv{};
         if (DIU_ONLY) {
             // A, B of plane k+1; exz, eyz between k and k+1; exy, fxy of k
-            const float *S1 = vS + ((k + 1) & 1) * kMPOS;
+            const float *S1 = sm_slot(k + 1);
             const float *A0 = vA + (k & 1) * kMPOS, *B0 = vB + (k & 1) * kMPOS;
             float *A1 = vA + ((k + 1) & 1) * kMPOS, *B1 = vB + ((k + 1) & 1) * kMPOS;
             float *XZ = vXZ + (k & 1) * kMPOS;
@@ -523,10 +534,10 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
                 vFXY[p] = t.xd((g.dy1[j + 1] * (A0[p - kMEX]) + g.dy1[j] * (A0[p])), g.dy1[j] + g.dy1[j + 1], g.rsy[j]);
             }
             __syncthreads();
-            vv = ViscView{vS + (k & 1) * kMPOS, S1, vXY, vFXY, vXZ + ((k + 1) & 1) * kMPOS, XZ, vYZ};
+            vv = ViscView{sm_slot(k), S1, vXY, vFXY, vXZ + ((k + 1) & 1) * kMPOS, XZ, vYZ};
         }
         cell(t, k, vv);
-        if (BAND) cp_async_wait<0>();
+        if (BAND || DIU_ONLY) cp_async_wait<0>();
         __syncthreads();
     }
 }
