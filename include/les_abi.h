@@ -273,6 +273,31 @@ les_status les_press_(const int *km, const int *jm, const int *im, float *rhs, c
                       const float *cn1, const float *cn2l, float *p, const float *cn2s,
                       const float *cn3l, const float *cn3s, const float *cn4l, const float *cn4s,
                       const int *n, const int *nmax, int *sor_iters);
+/* press.f95 in sub-steps (each copies in, runs on the device, copies out):
+ * les_press_rhsav_: press.f95:49-82, bondfg, rhs, rhsav and rhs -= rhsav;
+ *   rhsav (may be NULL) receives the average.
+ * les_press_sor_sweep_: press.f95:89-98 for colour *nrd (0 or 1), the sweep
+ *   then boundp1; rhs is the one press holds after the rhsav subtraction;
+ *   sor (may be NULL) receives this colour's sum of reltmp^2 (exact sum,
+ *   rounded once).
+ * les_press_residual_: one SOR iteration, press.f95:87-103 (both colours,
+ *   boundp1 after each, boundp2); sor receives the iteration's residual.
+ * les_press_pav_adj_: press.f95:123-146, pav, p -= pav, boundp1, boundp2;
+ *   pav (may be NULL) receives the average. */
+les_status les_press_rhsav_(const int *km, const int *jm, const int *im, float *rhs, const float *u,
+                            const float *dx1, const float *v, const float *dy1, const float *w,
+                            const float *dzn, float *f, float *g, float *h, const float *dt,
+                            float *rhsav);
+les_status les_press_sor_sweep_(const int *km, const int *jm, const int *im, const float *rhs,
+                                const float *cn1, const float *cn2l, float *p, const float *cn2s,
+                                const float *cn3l, const float *cn3s, const float *cn4l,
+                                const float *cn4s, const int *nrd, float *sor);
+les_status les_press_residual_(const int *km, const int *jm, const int *im, const float *rhs,
+                               const float *cn1, const float *cn2l, float *p, const float *cn2s,
+                               const float *cn3l, const float *cn3s, const float *cn4l,
+                               const float *cn4s, float *sor);
+les_status les_press_pav_adj_(const int *km, const int *jm, const int *im, float *p, const float *dx1,
+                              const float *dy1, const float *dzn, float *pav);
 /* bondFG.f95:5 */
 les_status les_bondfg_(const int *km, const int *jm, float *f, const int *im, float *g, float *h);
 /* boundp.f95:36 */

@@ -110,6 +110,7 @@ ROUTINES = {
     "les_velnw_": 15, "les_bondv1_": 11, "les_bondv1_ext_wind_profile_": 12, "les_velfg_": 44,
     "les_feedbf_": 21, "les_les_": 20, "les_boundsm_": 4, "les_adam_": 11, "les_press_": 25,
     "les_bondfg_": 6, "les_boundp1_": 4, "les_boundp2_": 4,
+    "les_press_rhsav_": 15, "les_press_sor_sweep_": 14, "les_press_residual_": 13, "les_press_pav_adj_": 8,
 }
 
 

@@ -71,7 +71,7 @@ def lib():
             getattr(L, n).argtypes = [C.c_int] * 3 + [_P] * 9
         L.oracle_init.argtypes = [C.c_int] * 3 + [_P] * 21
         L.oracle_feedbfm.argtypes = [C.c_int] * 3 + [_P] * 7
-        L.oracle_press_ex.argtypes = [C.c_int] * 3 + [_P] * 9 + [C.c_float] + [_P] * 7 + \
+        L.oracle_press_ex.argtypes = [C.c_int] * 3 + [_P] * 10 + [C.c_float] + [_P] * 8 + \
             [C.c_int, C.c_float, C.c_float] + [_P] * 3
         L.oracle_press_ex.restype = C.c_int
         _lib = L

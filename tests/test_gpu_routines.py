@@ -241,3 +241,70 @@ def test_press(require_gpu, state):
                                    I(10), C.byref(it)))
     assert it.value == it_o
     assert_bitexact(b, a, IP, JP, KP, ["rhs", "p", "f", "g", "h"])
+
+
+# ---- press.f95 sub-steps ---------------------------------------------------
+
+def _press_ex():
+    return oracle.lib().oracle_press_ex  # signature bound in oracle/__init__.py
+
+
+_PRESS = ["rhs", "u", "dx1", "v", "dy1", "w", "dzn", "f", "g", "h", "cn1", "cn2l", "p", "cn2s",
+          "cn3l", "cn3s", "cn4l", "cn4s"]
+
+
+def _press_base(state):
+    base = {n: state.arrays[n] for n in _PRESS}
+    base["rhs"] = _garbage("rhs", 5)
+    return _cp(base)
+
+
+def _oracle_press(a, dt, nmaxp):
+    sor, rhsav, pav = C.c_float(), C.c_float(), C.c_float()
+    args = [FL.ptr(a[n]) for n in _PRESS]
+    _press_ex()(KP, JP, IP, *args[:10], dt, *args[10:], nmaxp, -1.0, 1.0, C.byref(sor), C.byref(rhsav),
+                C.byref(pav))
+    return sor.value, rhsav.value, pav.value
+
+
+def _bits(x):
+    return np.float32(x).view(np.uint32)
+
+
+def test_press_rhsav_and_pav_adj(require_gpu, state):
+    dt = state.params.dt
+    a, b = _press_base(state), _press_base(state)
+    _, rhsav_o, pav_o = _oracle_press(a, dt, 0)
+    L = abi.lib()
+    rhsav, pav = C.c_float(), C.c_float()
+    abi.check(L.les_press_rhsav_(I(KP), I(JP), I(IP), *[FL.ptr(b[n]) for n in _PRESS[:10]], Fv(dt),
+                                 C.byref(rhsav)))
+    assert _bits(rhsav.value) == _bits(rhsav_o)
+    abi.check(L.les_press_pav_adj_(I(KP), I(JP), I(IP), FL.ptr(b["p"]), FL.ptr(b["dx1"]), FL.ptr(b["dy1"]),
+                                   FL.ptr(b["dzn"]), C.byref(pav)))
+    assert _bits(pav.value) == _bits(pav_o)
+    assert_bitexact(b, a, IP, JP, KP, ["rhs", "f", "g", "h", "p"])
+
+
+def test_press_sub_steps_compose_one_iteration(require_gpu, state):
+    dt = state.params.dt
+    a, b = _press_base(state), _press_base(state)
+    sor_o, _, _ = _oracle_press(a, dt, 1)
+    L = abi.lib()
+    abi.check(L.les_press_rhsav_(I(KP), I(JP), I(IP), *[FL.ptr(b[n]) for n in _PRESS[:10]], Fv(dt), None))
+    # two colour sweeps plus boundp2 on a copy must equal the full iteration
+    c2 = _cp({"rhs": b["rhs"], "p": b["p"]})
+    sor = C.c_float()
+    cn = [FL.ptr(b[n]) for n in ("cn1", "cn2l")]
+    tail = [FL.ptr(b[n]) for n in ("cn2s", "cn3l", "cn3s", "cn4l", "cn4s")]
+    abi.check(L.les_press_residual_(I(KP), I(JP), I(IP), FL.ptr(b["rhs"]), *cn, FL.ptr(b["p"]), *tail,
+                                    C.byref(sor)))
+    assert _bits(sor.value) == _bits(sor_o)
+    for nrd in (0, 1):
+        abi.check(L.les_press_sor_sweep_(I(KP), I(JP), I(IP), FL.ptr(c2["rhs"]), *cn, FL.ptr(c2["p"]), *tail,
+                                         I(nrd), None))
+    abi.check(L.les_boundp2_(I(JP), I(IP), FL.ptr(c2["p"]), I(KP)))
+    assert_bitexact({"p": c2["p"]}, {"p": b["p"]}, IP, JP, KP, ["p"])
+    abi.check(L.les_press_pav_adj_(I(KP), I(JP), I(IP), FL.ptr(b["p"]), FL.ptr(b["dx1"]), FL.ptr(b["dy1"]),
+                                   FL.ptr(b["dzn"]), None))
+    assert_bitexact(b, a, IP, JP, KP, ["rhs", "f", "g", "h", "p"])
