@@ -203,6 +203,43 @@ les_status les_halo_unpack_inner(float *array, const float *buffer, unsigned im,
                                  unsigned km, unsigned h_w, unsigned vdim, int device,
                                  void *stream);
 
+/* The same four operations for one component width each, named after the
+ * reference's kernels exchange_{1,2,4,16}_halo_read (pack) and
+ * exchange_{1,2,4,16}_halo_write (unpack), halo_exchange.cl:3-291 and
+ * halo_exchange_correct.cl (the _inner forms). */
+les_status les_halo_pack_1(const float *array, float *buffer, unsigned im, unsigned jm,
+                           unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_1(float *array, const float *buffer, unsigned im, unsigned jm,
+                             unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_pack_inner_1(const float *array, float *buffer, unsigned im, unsigned jm,
+                                 unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_inner_1(float *array, const float *buffer, unsigned im, unsigned jm,
+                                   unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_pack_2(const float *array, float *buffer, unsigned im, unsigned jm,
+                           unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_2(float *array, const float *buffer, unsigned im, unsigned jm,
+                             unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_pack_inner_2(const float *array, float *buffer, unsigned im, unsigned jm,
+                                 unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_inner_2(float *array, const float *buffer, unsigned im, unsigned jm,
+                                   unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_pack_4(const float *array, float *buffer, unsigned im, unsigned jm,
+                           unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_4(float *array, const float *buffer, unsigned im, unsigned jm,
+                             unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_pack_inner_4(const float *array, float *buffer, unsigned im, unsigned jm,
+                                 unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_inner_4(float *array, const float *buffer, unsigned im, unsigned jm,
+                                   unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_pack_16(const float *array, float *buffer, unsigned im, unsigned jm,
+                           unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_16(float *array, const float *buffer, unsigned im, unsigned jm,
+                             unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_pack_inner_16(const float *array, float *buffer, unsigned im, unsigned jm,
+                                 unsigned km, unsigned h_w, int device, void *stream);
+les_status les_halo_unpack_inner_16(float *array, const float *buffer, unsigned im, unsigned jm,
+                                   unsigned km, unsigned h_w, int device, void *stream);
+
 /* ---- setup feeding the step (a14) ------------------------------------ */
 /* grid.f95:55-82 metric derivation: given dx1(-1:ip+1), dy1(0:jp+1) and
  * dzn(1:kp+1) (in an array with bounds -1:kp+2), fill dxl, dyl, z2, the

@@ -95,6 +95,8 @@ _SIGS = {
     "les_halo_unpack": (C.c_int, [_P, _P, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, _P]),
     "les_halo_pack_inner": (C.c_int, [_P, _P, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, _P]),
     "les_halo_unpack_inner": (C.c_int, [_P, _P, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, _P]),
+    **{f"les_halo_{op}_{v}": (C.c_int, [_P, _P, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, _P])
+       for op in ("pack", "unpack", "pack_inner", "unpack_inner") for v in (1, 2, 4, 16)},
     "les_grid_metrics": (C.c_int, [C.c_int, C.c_int, C.c_int] + [_P] * 9),
     "les_poisson_coeffs": (C.c_int, [C.c_int, C.c_int, C.c_int] + [_P] * 10),
     "les_building_masks": (C.c_int, [C.c_int, C.c_int, C.c_int] + [_P] * 7),

@@ -247,6 +247,31 @@ les_status les_halo_unpack(float *a, const float *b, unsigned im, unsigned jm, u
                            int device, void *stream) {
     return halo_common(b, a, im, jm, km, hw, vdim, device, stream, 0, 1);
 }
+// One entry per component width, named after the reference's kernels
+// exchange_{1,2,4,16}_halo_read/_write (halo_exchange.cl, _correct.cl).
+#define LES_HALO_WIDTH(V)                                                                                        \
+    les_status les_halo_pack_##V(const float *a, float *b, unsigned im, unsigned jm, unsigned km, unsigned hw,     \
+                                 int device, void *stream) {                                                     \
+        return halo_common(a, b, im, jm, km, hw, V, device, stream, 0, 0);                                        \
+    }                                                                                                            \
+    les_status les_halo_unpack_##V(float *a, const float *b, unsigned im, unsigned jm, unsigned km, unsigned hw,   \
+                                   int device, void *stream) {                                                   \
+        return halo_common(b, a, im, jm, km, hw, V, device, stream, 0, 1);                                        \
+    }                                                                                                            \
+    les_status les_halo_pack_inner_##V(const float *a, float *b, unsigned im, unsigned jm, unsigned km,            \
+                                       unsigned hw, int device, void *stream) {                                  \
+        return halo_common(a, b, im, jm, km, hw, V, device, stream, 1, 0);                                        \
+    }                                                                                                            \
+    les_status les_halo_unpack_inner_##V(float *a, const float *b, unsigned im, unsigned jm, unsigned km,          \
+                                         unsigned hw, int device, void *stream) {                                \
+        return halo_common(b, a, im, jm, km, hw, V, device, stream, 1, 1);                                        \
+    }
+LES_HALO_WIDTH(1)
+LES_HALO_WIDTH(2)
+LES_HALO_WIDTH(4)
+LES_HALO_WIDTH(16)
+#undef LES_HALO_WIDTH
+
 les_status les_halo_pack_inner(const float *a, float *b, unsigned im, unsigned jm, unsigned km, unsigned hw,
                                unsigned vdim, int device, void *stream) {
     return halo_common(a, b, im, jm, km, hw, vdim, device, stream, 1, 0);

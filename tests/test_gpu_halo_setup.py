@@ -111,3 +111,26 @@ def test_masks_and_poisson_bitexact(require_gpu, dims):
     for n in FL.MASKS + FL.POISSON:
         np.testing.assert_array_equal(g[n], o[n], err_msg=n)
     assert g["amask1"].min() == 0.0  # buildings present
+
+
+@pytest.mark.parametrize("vd", [1, 2, 4, 16])
+def test_per_width_entries_match_the_oracle(require_gpu, vd):
+    # les_halo_{pack,unpack}[_inner]_<vd> (host pointers)
+    im, jm, km, hw = 13, 11, 5, 2
+    L = abi.lib()
+    rng = np.random.default_rng(vd)
+    for inner, sfx in ((False, ""), (True, "_inner")):
+        arr = rng.standard_normal(vd * im * jm * km).astype(np.float32)
+        nb = oracle.halo_buffer_floats(im, jm, km, hw, vd, inner)
+        b_ref = np.zeros(nb, np.float32)
+        b_gpu = np.zeros(nb, np.float32)
+        oracle.halo_pack(arr, b_ref, im, jm, km, hw, vd, inner=inner)
+        abi.check(getattr(L, f"les_halo_pack{sfx}_{vd}")(arr.ctypes.data, b_gpu.ctypes.data, im, jm, km, hw, 0,
+                                                         None))
+        np.testing.assert_array_equal(b_gpu, b_ref)
+        buf = rng.standard_normal(oracle.halo_buffer_floats(im, jm, km, hw, vd, False)).astype(np.float32)
+        a_ref, a_gpu = arr.copy(), arr.copy()
+        oracle.halo_unpack(a_ref, buf, im, jm, km, hw, vd, inner=inner)
+        abi.check(getattr(L, f"les_halo_unpack{sfx}_{vd}")(a_gpu.ctypes.data, buf.ctypes.data, im, jm, km, hw, 0,
+                                                           None))
+        np.testing.assert_array_equal(a_gpu, a_ref)

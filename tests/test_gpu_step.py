@@ -64,6 +64,23 @@ def test_interior_tiles_bitexact(require_gpu, spacing):
     gpu.close()
 
 
+@pytest.mark.slow
+def test_benchmark_case_200_steps(require_gpu):
+    # the 150 x 150 x 90 benchmark case (les_synth_default) over 200 time
+    # steps, the reference's run length: bit-exact, so within the stated
+    # 1e-5 relative L2 on u, v, w, p
+    ip, jp, kp = 150, 150, 90
+    ref, dev = _pair(ip, jp, kp, seed=1)
+    gpu = GpuLes(dev)
+    oracle.ifdata(ref, 1)
+    gpu.warmup(1)
+    oracle.run_steps(ref, 1, 200)
+    gpu.step(1, 200)
+    assert gpu.metrics()["n"] == 200
+    _compare(gpu, ref)
+    gpu.close()
+
+
 def test_power_law_inflow(require_gpu):
     ip, jp, kp = 12, 10, 80
     ref, dev = _pair(ip, jp, kp, seed=3, inflow="power")
