@@ -109,6 +109,7 @@ struct Scal {
     int pbuf;  // SOR result buffer: 0 = p, 1 = the second p buffer
     int redo;  // iterations to redo after a pass that converged part-way
     float probe[4];
+    int exact_sums;  // 1: the rest of this step's SOR passes sum the residual exactly
 };
 
 __device__ __forceinline__ int IX(const Geo &g, int i, int j, int k) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <map>
@@ -186,12 +187,15 @@ struct les_ctx {
     bool cn1_by_k = false;           // uniform dx, dy: cn1 from a per-k table
     bool p_ghosts_ok = false;        // p's ghosts hold what boundp1/boundp2 give
     bool force_exact_sor = false;    // testing: always the per-colour path
+    bool sor_fp32_test = true;       // LES_SOR_SUMS=exact clears it: every pass sums exactly
 };
 
 namespace {
 
 float *field_ptr(les_ctx *c, int f) { return c->d_fields + (size_t)f * c->box_elems; }
-les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, bool tuning = false);
+les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, int itmax,
+                         bool tuning = false);
+bool tb_fast_ok(const les_ctx *c, const TbShape &sh);
 
 // Host copies of the 1-D tables -> device; builds cnA/B/C, smc, wind.
 // Tables not given stay zero (the per-routine entries pass only theirs).
@@ -422,15 +426,23 @@ les_status enqueue_press(les_ctx *c, bool exact) {
             LAUNCH(c, k_final_sor, dim3(1), dim3(1024), c->d_part, 2 * np, c->prm.pjuge, c->d_scal);
         }
     } else {
-        for (int done = 0, pass = 0; done < c->prm.nmaxp; ++pass) {
-            const int nit = std::min(c->tb.T, c->prm.nmaxp - done);
+        const int nmaxp = c->prm.nmaxp;
+        for (int done = 0, pass = 0; done < nmaxp; ++pass) {
+            const int nit = std::min(c->tb.T, nmaxp - done);
             if (pass == 0) MARK(c, EV_SOR1_START);
-            les_status st = launch_sor_tb(c, c->tb, nit, 0, c->prm.pjuge);
+            les_status st = launch_sor_tb(c, c->tb, nit, 0, c->prm.pjuge, nmaxp);
             if (st != LES_OK) return st;
             if (pass == 0) MARK(c, EV_SOR1_END);
             // a pass of one iteration cannot stop part-way: no redo launch
-            if (nit > 1 && (st = launch_sor_tb(c, c->tb, nit, 1, c->prm.pjuge)) != LES_OK) return st;
+            if (nit > 1 && (st = launch_sor_tb(c, c->tb, nit, 1, c->prm.pjuge, nmaxp)) != LES_OK) return st;
             done += nit;
+        }
+        // an iteration whose FP32 stop test was undecided runs again with
+        // exact sums (at most once per step): one more pass, which returns
+        // at once when all nmaxp iterations are done or the SOR stopped
+        if (nmaxp >= 2 && tb_fast_ok(c, c->tb)) {
+            les_status st = launch_sor_tb(c, c->tb, 1, 0, c->prm.pjuge, nmaxp);
+            if (st != LES_OK) return st;
         }
     }
     MARK(c, EV_SOR_END);
@@ -471,10 +483,24 @@ les_status check_params(const les_params *p) {
     return LES_OK;
 }
 
-// Launch one temporal-blocked SOR pass (mode 0) or its redo (mode 1).
-// tuning: read and write only the second p buffer (scratch between steps),
-// so timing passes leave the model state alone.
-les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, bool tuning) {
+// One-iteration passes of this shape may take the FP32 stop test of
+// tb_finish_fast: at most 2^16 adds from a term to the root of its sum
+// (4 per plane of a k chunk, two block sums of 5 + warps adds, and the
+// strided pass over the block partials), a threshold below 2^40, and
+// LES_SOR_SUMS not set to "exact".
+bool tb_fast_ok(const les_ctx *c, const TbShape &sh) {
+    if (sh.T != 1 || !c->sor_fp32_test || !(c->prm.pjuge < 0x1p40f)) return false;
+    const int kc = cdiv(c->prm.kp, sh.nch), nt = 32 * tb_warps(sh.T, sh.ty);
+    const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(sh.T)) * cdiv(c->prm.jp, sh.ty) * cdiv(c->prm.kp, kc);
+    const long long depth = 4LL * kc + 2 * (5 + nt / 32) + (nblk + nt - 1) / nt;
+    return depth <= (1LL << 16);
+}
+
+// Launch one temporal-blocked SOR pass (mode 0) or its redo (mode 1); the
+// step has itmax iterations.  tuning: read and write only the second p
+// buffer (scratch between steps), so timing passes leave the model state
+// alone.
+les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, int itmax, bool tuning) {
     const int kc = cdiv(c->prm.kp, sh.nch);
     const dim3 grid(cdiv(c->prm.ip, tb_tx(sh.T)), cdiv(c->prm.jp, sh.ty), cdiv(c->prm.kp, kc));
     const dim3 block(32 * tb_warps(sh.T, sh.ty));
@@ -488,6 +514,8 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     a.kc = kc;
     a.niter = niter;
     a.mode = mode;
+    a.itmax = itmax;
+    a.fast = tb_fast_ok(c, sh) ? 1 : 0;
     a.pjuge = pjuge;
     a.part = c->d_part;
     a.sc = c->d_scal;
@@ -592,11 +620,11 @@ les_status autotune_sor(les_ctx *c) {
                         sh.nch = nch;
                         if (sh.ty < 4 || (nch > 1 && cdiv(c->prm.kp, nch) < 8) || !tb_shape_ok(c, sh)) continue;
                         CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
-                        les_status st = launch_sor_tb(c, sh, T, 0, -1.0f, true);
+                        les_status st = launch_sor_tb(c, sh, T, 0, -1.0f, INT_MAX, true);
                         if (st != LES_OK) return st;
                         CK(cudaEventRecord(e0, c->stream));
                         for (int r = 0; r < 2; ++r)
-                            if ((st = launch_sor_tb(c, sh, T, 0, -1.0f, true)) != LES_OK) return st;
+                            if ((st = launch_sor_tb(c, sh, T, 0, -1.0f, INT_MAX, true)) != LES_OK) return st;
                         CK(cudaEventRecord(e1, c->stream));
                         CK(cudaEventSynchronize(e1));
                         float ms = 0.0f;
@@ -684,6 +712,7 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     }
     les_ctx *c = new les_ctx();
     c->prm = *prm;
+    if (const char *sums = std::getenv("LES_SOR_SUMS")) c->sor_fp32_test = std::strcmp(sums, "exact") != 0;
     const int ip = prm->ip, jp = prm->jp, kp = prm->kp;
     Geo &g = c->geo;
     g.im = ip;

@@ -286,6 +286,7 @@ __global__ void k_step_begin(Scal *s, int n) {
     s->sor_iters = 0;
     s->redo = 0;
     s->pbuf = 0;
+    s->exact_sums = 0;
     s->n = n;
 }
 __global__ void k_probe(Geo g, Fields F, Scal *s) {

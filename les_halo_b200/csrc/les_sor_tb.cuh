@@ -76,6 +76,8 @@ struct TbArgs {
     const float *rhs;         // raw rhs (rhsav not yet subtracted)
     const float *cn1k;        // cn1 per k when it depends on k only
     int ty, kc, niter, mode;  // tile rows, planes per k chunk, iterations, 0 pass / 1 redo
+    int itmax;                // iterations of the step (nmaxp): a pass starting at itmax does nothing
+    int fast;                 // one-iteration passes may take the FP32 stop test (tb_finish_fast)
     float pjuge;              // stop threshold (press.f95:107)
     FixPart *part;            // kTbTMax partial sums per block
     Scal *sc;
@@ -103,6 +105,20 @@ __device__ __forceinline__ void fix_add_nonneg(float x, unsigned long long &hi, 
     const unsigned long long o = lo;
     lo += fr;
     hi += ip + (lo < o ? 1ull : 0ull);
+}
+
+// Sum of v over a block of whole warps, returned to thread 0: shuffles
+// within each warp, then thread 0 adds the warp sums in order.  Adds on any
+// leaf-to-root path: 5 + warps.
+__device__ __forceinline__ float block_float_sum0(float v) {
+    __shared__ float s_f[32];
+    for (int off = 16; off >= 1; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) s_f[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float t = 0.0f;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_f[w];
+    return t;
 }
 
 // block_fix_sum for any block of whole warps (up to 1024 threads).
@@ -169,6 +185,40 @@ __device__ void tb_finish_pass(const FixPart *part, int nblocks, int nit, float 
     if (threadIdx.x == 0 && s->redo == 0) s->pbuf ^= 1;
 }
 
+// FP32 stop test of a one-iteration pass that is not the step's last
+// iteration.  The exact test of press.f95:114 is sor < pjuge with sor the
+// exact sum S_x of the terms t = fl(reltmp^2) (each truncated to 2^-64,
+// les_fix.h) rounded to FP32.  Here the terms were summed in FP32 along a
+// tree with at most d adds from any term to the root (per thread 4 per
+// plane, block_float_sum0 twice, and the strided pass below; the host
+// keeps d <= 2^16).  With round-to-nearest on non-negative numbers the
+// computed sum v <= (1+u)^d * sum(t), u = 2^-24, so
+//     S_x >= v * (1 - d u) - n 2^-64 >= v * (1 - 2^-8) - 2^-33  (n < 2^31 cells),
+// evaluated below with rounding toward -inf as lb.  If pjuge <= lb < 2^40
+// then S_x >= lb, no exact partial overflows, and rounding S_x to FP32
+// gives at least lb (lb is an FP32 number): the exact test would not stop
+// either.  The iteration is then counted and its output buffer becomes
+// current.  Otherwise (possibly converged, or NaN/inf/huge sums) nothing is
+// counted, the buffers stay as they were, and every later pass of the step
+// sums exactly: the next launch repeats this iteration from the unchanged
+// input buffer (a pass reads one buffer and writes the other), so the
+// decision, the reported residual and p are those of exact sums.
+__device__ void tb_finish_fast(const FixPart *part, int nblocks, float pjuge, Scal *s) {
+    float v = 0.0f;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        v += __uint_as_float((unsigned)__ldcg(&part[(size_t)b * kTbTMax].lo));
+    v = block_float_sum0(v);
+    if (threadIdx.x == 0) {
+        const float lb = __fsub_rd(__fmul_rd(v, 0.99609375f), 0x1p-33f);
+        if (lb >= pjuge && lb < 0x1p40f) {
+            s->sor_iters += 1;
+            s->pbuf ^= 1;
+        } else {
+            s->exact_sums = 1;
+        }
+    }
+}
+
 // One pass of niter <= T iterations (mode 0), or the redo of scal->redo
 // iterations after a pass that converged part-way (mode 1).
 // CN1K: cn1 depends on k only (uniform dx and dy), read from cn1k[k].
@@ -178,7 +228,10 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
     extern __shared__ float4 smem4[];
     Scal *sc = a.sc;
     const bool redo = (a.mode == 1);
-    if (!redo && sc->converged) return;
+    if (!redo && (sc->converged || sc->sor_iters >= a.itmax)) return;
+    // FP32 residual sum for one-iteration passes before the step's last
+    // iteration, until a pass cannot decide in FP32 (tb_finish_fast)
+    const bool fast = T == 1 && a.fast && !redo && !sc->exact_sums && sc->sor_iters + 1 < a.itmax;
     const int nit = redo ? sc->redo : a.niter;
     if (nit <= 0) return;
     constexpr int R = tb_ring(T), RX = tb_ringx(T), TX = tb_tx(T), NS = tb_ns(T), D = kTbDepth, W = 2 * T + 2;
@@ -239,6 +292,7 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
     // reltmp^2 sums of iterations 0, 1, 2 of the pass
     unsigned long long h0 = 0, l0 = 0, h1 = 0, l1 = 0, h2 = 0, l2 = 0;
     int bad = 0;
+    float fsum = 0.0f;  // the FP32 sum of a fast pass
 
     // plane k of this warp's row: one 16-byte copy per lane and array
     const int d0 = y * RW4 + lane;
@@ -304,12 +358,15 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
                                                   pc);
                     w[C][s + 1] = ok ? pc + reltmp : pc;
                     if (acc && ok) {
-                        if (s < 2)
-                            fix_add_nonneg(reltmp * reltmp, h0, l0, bad);
+                        const float t2 = reltmp * reltmp;
+                        if (fast)
+                            fsum += t2;
+                        else if (s < 2)
+                            fix_add_nonneg(t2, h0, l0, bad);
                         else if (s < 4)
-                            fix_add_nonneg(reltmp * reltmp, h1, l1, bad);
+                            fix_add_nonneg(t2, h1, l1, bad);
                         else
-                            fix_add_nonneg(reltmp * reltmp, h2, l2, bad);
+                            fix_add_nonneg(t2, h2, l2, bad);
                     }
                 };
                 // x parity of this colour's cells on the row
@@ -348,7 +405,15 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
     // per-iteration partial sums, then the last block finishes the pass
     const int nblocks = gridDim.x * gridDim.y * gridDim.z;
     const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (!redo) {
+    if (fast) {
+        __syncthreads();
+        const float v = block_float_sum0(fsum);
+        if (threadIdx.x == 0) {
+            FixPart fp{};
+            fp.lo = __float_as_uint(v);
+            a.part[b * kTbTMax] = fp;
+        }
+    } else if (!redo) {
 #pragma unroll
         for (int t = 0; t < T; ++t) {
             __syncthreads();
@@ -374,7 +439,10 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
         }
         return;
     }
-    tb_finish_pass(a.part, nblocks, nit, a.pjuge, sc);
+    if (fast)
+        tb_finish_fast(a.part, nblocks, a.pjuge, sc);
+    else
+        tb_finish_pass(a.part, nblocks, nit, a.pjuge, sc);
 }
 
 }  // namespace

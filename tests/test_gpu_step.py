@@ -128,7 +128,7 @@ def test_multi_step_call_and_metrics(require_gpu):
     gpu.close()
 
 
-@pytest.mark.parametrize("shape", ["3,8,1", "2,8,2"])
+@pytest.mark.parametrize("shape", ["3,8,1", "2,8,2", "1,8,1"])
 @pytest.mark.parametrize("pjuge", [2.0e4, 6.0e3, 2.0e3, 7.0e2])
 def test_sor_stops_midway_through_a_pass(require_gpu, monkeypatch, pjuge, shape):
     # thresholds chosen so the SOR stops at different iteration counts, also
@@ -150,6 +150,62 @@ def test_sor_stops_midway_through_a_pass(require_gpu, monkeypatch, pjuge, shape)
         seen.append(iters[0])
         _compare(gpu, ref)
     gpu.close()
+
+
+def _residual_after(ip, jp, kp, seed, iters, monkeypatch):
+    """The SOR residual of step 1 after `iters` iterations (exact sums, no stop)."""
+    monkeypatch.setenv("LES_SOR_SUMS", "exact")
+    _, probe = _pair(ip, jp, kp, seed=seed)
+    probe.params.pjuge = -1.0
+    probe.params.nmaxp = iters
+    g = GpuLes(probe)
+    g.warmup(1)
+    g.step(1, 1)
+    r = g.metrics()["sor"]
+    g.close()
+    monkeypatch.delenv("LES_SOR_SUMS")
+    return r
+
+
+@pytest.mark.parametrize("shape", ["1,8,1", "1,12,2"])
+@pytest.mark.parametrize("at,scale", [(6, 1.0), (6, 1.0009765625), (1, 1.0), (1, 1.0009765625),
+                                      (24, 1.0), (24, 1.0009765625)])
+def test_undecided_fp32_stop_test_repeats_the_iteration_exactly(require_gpu, monkeypatch, shape, at, scale):
+    # One-iteration passes before the last iteration take an FP32 stop test
+    # that only rules out convergence.  A threshold at iteration `at`'s exact
+    # residual (scale 1: the exact test does not stop there) or just above
+    # it (it stops there) leaves that test undecided: the iteration runs
+    # again with exact sums, also on the first iteration and on the one
+    # before the last (which then needs the extra pass of the step).  The
+    # result must be the oracle's, with the residual and iteration count of
+    # exact sums throughout, and the next step starts in FP32 again.
+    monkeypatch.setenv("LES_SOR_TILE", shape)
+    ip, jp, kp, seed, nmaxp = 20, 16, 10, 4, 25
+    r = _residual_after(ip, jp, kp, seed, at, monkeypatch)
+    pjuge = float(np.float32(r) * np.float32(scale))
+    ref, dev = _pair(ip, jp, kp, seed=seed)
+    for c in (ref, dev):
+        c.params.pjuge = pjuge
+        c.params.nmaxp = nmaxp
+    monkeypatch.setenv("LES_SOR_SUMS", "exact")
+    ex = GpuLes(dev.copy())
+    monkeypatch.delenv("LES_SOR_SUMS")
+    gpu = GpuLes(dev)
+    oracle.ifdata(ref, 1)
+    for g in (gpu, ex):
+        g.warmup(1)
+    for n in (1, 2):
+        iters = oracle.run_steps(ref, n, 1)
+        for g in (gpu, ex):
+            g.step(n, 1)
+        m, me = gpu.metrics(), ex.metrics()
+        assert m["sor_iters"] == me["sor_iters"] == iters[0]
+        assert np.float32(m["sor"]).view(np.uint32) == np.float32(me["sor"]).view(np.uint32)
+        if n == 1 and scale > 1.0:
+            assert iters[0] <= at
+        _compare(gpu, ref)
+    gpu.close()
+    ex.close()
 
 
 def test_multi_iteration_passes_equal_per_colour_sweeps(require_gpu):
