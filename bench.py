@@ -34,6 +34,9 @@ METRIC = "time-step Mpts/s: plain vs FP64-refined press at ≤1e-5 err; adjoint/
 WORKLOAD = dict(ip=600, jp=600, kp=120, plan_area=0.35, h_max=120.0, dt=0.05, nmaxp=50, seed=1)
 SOR_BYTES_PER_CELL_PER_ITER = 12.0   # algorithmic bytes of one SOR iteration: p read, rhs read, p write
 STEP_BYTES_PER_CELL = 204.0 + 12.0 * 50  # algorithmic bytes per cell per step at 50 SOR iterations
+# aveflow's running sums (aveflow.f95:72-88): read u, v, w, p, sm (20 B),
+# read and write the ten sums (80 B)
+AVE_BYTES_PER_CELL = 100.0
 
 
 def _dist():
@@ -282,6 +285,22 @@ def run_ours(args):
         abi.check(L.les_last_metrics(gpu.ctx, C.byref(mrec)))
     e2e_s = time.perf_counter() - t0
 
+    # aveflow.f95:72-88 on the device-resident state (main_ocl.f95:313 calls
+    # it after every step), timed alone with CUDA events: one call starts
+    # the sums (allocating them), then K accumulating calls.  The ten sums
+    # (1.7 GB at 600x600x120) are far larger than L2.
+    ave_k = max(3, min(args.steps, 10))
+    big = 1 << 30
+    gpu.aveflow(1, 1, big)
+    torch.cuda.synchronize()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for s in range(ave_k):
+        gpu.aveflow(2 + s, 1, big)
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    ave_ms = ev2.elapsed_time(ev3) / ave_k
+
     ms_total, e2e_s, value, e2e_val = job_rates(ms_total, e2e_s, cells, args.steps, e2e_steps, ws,
                                                 dist, "cuda")
     ms_step = ms_total / args.steps
@@ -330,6 +349,11 @@ def run_ours(args):
                     "path": "C ABI: les_set_wind_profile + les_step + les_ctx_halo_read/write x7 + "
                             "les_last_metrics, pinned host buffers, wall clock"},
             "clocks": clocks,
+            "aveflow": {"kernel": "k_ave_accum", "ms_per_call": round(ave_ms, 4),
+                        "achieved": round(AVE_BYTES_PER_CELL * cells / (ave_ms / 1e3) / 1e9, 1),
+                        "peak": peak, "unit": "GB/s",
+                        "frac": round(AVE_BYTES_PER_CELL * cells / (ave_ms / 1e3) / 1e9 / peak, 4),
+                        "bytes_per_cell": AVE_BYTES_PER_CELL, "calls": ave_k},
         }
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)

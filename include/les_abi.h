@@ -36,7 +36,8 @@ typedef enum les_status {
     LES_ERR_TIMEOUT = 4, /* a bounded device wait gave up               */
     LES_ERR_NAN = 5,     /* non-finite value found by a checking call   */
     LES_ERR_NOMEM = 6,   /* device allocation failed                    */
-    LES_ERR_STATE = 7    /* call out of order (e.g. step before upload) */
+    LES_ERR_STATE = 7,   /* call out of order (e.g. step before upload) */
+    LES_ERR_IO = 8       /* file missing, unreadable or of the wrong shape */
 } les_status;
 
 /* Last error message of the calling thread ("" after success). */
@@ -361,6 +362,64 @@ les_status les_press_rhs_noalloc(int km, int jm, int im, float *rhs, const float
                                  const float *dx1, const float *v, const float *dy1,
                                  const float *w, const float *dzn, float *f, float *g, float *h,
                                  float dt, float *rhsav, void *stream);
+
+/* ---- Time statistics: aveflow.f95:5-179 ------------------------------------
+ * The eleven (ip,jp,kp) arrays and seven (ip,kp) arrays of aveflow, Fortran
+ * order, interior only.  A NULL member is skipped by upload/download. */
+typedef struct les_aveflow_fields {
+    float *aveu, *avev, *avew, *avep, *avel, *aveuu, *avevv, *aveww, *avesm, *avesmsm,
+        *uwfx;                                                    /* (ip,jp,kp) */
+    float *avesu, *avesv, *avesw, *avesuu, *avesvv, *avesww, *uwfxs; /* (ip,kp)    */
+} les_aveflow_fields;
+
+/* aveflow.f95:42-175 on the context's state after step n (call it after
+ * les_step for n, as main_ocl.f95:313 calls aveflow after the step): at
+ * n == n1 the sums restart, for n >= n1 u, v, w, p, sm, their squares and
+ * the uw flux are added, and at n == nmax the means, rms values and j means
+ * are formed and, for each non-NULL, non-blank file name, the data10 file
+ * (n,time; aveu, avew, avev) and the data11 file (n,time; aveuu, aveww,
+ * avevv, uwfx) are written as the reference writes them (gfortran
+ * unformatted sequential records, big-endian).  The statistics stay on the
+ * device (allocated and zeroed on the first call); uwfxs is accumulated
+ * from its current value, as in the reference, which never zeroes it.
+ * Bit-identical to the reference's loops except at k = 1 of the uwfx
+ * finish (aveflow.f95:112), where the reference reads aveu and avew before
+ * the start of the arrays; those values are taken as 0 here. */
+les_status les_aveflow(les_ctx *ctx, int n, int n1, int nmax, float time, const char *data10,
+                       const char *data11);
+les_status les_aveflow_upload(les_ctx *ctx, const les_aveflow_fields *stats);
+les_status les_aveflow_download(les_ctx *ctx, les_aveflow_fields *stats);
+/* aveflow.f95:5 with its Fortran argument order (host arrays by reference;
+ * data10/data11 are file names, NULL or blank for no file).  u, v, w use the
+ * bounds of main_ocl.f95, p (0:ip+2,0:jp+2,0:kp+1), sm (-1:ip+1,-1:jp+1,0:kp+1). */
+les_status les_aveflow_(const int *n, const int *n1, const int *km, const int *jm, const int *im,
+                        float *aveu, float *avev, float *avew, float *avep, float *avel,
+                        float *aveuu, float *avevv, float *aveww, float *avesm, float *avesmsm,
+                        float *uwfx, float *avesu, float *avesv, float *avesw, float *avesuu,
+                        float *avesvv, float *avesww, const float *u, const float *v,
+                        const float *w, const float *p, const float *sm, const int *nmax,
+                        float *uwfxs, const char *data10, const float *time, const char *data11);
+
+/* ---- Restart files ----------------------------------------------------------
+ * les_write_restart writes the reference's restart records from the
+ * context's state: data20 = u, v, w, p, usum, vsum, wsum (press.f95:191-201,
+ * write_uvw_p_uvwsum_to_file at module_LES_combined_ocl_TEMPL_V2.f95:1194)
+ * and data21 = fold, gold, hold (write_fgh_old_to_file,
+ * module_LES_combined_ocl_TEMPL_V2.f95:1217) plus fghold as a fourth record
+ * when fghold is not NULL (adam.f95:22-31 writes four).  Interior
+ * (1:ip,1:jp,1:kp) of each array, one record each, big-endian gfortran
+ * unformatted.  The reference writes them when mod(n,1000) == 0 or n == nmax;
+ * the caller decides.  A NULL or blank name skips that file.
+ * les_read_restart is the ICAL=1 reader of ifdata.f95:227-247: data30 holds
+ * (n,time) and then the seven data20 records, data31 the data21 records
+ * (fghold, if requested, must be the fourth).  Both files are read and
+ * checked before the device state changes; the interiors of u, v, w, p,
+ * usum, vsum, wsum, fold, gold, hold are replaced and their ghosts kept.
+ * Follow with les_ctx_warmup, as ifdata continues after reading. */
+les_status les_write_restart(les_ctx *ctx, const char *data20, const char *data21,
+                             const float *fghold);
+les_status les_read_restart(les_ctx *ctx, const char *data30, const char *data31, int *n,
+                            float *time, float *fghold);
 
 #ifdef __cplusplus
 }

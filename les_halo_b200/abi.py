@@ -11,7 +11,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "liblesb200.so"
 
 LES_OK, LES_ERR_BAD_ARG, LES_ERR_DIMS, LES_ERR_CUDA, LES_ERR_TIMEOUT, LES_ERR_NAN, \
-    LES_ERR_NOMEM, LES_ERR_STATE = range(8)
+    LES_ERR_NOMEM, LES_ERR_STATE, LES_ERR_IO = range(9)
 LES_INFLOW_POWER_LAW, LES_INFLOW_EXTERNAL = 0, 1
 FIELD_IDS = ["u", "v", "w", "p", "usum", "vsum", "wsum", "f", "g", "h", "fold", "gold", "hold",
              "rhs", "sm", "amask1", "bmask1", "cmask1", "dmask1"]
@@ -42,6 +42,15 @@ class LesMetrics(C.Structure):
     _fields_ = [("n", C.c_int), ("sor_iters", C.c_int), ("sor", C.c_float), ("rhsav", C.c_float),
                 ("pav", C.c_float), ("uout", C.c_float), ("p_centre", C.c_float),
                 ("u_centre", C.c_float), ("v_centre", C.c_float), ("w_centre", C.c_float)]
+
+
+AVEFLOW_CELL = ["aveu", "avev", "avew", "avep", "avel", "aveuu", "avevv", "aveww", "avesm", "avesmsm",
+                "uwfx"]
+AVEFLOW_COL = ["avesu", "avesv", "avesw", "avesuu", "avesvv", "avesww", "uwfxs"]
+
+
+class LesAveflowFields(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in AVEFLOW_CELL + AVEFLOW_COL]
 
 
 class LesSynthCfg(C.Structure):
@@ -105,6 +114,11 @@ _SIGS = {
     "les_synth_terrain": (C.c_float, [C.POINTER(LesSynthCfg), _P]),
     "les_synth_inflow": (C.c_int, [C.POINTER(LesSynthCfg), _P, _P, _P]),
     "les_press_rhs_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int] + [_P] * 10 + [C.c_float, _P, _P]),
+    "les_aveflow": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_char_p, C.c_char_p]),
+    "les_aveflow_upload": (C.c_int, [_P, C.POINTER(LesAveflowFields)]),
+    "les_aveflow_download": (C.c_int, [_P, C.POINTER(LesAveflowFields)]),
+    "les_write_restart": (C.c_int, [_P, C.c_char_p, C.c_char_p, _P]),
+    "les_read_restart": (C.c_int, [_P, C.c_char_p, C.c_char_p, _I, _F, _P]),
 }
 
 # Per-routine entries: every argument is a pointer (Fortran by-reference).
@@ -113,6 +127,7 @@ ROUTINES = {
     "les_feedbf_": 21, "les_les_": 20, "les_boundsm_": 4, "les_adam_": 11, "les_press_": 25,
     "les_bondfg_": 6, "les_boundp1_": 4, "les_boundp2_": 4,
     "les_press_rhsav_": 15, "les_press_sor_sweep_": 14, "les_press_residual_": 13, "les_press_pav_adj_": 8,
+    "les_aveflow_": 32,
 }
 
 

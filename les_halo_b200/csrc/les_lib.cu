@@ -21,6 +21,7 @@
 #include "les_press.cuh"
 #include "les_routines.cuh"
 #include "les_sor_tb.cuh"
+#include "les_stats.cuh"
 #include "les_step.cuh"
 
 using namespace les;
@@ -188,6 +189,7 @@ struct les_ctx {
     bool p_ghosts_ok = false;        // p's ghosts hold what boundp1/boundp2 give
     bool force_exact_sor = false;    // testing: always the per-colour path
     bool sor_fp32_test = true;       // LES_SOR_SUMS=exact clears it: every pass sums exactly
+    float *d_ave = nullptr;          // aveflow statistics (les_stats.cuh), allocated on first use
 };
 
 namespace {
@@ -836,6 +838,7 @@ les_status les_ctx_destroy(les_ctx *c) {
     cudaFree(c->d_part);
     cudaFree(c->d_stage);
     cudaFree(c->d_p2);
+    cudaFree(c->d_ave);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ok();
@@ -1199,3 +1202,4 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 }  // extern "C"
 
 #include "les_routines_api.inc"
+#include "les_stats_io.inc"

@@ -104,3 +104,8 @@ def ptr(a):
         return None
     assert a.dtype == np.float32 and a.flags["F_CONTIGUOUS"], "need Fortran-ordered float32"
     return a.ctypes.data
+
+
+def set_interior(name: str, arr: np.ndarray, values: np.ndarray, ip: int, jp: int, kp: int):
+    """arr(1:ip, 1:jp, 1:kp) = values (ghosts untouched)."""
+    arr[index(name, ip, jp, kp, slice(1, ip), slice(1, jp), slice(1, kp))] = values

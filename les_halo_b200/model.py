@@ -148,6 +148,42 @@ class GpuLes:
         abi.check(abi.lib().les_ctx_download(self.ctx, C.byref(hf)))
         return out
 
+    # -- time statistics and restart files (aveflow.f95, press.f95:191-201,
+    # adam.f95:22-31, ifdata.f95:227-247) --
+    def aveflow(self, n, n1, nmax, time=0.0, data10=None, data11=None):
+        enc = lambda x: None if x is None else str(x).encode()
+        abi.check(abi.lib().les_aveflow(self.ctx, n, n1, nmax, time, enc(data10), enc(data11)))
+
+    def _ave_fields(self, stats: dict) -> abi.LesAveflowFields:
+        s = abi.LesAveflowFields()
+        for n, a in stats.items():
+            assert a.dtype == np.float32 and a.flags["F_CONTIGUOUS"]
+            setattr(s, n, a.ctypes.data)
+        return s
+
+    def aveflow_download(self) -> dict:
+        ip, jp, kp = self.case.ip, self.case.jp, self.case.kp
+        out = {n: np.zeros((ip, jp, kp), np.float32, order="F") for n in abi.AVEFLOW_CELL}
+        out.update({n: np.zeros((ip, kp), np.float32, order="F") for n in abi.AVEFLOW_COL})
+        abi.check(abi.lib().les_aveflow_download(self.ctx, C.byref(self._ave_fields(out))))
+        return out
+
+    def aveflow_upload(self, stats: dict):
+        abi.check(abi.lib().les_aveflow_upload(self.ctx, C.byref(self._ave_fields(stats))))
+
+    def write_restart(self, data20, data21, fghold=None):
+        abi.check(abi.lib().les_write_restart(self.ctx, str(data20).encode() if data20 else None,
+                                              str(data21).encode() if data21 else None,
+                                              None if fghold is None else FL.ptr(fghold)))
+
+    def read_restart(self, data30, data31, fghold=None):
+        """Returns (n, time) of the data30 header."""
+        n, t = C.c_int(), C.c_float()
+        abi.check(abi.lib().les_read_restart(self.ctx, str(data30).encode(), str(data31).encode(),
+                                             C.byref(n), C.byref(t),
+                                             None if fghold is None else FL.ptr(fghold)))
+        return n.value, t.value
+
     def launches(self) -> int:
         return int(abi.lib().les_ctx_launch_count(self.ctx))
 

@@ -74,6 +74,7 @@ def lib():
         L.oracle_press_ex.argtypes = [C.c_int] * 3 + [_P] * 10 + [C.c_float] + [_P] * 8 + \
             [C.c_int, C.c_float, C.c_float] + [_P] * 3
         L.oracle_press_ex.restype = C.c_int
+        L.oracle_aveflow.argtypes = [C.c_int] * 5 + [_P] * 22 + [C.c_int, _P]
         _lib = L
     return _lib
 
@@ -143,3 +144,24 @@ def halo_unpack(array, buffer, im, jm, km, hw, vdim, soa=False, inner=False):
 
 def halo_buffer_floats(im, jm, km, hw, vdim, inner=False):
     return int(lib().oracle_halo_buffer_floats(im, jm, km, hw, vdim, int(inner)))
+
+
+AVE_CELL = ["aveu", "avev", "avew", "avep", "avel", "aveuu", "avevv", "aveww", "avesm", "avesmsm",
+            "uwfx"]
+AVE_COL = ["avesu", "avesv", "avesw", "avesuu", "avesvv", "avesww", "uwfxs"]
+
+
+def ave_alloc(ip, jp, kp):
+    """Zeroed aveflow arrays: (ip,jp,kp) and (ip,kp), Fortran order."""
+    out = {n: np.zeros((ip, jp, kp), np.float32, order="F") for n in AVE_CELL}
+    out.update({n: np.zeros((ip, kp), np.float32, order="F") for n in AVE_COL})
+    return out
+
+
+def aveflow(case, stats: dict, n, n1, nmax):
+    """aveflow.f95:42-157 on the case's u, v, w, p, sm into stats (in place)."""
+    A = case.arrays
+    c = [ptr(stats[k]) for k in AVE_CELL]
+    col = [ptr(stats[k]) for k in AVE_COL]
+    lib().oracle_aveflow(n, n1, case.kp, case.jp, case.ip, *c, *col[:6], ptr(A["u"]), ptr(A["v"]),
+                         ptr(A["w"]), ptr(A["p"]), ptr(A["sm"]), nmax, col[6])

@@ -876,6 +876,133 @@ void oracle_adam(int n, int nmax, float *fold_, int im, int jm, int km, float *g
             }
 }
 
+// aveflow.f95:42-157 (the data10/data11 writes of :159-174 are left to the
+// caller).  Serial loops in the Fortran order.  At k = 1 the finish of uwfx
+// (:112-113) reads aveu(i,j,0), avew(i,j,0) and avew(i+1,j,0): they are
+// taken at their flattened index in the (ip,jp,kp) arrays, 0 where that
+// index lies before the first element (outside the arrays in the reference).
+void oracle_aveflow(int n, int n1, int km, int jm, int im, float *aveu_, float *avev_, float *avew_,
+                    float *avep_, float *avel_, float *aveuu_, float *avevv_, float *aveww_,
+                    float *avesm_, float *avesmsm_, float *uwfx_, float *avesu_, float *avesv_,
+                    float *avesw_, float *avesuu_, float *avesvv_, float *avesww_, const float *u_,
+                    const float *v_, const float *w_, const float *p_, const float *sm_, int nmax,
+                    float *uwfxs_) {
+    const int ip = im, jp = jm, kp = km;
+    A3 aveu = ARR_I(aveu_), avev = ARR_I(avev_), avew = ARR_I(avew_), avep = ARR_I(avep_);
+    A3 avel = ARR_I(avel_), aveuu = ARR_I(aveuu_), avevv = ARR_I(avevv_), aveww = ARR_I(aveww_);
+    A3 avesm = ARR_I(avesm_), avesmsm = ARR_I(avesmsm_), uwfx = ARR_I(uwfx_);
+    A3 avesu = mk(avesu_, 1, ip, 1, kp, 1, 1), avesv = mk(avesv_, 1, ip, 1, kp, 1, 1);
+    A3 avesw = mk(avesw_, 1, ip, 1, kp, 1, 1), avesuu = mk(avesuu_, 1, ip, 1, kp, 1, 1);
+    A3 avesvv = mk(avesvv_, 1, ip, 1, kp, 1, 1), avesww = mk(avesww_, 1, ip, 1, kp, 1, 1);
+    A3 uwfxs = mk(uwfxs_, 1, ip, 1, kp, 1, 1);
+    A3 u = ARR_U(u_), v = ARR_U(v_), w = ARR_W(w_), p = ARR_P(p_), sm = ARR_SM(sm_);
+    // the flattened read of the uwfx finish
+    auto flat = [&](const float *a, int i, int j, int k) {
+        const long long idx = (long long)(i - 1) + (long long)ip * ((j - 1) + (long long)jp * (k - 1));
+        return idx < 0 ? 0.0f : a[idx];
+    };
+    if (n == n1) {
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) {
+                    aveu(i, j, k) = 0.0f;
+                    avev(i, j, k) = 0.0f;
+                    avew(i, j, k) = 0.0f;
+                    avep(i, j, k) = 0.0f;
+                    avel(i, j, k) = 0.0f;
+                    aveuu(i, j, k) = 0.0f;
+                    avevv(i, j, k) = 0.0f;
+                    aveww(i, j, k) = 0.0f;
+                    avesm(i, j, k) = 0.0f;
+                    avesmsm(i, j, k) = 0.0f;
+                    uwfx(i, j, k) = 0.0f;
+                }
+        for (int k = 1; k <= km; ++k)
+            for (int i = 1; i <= im; ++i) {
+                avesu(i, k, 1) = 0.0f;
+                avesv(i, k, 1) = 0.0f;
+                avesw(i, k, 1) = 0.0f;
+                avesuu(i, k, 1) = 0.0f;
+                avesvv(i, k, 1) = 0.0f;
+                avesww(i, k, 1) = 0.0f;
+            }
+    }
+    if (n >= n1) {
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) {
+                    aveu(i, j, k) = aveu(i, j, k) + u(i, j, k);
+                    avev(i, j, k) = avev(i, j, k) + v(i, j, k);
+                    avew(i, j, k) = avew(i, j, k) + w(i, j, k);
+                    avep(i, j, k) = avep(i, j, k) + p(i, j, k);
+                    aveuu(i, j, k) = aveuu(i, j, k) + u(i, j, k) * u(i, j, k);
+                    avevv(i, j, k) = avevv(i, j, k) + v(i, j, k) * v(i, j, k);
+                    aveww(i, j, k) = aveww(i, j, k) + w(i, j, k) * w(i, j, k);
+                    avesm(i, j, k) = avesm(i, j, k) + sm(i, j, k);
+                    avesmsm(i, j, k) = avesmsm(i, j, k) + sm(i, j, k) * sm(i, j, k);
+                    uwfx(i, j, k) = uwfx(i, j, k) + 0.5f * (u(i, j, k - 1) + u(i, j, k)) * 0.5f *
+                                                        (w(i, j, k - 1) + w(i + 1, j, k - 1));
+                }
+    }
+    if (n == nmax) {
+        const float cnt = (float)(nmax - n1 + 1);
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) {
+                    aveu(i, j, k) = aveu(i, j, k) / cnt;
+                    avev(i, j, k) = avev(i, j, k) / cnt;
+                    avew(i, j, k) = avew(i, j, k) / cnt;
+                    avep(i, j, k) = avep(i, j, k) / cnt;
+                    avel(i, j, k) = avel(i, j, k) / cnt;
+                    aveuu(i, j, k) = aveuu(i, j, k) / cnt;
+                    avevv(i, j, k) = avevv(i, j, k) / cnt;
+                    aveww(i, j, k) = aveww(i, j, k) / cnt;
+                    avesm(i, j, k) = avesm(i, j, k) / cnt;
+                    avesmsm(i, j, k) = avesmsm(i, j, k) / cnt;
+                }
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i)
+                    uwfx(i, j, k) = uwfx(i, j, k) / cnt - 0.5f * (flat(aveu_, i, j, k - 1) + aveu(i, j, k)) * 0.5f *
+                                                              (flat(avew_, i, j, k - 1) + flat(avew_, i + 1, j, k - 1));
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) {
+                    avesu(i, k, 1) = avesu(i, k, 1) + aveu(i, j, k);
+                    avesv(i, k, 1) = avesv(i, k, 1) + avev(i, j, k);
+                    avesw(i, k, 1) = avesw(i, k, 1) + avew(i, j, k);
+                    avesuu(i, k, 1) = avesuu(i, k, 1) + aveuu(i, j, k);
+                    avesvv(i, k, 1) = avesvv(i, k, 1) + avevv(i, j, k);
+                    avesww(i, k, 1) = avesww(i, k, 1) + aveww(i, j, k);
+                    uwfxs(i, k, 1) = uwfxs(i, k, 1) + uwfx(i, j, k);
+                }
+        const float rjm = (float)jm;
+        for (int k = 1; k <= km; ++k)
+            for (int i = 1; i <= im; ++i) {
+                avesu(i, k, 1) = avesu(i, k, 1) / rjm;
+                avesv(i, k, 1) = avesv(i, k, 1) / rjm;
+                avesw(i, k, 1) = avesw(i, k, 1) / rjm;
+                avesuu(i, k, 1) = avesuu(i, k, 1) / rjm;
+                avesvv(i, k, 1) = avesvv(i, k, 1) / rjm;
+                avesww(i, k, 1) = avesww(i, k, 1) / rjm;
+                uwfxs(i, k, 1) = uwfxs(i, k, 1) / rjm;
+            }
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) {
+                    aveuu(i, j, k) = std::sqrt(std::fabs(aveuu(i, j, k) - aveu(i, j, k) * aveu(i, j, k)));
+                    avevv(i, j, k) = std::sqrt(std::fabs(avevv(i, j, k) - avev(i, j, k) * avev(i, j, k)));
+                    aveww(i, j, k) = std::sqrt(std::fabs(aveww(i, j, k) - avew(i, j, k) * avew(i, j, k)));
+                }
+        for (int k = 1; k <= km; ++k)
+            for (int i = 1; i <= im; ++i) {
+                avesuu(i, k, 1) = std::sqrt(std::fabs(avesuu(i, k, 1) - avesu(i, k, 1) * avesu(i, k, 1)));
+                avesvv(i, k, 1) = std::sqrt(std::fabs(avesvv(i, k, 1) - avesv(i, k, 1) * avesv(i, k, 1)));
+                avesww(i, k, 1) = std::sqrt(std::fabs(avesww(i, k, 1) - avesw(i, k, 1) * avesw(i, k, 1)));
+            }
+    }
+}
+
 // bondFG.f95:15-31
 void oracle_bondfg(int km, int jm, float *f_, int im, float *g_, float *h_) {
     const int ip = im, jp = jm, kp = km;

@@ -99,6 +99,13 @@ void oracle_boundsm(int km, int jm, float *sm, int im);
 void oracle_adam(int n, int nmax, float *fold, int im, int jm, int km, float *gold, float *hold,
                  float *f, float *g, float *h);
 void oracle_bondfg(int km, int jm, float *f, int im, float *g, float *h);
+/* aveflow.f95:42-157 (no file output).  aveu..uwfx (ip,jp,kp); avesu..avesww,
+ * uwfxs (ip,kp); u, v, w, p, sm with the main_ocl.f95 bounds. */
+void oracle_aveflow(int n, int n1, int km, int jm, int im, float *aveu, float *avev, float *avew,
+                    float *avep, float *avel, float *aveuu, float *avevv, float *aveww, float *avesm,
+                    float *avesmsm, float *uwfx, float *avesu, float *avesv, float *avesw,
+                    float *avesuu, float *avesvv, float *avesww, const float *u, const float *v,
+                    const float *w, const float *p, const float *sm, int nmax, float *uwfxs);
 void oracle_boundp1(int km, int jm, float *p, int im);
 void oracle_boundp2(int jm, int im, float *p, int km);
 /* press.f95:49-146 (the I/O and print branches are omitted). Returns the
