@@ -200,6 +200,64 @@ def run_reference(args):
     return 0
 
 
+ENSEMBLE = dict(members=64, size_lo=96, size_hi=256, kp=80, ustar_lo=0.2, ustar_hi=0.5, seed=2024)
+
+
+def ensemble_bench(steps, warmup):
+    """64 uneven domains (ip, jp ~ U{96..256}, kp=80, own terrain seed, u* ~
+    U[0.2, 0.5]) advanced `steps` steps by one graph launch per step, and the
+    same members advanced one after another with les_step (64 sequential
+    runs); CUDA events on the launching streams."""
+    import torch
+    import les_halo_b200 as lh
+    E = ENSEMBLE
+    rng = np.random.default_rng(E["seed"])
+    members, cells = [], 0
+    for m in range(E["members"]):
+        ip, jp = (int(x) for x in rng.integers(E["size_lo"], E["size_hi"] + 1, size=2))
+        ustar = float(rng.uniform(E["ustar_lo"], E["ustar_hi"]))
+        case = lh.synthetic_case(ip, jp, E["kp"], seed=E["seed"] + 1 + m, dt=0.05, nmaxp=50,
+                                 ustar=ustar)
+        g = lh.GpuLes(case)
+        g.warmup(1)
+        members.append(g)
+        cells += ip * jp * E["kp"]
+    ens = lh.Ensemble(members)
+    ens.step(1, warmup)
+    ens.sync()
+    st = torch.cuda.ExternalStream(ens.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ens.launches()
+    e0.record(st)
+    ens.step(1 + warmup, steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ens_ms = e0.elapsed_time(e1)
+    launches = ens.launches() - l0
+    n = 1 + warmup + steps
+    seq_ms = 0.0
+    for g in members:  # one run after another
+        ms = torch.cuda.ExternalStream(g.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ms)
+        g.step(n, steps)
+        b.record(ms)
+        torch.cuda.synchronize()
+        seq_ms += a.elapsed_time(b)
+    ens.close()
+    for g in members:
+        g.close()
+    return {"members": E["members"], "cells": cells, "kp": E["kp"], "steps": steps,
+            "ensemble_mpts": round(cells * steps / (ens_ms / 1e3) / 1e6, 1),
+            "ensemble_ms_per_step": round(ens_ms / steps, 3),
+            "sequential_mpts": round(cells * steps / (seq_ms / 1e3) / 1e6, 1),
+            "sequential_ms_per_step": round(seq_ms / steps, 3),
+            "speedup": round(seq_ms / ens_ms, 3), "graph_launches_per_step": 1,
+            "kernels_per_step": int(launches // max(steps, 1)),
+            "config": f"ip,jp ~ U{{{E['size_lo']}..{E['size_hi']}}}, kp={E['kp']}, u* ~ "
+                      f"U[{E['ustar_lo']},{E['ustar_hi']}], seed {E['seed']}"}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = _dist()
@@ -355,6 +413,11 @@ def run_ours(args):
                         "frac": round(AVE_BYTES_PER_CELL * cells / (ave_ms / 1e3) / 1e9 / peak, 4),
                         "bytes_per_cell": AVE_BYTES_PER_CELL, "calls": ave_k},
         }
+        if ws == 1 and not args.profile and not args.no_ensemble:
+            try:
+                line["ensemble"] = ensemble_bench(args.steps, args.warmup)
+            except Exception as exc:  # reported, never fatal to the headline line
+                line["ensemble"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
@@ -371,6 +434,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the 64-domain ensemble measurement")
     ap.add_argument("--profile", action="store_true",
                     help="no in-graph timing events (for runs under ncu)")
     ap.add_argument("--grid", default=None,

@@ -421,6 +421,27 @@ les_status les_write_restart(les_ctx *ctx, const char *data20, const char *data2
 les_status les_read_restart(les_ctx *ctx, const char *data30, const char *data31, int *n,
                             float *time, float *fghold);
 
+/* ---- Batched ensemble: many domains, one graph launch per step -------------
+ * The reference advances one domain per run (main_ocl.f95:232-317); an
+ * ensemble of uneven domains is this library's addition.  Members are
+ * ordinary contexts, created, uploaded and (optionally) warmed up by the
+ * caller, each with its own grid, terrain, inflow and autotuned SOR pass
+ * shape; the ensemble borrows them (destroy it before them).
+ * les_ensemble_step advances every member from step n0 to n0+nsteps-1 with
+ * one cudaGraphLaunch per step: each member's step is a branch of one
+ * captured graph, so the members' kernels run concurrently.  Results equal
+ * les_step on each member, bit for bit.  Work queued earlier on a member's
+ * stream runs first, and work queued on it afterwards (downloads,
+ * les_last_metrics, les_step) waits for the ensemble's steps. */
+typedef struct les_ensemble les_ensemble;
+les_status les_ensemble_create(int nmembers, les_ctx *const *members, les_ensemble **ens);
+les_status les_ensemble_step(les_ensemble *ens, int n0, int nsteps);
+les_status les_ensemble_sync(les_ensemble *ens);
+void *les_ensemble_stream(les_ensemble *ens);
+/* kernels launched by the ensemble so far (all members) */
+uint64_t les_ensemble_launch_count(les_ensemble *ens);
+les_status les_ensemble_destroy(les_ensemble *ens);
+
 #ifdef __cplusplus
 }
 #endif

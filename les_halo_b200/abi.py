@@ -119,6 +119,12 @@ _SIGS = {
     "les_aveflow_download": (C.c_int, [_P, C.POINTER(LesAveflowFields)]),
     "les_write_restart": (C.c_int, [_P, C.c_char_p, C.c_char_p, _P]),
     "les_read_restart": (C.c_int, [_P, C.c_char_p, C.c_char_p, _I, _F, _P]),
+    "les_ensemble_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "les_ensemble_step": (C.c_int, [_P, C.c_int, C.c_int]),
+    "les_ensemble_sync": (C.c_int, [_P]),
+    "les_ensemble_stream": (C.c_void_p, [_P]),
+    "les_ensemble_launch_count": (C.c_uint64, [_P]),
+    "les_ensemble_destroy": (C.c_int, [_P]),
 }
 
 # Per-routine entries: every argument is a pointer (Fortran by-reference).

@@ -1203,3 +1203,4 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 
 #include "les_routines_api.inc"
 #include "les_stats_io.inc"
+#include "les_ensemble.inc"

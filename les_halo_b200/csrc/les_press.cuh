@@ -289,6 +289,19 @@ __global__ void k_step_begin(Scal *s, int n) {
     s->exact_sums = 0;
     s->n = n;
 }
+// k_step_begin with n read from device memory (ensemble graphs: one
+// captured graph serves every step, k_ens_advance moves n on).
+__global__ void k_step_begin_dev(Scal *s, const int *n) {
+    s->uout_pos = 0u;
+    s->uout_neg = 0u;
+    s->converged = 0;
+    s->sor_iters = 0;
+    s->redo = 0;
+    s->pbuf = 0;
+    s->exact_sums = 0;
+    s->n = *n;
+}
+__global__ void k_ens_advance(int *n) { *n += 1; }
 __global__ void k_probe(Geo g, Fields F, Scal *s) {
     const int c = IX(g, g.im / 2, g.jm / 2, g.km / 2);
     s->probe[0] = F.p[c];

@@ -197,3 +197,36 @@ class GpuLes:
         abi.check(abi.lib().les_ctx_field(self.ctx, abi.FIELD_IDS.index(name), C.byref(d),
                                           C.byref(ox), C.byref(si), C.byref(sj), C.byref(sk)))
         return d.value, ox.value, si.value, sj.value, sk.value
+
+
+class Ensemble:
+    """Independent domains (GpuLes members) advanced by one graph launch per step."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.ctx.value for m in self.members])
+        self.h = C.c_void_p()
+        abi.check(abi.lib().les_ensemble_create(len(self.members), arr, C.byref(self.h)))
+
+    def step(self, n0, nsteps=1):
+        abi.check(abi.lib().les_ensemble_step(self.h, n0, nsteps))
+
+    def sync(self):
+        abi.check(abi.lib().les_ensemble_sync(self.h))
+
+    def stream(self) -> int:
+        return int(abi.lib().les_ensemble_stream(self.h) or 0)
+
+    def launches(self) -> int:
+        return int(abi.lib().les_ensemble_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            abi.lib().les_ensemble_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
