@@ -200,6 +200,7 @@ def run_reference(args):
     return 0
 
 
+REFINE = dict(outer=2, inner=50, tol=1e-9)
 ENSEMBLE = dict(members=64, size_lo=96, size_hi=256, kp=80, ustar_lo=0.2, ustar_hi=0.5, seed=2024)
 
 
@@ -359,6 +360,33 @@ def run_ours(args):
     torch.cuda.synchronize()
     ave_ms = ev2.elapsed_time(ev3) / ave_k
 
+    # FP64-refined press on the same state: FP64 rhsav, residual norms and
+    # pav, and REF_OUTER defect corrections of REF_INNER FP32 SOR iterations
+    # each after the plain sweeps; CUDA events around ref_k steps.
+    refined = None
+    if not args.profile and args.refine:
+        try:
+            outer, inner, tol = REFINE["outer"], REFINE["inner"], REFINE["tol"]
+            abi.check(L.les_press_refine_fp64(gpu.ctx, outer, inner, tol))
+            gpu.step(n, 1)
+            n += 1
+            ref_k = max(3, min(args.steps, 5))
+            torch.cuda.synchronize()
+            ev2.record(stream)
+            gpu.step(n, ref_k)
+            ev3.record(stream)
+            torch.cuda.synchronize()
+            n += ref_k
+            ref_ms = ev2.elapsed_time(ev3) / ref_k
+            rm = gpu.refine_metrics()
+            abi.check(L.les_press_refine_fp64(gpu.ctx, 0, 0, 0.0))
+            refined = {"outer": outer, "inner_sweeps": inner, "rel_tol": tol, "ms_per_step": round(ref_ms, 4),
+                       "mpts": round(cells / (ref_ms / 1e3) / 1e6, 1), "steps": ref_k,
+                       "rel_residual_after_fp32_sweeps": rm["rel_initial"],
+                       "rel_residual_final": rm["rel_final"], "corrections": rm["outer"]}
+        except Exception as exc:
+            refined = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+
     ms_total, e2e_s, value, e2e_val = job_rates(ms_total, e2e_s, cells, args.steps, e2e_steps, ws,
                                                 dist, "cuda")
     ms_step = ms_total / args.steps
@@ -407,6 +435,8 @@ def run_ours(args):
                     "path": "C ABI: les_set_wind_profile + les_step + les_ctx_halo_read/write x7 + "
                             "les_last_metrics, pinned host buffers, wall clock"},
             "clocks": clocks,
+            "refined_press": dict(refined, time_vs_plain=round(refined["ms_per_step"] / ms_step, 3))
+            if refined and "ms_per_step" in refined else refined,
             "aveflow": {"kernel": "k_ave_accum", "ms_per_call": round(ave_ms, 4),
                         "achieved": round(AVE_BYTES_PER_CELL * cells / (ave_ms / 1e3) / 1e9, 1),
                         "peak": peak, "unit": "GB/s",
@@ -434,6 +464,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-refine", dest="refine", action="store_false",
+                    help="skip the FP64-refined press measurement")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 64-domain ensemble measurement")
     ap.add_argument("--profile", action="store_true",

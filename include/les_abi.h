@@ -421,6 +421,25 @@ les_status les_write_restart(les_ctx *ctx, const char *data20, const char *data2
 les_status les_read_restart(les_ctx *ctx, const char *data30, const char *data31, int *n,
                             float *time, float *fghold);
 
+/* ---- FP64-refined pressure solve (no counterpart in the reference) -------
+ * outer > 0 turns it on for the following steps: after the plain FP32 SOR
+ * of press.f95:87-115, `outer` FP64 defect corrections follow, each
+ * r = b - A p64 in FP64 (b = rhs - rhsav with rhsav in FP64; A the operator
+ * the sweeps relax, cn1 included), A e = r by `inner` FP32 SOR iterations
+ * from e = 0, p64 += e; a correction is skipped once ||r||2/||b||2 <= rel_tol.
+ * pav (press.f95:123-133) is then formed in FP64 and p = (float)(p64 - pav)
+ * with its boundp1/boundp2 copies.  outer = 0 restores the plain press.
+ * Needs even jp (the inner sweeps are the temporal-blocked passes).
+ * les_last_refine_metrics reports the last step's FP64 rhsav and pav, the
+ * relative residual before the first and after the last correction, and
+ * the corrections applied. */
+typedef struct les_refine_metrics {
+    double rhsav, pav, rel_initial, rel_final;
+    int outer;
+} les_refine_metrics;
+les_status les_press_refine_fp64(les_ctx *ctx, int outer, int inner, double rel_tol);
+les_status les_last_refine_metrics(les_ctx *ctx, les_refine_metrics *m);
+
 /* ---- Batched ensemble: many domains, one graph launch per step -------------
  * The reference advances one domain per run (main_ocl.f95:232-317); an
  * ensemble of uneven domains is this library's addition.  Members are

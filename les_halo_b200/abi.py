@@ -53,6 +53,11 @@ class LesAveflowFields(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in AVEFLOW_CELL + AVEFLOW_COL]
 
 
+class LesRefineMetrics(C.Structure):
+    _fields_ = [("rhsav", C.c_double), ("pav", C.c_double), ("rel_initial", C.c_double),
+                ("rel_final", C.c_double), ("outer", C.c_int)]
+
+
 class LesSynthCfg(C.Structure):
     _fields_ = [("ip", C.c_int), ("jp", C.c_int), ("kp", C.c_int),
                 ("dx", C.c_float), ("dy", C.c_float), ("dz0", C.c_float), ("dz_growth", C.c_float),
@@ -125,6 +130,8 @@ _SIGS = {
     "les_ensemble_stream": (C.c_void_p, [_P]),
     "les_ensemble_launch_count": (C.c_uint64, [_P]),
     "les_ensemble_destroy": (C.c_int, [_P]),
+    "les_press_refine_fp64": (C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
+    "les_last_refine_metrics": (C.c_int, [_P, C.POINTER(LesRefineMetrics)]),
 }
 
 # Per-routine entries: every argument is a pointer (Fortran by-reference).

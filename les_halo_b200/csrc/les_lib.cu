@@ -22,6 +22,7 @@
 #include "les_routines.cuh"
 #include "les_sor_tb.cuh"
 #include "les_stats.cuh"
+#include "les_refine.cuh"
 #include "les_step.cuh"
 
 using namespace les;
@@ -190,13 +191,29 @@ struct les_ctx {
     bool force_exact_sor = false;    // testing: always the per-colour path
     bool sor_fp32_test = true;       // LES_SOR_SUMS=exact clears it: every pass sums exactly
     float *d_ave = nullptr;          // aveflow statistics (les_stats.cuh), allocated on first use
+    // FP64-refined press (les_refine.cuh): corrections per step, inner sweeps, tolerance
+    int ref_outer = 0, ref_inner = 0;
+    double ref_tol = 0.0;
+    double *d_p64 = nullptr;              // FP64 p (box)
+    float *d_r32 = nullptr, *d_e0 = nullptr, *d_e1 = nullptr;  // inner rhs and correction buffers
+    Scal *d_scal2 = nullptr;              // scalars of the inner sweeps
+    Ref64 *d_ref = nullptr;
+    double2 *d_dpart = nullptr;           // FP64 per-block partial sums
+};
+
+// Buffers of an SOR pass other than the context's p / second p / rhs / scalars.
+struct SorBufs {
+    float *pb0, *pb1;
+    const float *rhs;
+    Scal *sc;
 };
 
 namespace {
 
 float *field_ptr(les_ctx *c, int f) { return c->d_fields + (size_t)f * c->box_elems; }
 les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, int itmax,
-                         bool tuning = false);
+                         bool tuning = false, const SorBufs *bufs = nullptr);
+les_status enqueue_refine(les_ctx *c);
 bool tb_fast_ok(const les_ctx *c, const TbShape &sh);
 
 // Host copies of the 1-D tables -> device; builds cnA/B/C, smc, wind.
@@ -410,6 +427,7 @@ les_status enqueue_press(les_ctx *c, bool exact) {
     const long long n2 = 2LL * (g.im + 2) * (g.jm + 2);
     LAUNCH(c, k_rhs, rg, rb, g, c->F, c->red_kchunk, c->d_part);
     LAUNCH(c, k_final_rhsav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
+    if (c->ref_outer > 0) LAUNCH(c, k_ref_rhsav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_ref);
     MARK(c, EV_RHS);
     if (exact) {
         for (int l = 0; l < c->prm.nmaxp; ++l) {
@@ -448,6 +466,11 @@ les_status enqueue_press(les_ctx *c, bool exact) {
         }
     }
     MARK(c, EV_SOR_END);
+    if (c->ref_outer > 0) {
+        les_status st = enqueue_refine(c);
+        MARK(c, EV_PAV);
+        return st;
+    }
     LAUNCH(c, k_pav_reduce, rg, rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, c->red_kchunk, c->d_part, c->d_scal);
     LAUNCH(c, k_final_pav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
     LAUNCH(c, k_pav_adjust, dim3(c->red_gx, c->red_gy, g.km), rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p,
@@ -502,7 +525,8 @@ bool tb_fast_ok(const les_ctx *c, const TbShape &sh) {
 // step has itmax iterations.  tuning: read and write only the second p
 // buffer (scratch between steps), so timing passes leave the model state
 // alone.
-les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, int itmax, bool tuning) {
+les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, int itmax, bool tuning,
+                         const SorBufs *bufs) {
     const int kc = cdiv(c->prm.kp, sh.nch);
     const dim3 grid(cdiv(c->prm.ip, tb_tx(sh.T)), cdiv(c->prm.jp, sh.ty), cdiv(c->prm.kp, kc));
     const dim3 block(32 * tb_warps(sh.T, sh.ty));
@@ -521,6 +545,12 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     a.pjuge = pjuge;
     a.part = c->d_part;
     a.sc = c->d_scal;
+    if (bufs) {
+        a.pb0 = bufs->pb0;
+        a.pb1 = bufs->pb1;
+        a.rhs = bufs->rhs;
+        a.sc = bufs->sc;
+    }
     const Geo &g = c->geo;
 #define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a)
     switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
@@ -839,6 +869,13 @@ les_status les_ctx_destroy(les_ctx *c) {
     cudaFree(c->d_stage);
     cudaFree(c->d_p2);
     cudaFree(c->d_ave);
+    cudaFree(c->d_p64);
+    cudaFree(c->d_r32);
+    cudaFree(c->d_e0);
+    cudaFree(c->d_e1);
+    cudaFree(c->d_scal2);
+    cudaFree(c->d_ref);
+    cudaFree(c->d_dpart);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ok();
@@ -998,7 +1035,7 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
         const int n = n0 + s;
         const bool exact = c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok;
         const int gi = ((n == 1 && c->prm.ical == 0) ? 1 : 0) + (exact ? 2 : 0);
-        if (!exact && c->tb.T == 0) {
+        if ((!exact || c->ref_outer > 0) && c->tb.T == 0) {  // the refined press uses the passes too
             les_status st = autotune_sor(c);
             if (st != LES_OK) return st;
         }
@@ -1204,3 +1241,4 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 #include "les_routines_api.inc"
 #include "les_stats_io.inc"
 #include "les_ensemble.inc"
+#include "les_refine.inc"

@@ -184,6 +184,14 @@ class GpuLes:
                                              None if fghold is None else FL.ptr(fghold)))
         return n.value, t.value
 
+    def press_refine_fp64(self, outer, inner, rel_tol=0.0):
+        abi.check(abi.lib().les_press_refine_fp64(self.ctx, outer, inner, rel_tol))
+
+    def refine_metrics(self) -> dict:
+        m = abi.LesRefineMetrics()
+        abi.check(abi.lib().les_last_refine_metrics(self.ctx, C.byref(m)))
+        return {n: getattr(m, n) for n, _ in m._fields_}
+
     def launches(self) -> int:
         return int(abi.lib().les_ctx_launch_count(self.ctx))
 

@@ -75,6 +75,9 @@ def lib():
             [C.c_int, C.c_float, C.c_float] + [_P] * 3
         L.oracle_press_ex.restype = C.c_int
         L.oracle_aveflow.argtypes = [C.c_int] * 5 + [_P] * 22 + [C.c_int, _P]
+        L.oracle_set_press_refine.argtypes = [C.c_int, C.c_int, C.c_double]
+        L.oracle_last_refine.argtypes = [C.POINTER(C.c_double)]
+        L.oracle_last_refine.restype = C.c_int
         _lib = L
     return _lib
 
@@ -165,3 +168,14 @@ def aveflow(case, stats: dict, n, n1, nmax):
     col = [ptr(stats[k]) for k in AVE_COL]
     lib().oracle_aveflow(n, n1, case.kp, case.jp, case.ip, *c, *col[:6], ptr(A["u"]), ptr(A["v"]),
                          ptr(A["w"]), ptr(A["p"]), ptr(A["sm"]), nmax, col[6])
+
+
+def set_press_refine(outer, inner, tol):
+    """FP64-refined press for the following oracle steps (outer = 0: plain)."""
+    lib().oracle_set_press_refine(outer, inner, tol)
+
+
+def last_refine():
+    out = (C.c_double * 4)()
+    n = lib().oracle_last_refine(out)
+    return {"rhsav": out[0], "pav": out[1], "rel_initial": out[2], "rel_final": out[3], "outer": n}

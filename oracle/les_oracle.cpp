@@ -60,6 +60,11 @@ inline A1 mk1(const float *p, int l) { return A1{const_cast<float *>(p), l}; }
 
 int g_red_mode = ORACLE_RED_CANONICAL;
 float g_last_uout = 0.0f;
+// FP64-refined press (oracle_set_press_refine): settings and last report
+int g_ref_outer = 0, g_ref_inner = 0;
+double g_ref_tol = 0.0;
+double g_ref_out[4] = {0, 0, 0, 0};  // rhsav, pav, rel_initial, rel_final
+int g_ref_done = 0;
 
 // ---------------------------------------------------------------------------
 // Canonical global sum (shared definition with the CUDA kernels).
@@ -114,6 +119,15 @@ double canonical_sum3(int im, int jm, int km, F x) {
 extern "C" {
 
 void oracle_set_reduction_mode(int mode) { g_red_mode = mode; }
+void oracle_set_press_refine(int outer, int inner, double tol) {
+    g_ref_outer = outer;
+    g_ref_inner = inner;
+    g_ref_tol = tol;
+}
+int oracle_last_refine(double *out4) {
+    for (int q = 0; q < 4; ++q) out4[q] = g_ref_out[q];
+    return g_ref_done;
+}
 int oracle_get_reduction_mode(void) { return g_red_mode; }
 float oracle_last_uout(void) { return g_last_uout; }
 
@@ -1046,6 +1060,107 @@ void oracle_boundp1(int km, int jm, float *p_, int im) {
 }
 
 // press.f95:49-146
+// FP64-refined press after the FP32 SOR (the CUDA path's les_refine.cuh):
+// p64 = p; for m = 0..M: r = b - A p64 (FP64, b = rhs_raw - rhsav64, A the
+// operator the sweeps relax with the boundp1/boundp2 neighbours), the
+// relative residual and the stop test; if m < M and not stopped: A e = r by
+// `inner` FP32 SOR iterations from e = 0 (press.f95:87-115 with rhs = (float)
+// r, no rhsav, no stop test), p64 += e.  Then pav in FP64 and
+// p = (float)(p64 - pav) with boundp1/boundp2.  Returns (float) pav.
+static float oracle_refine_tail(int km, int jm, int im, float *p_, const float *rraw, double rav,
+                                const float *dx1_, const float *dy1_, const float *dzn_, const float *cn1_,
+                                const float *cn2l_, const float *cn2s_, const float *cn3l_, const float *cn3s_,
+                                const float *cn4l_, const float *cn4s_, float omega) {
+    const int ip = im, jp = jm, kp = km;
+    A3 p = ARR_P(p_), cn1 = ARR_I(cn1_);
+    A1 dx1 = mk1(dx1_, -1), dy1 = mk1(dy1_, 0), dzn = mk1(dzn_, -1);
+    A1 cn2l = mk1(cn2l_, 1), cn2s = mk1(cn2s_, 1), cn3l = mk1(cn3l_, 1), cn3s = mk1(cn3s_, 1),
+       cn4l = mk1(cn4l_, 1), cn4s = mk1(cn4s_, 1);
+    const size_t n = (size_t)im * jm * km;
+    auto at = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)); };
+    std::vector<double> p64(n);
+    for (int k = 1; k <= km; ++k)
+        for (int j = 1; j <= jm; ++j)
+            for (int i = 1; i <= im; ++i) p64[at(i, j, k)] = (double)p(i, j, k);
+    std::vector<float> er_((size_t)(ip + 2) * (jp + 2) * (kp + 2), 0.0f), e_((size_t)(ip + 3) * (jp + 3) * (kp + 2));
+    A3 er = ARR_RHS(er_.data()), e = ARR_P(e_.data());
+    double bnorm2 = 0.0, rel = 0.0;
+    bool stop = false;
+    g_ref_done = 0;
+    for (int m = 0; m <= g_ref_outer; ++m) {
+        double r2 = 0.0, b2 = 0.0;
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) {
+                    const int jn = (j == jm) ? 1 : j + 1, js = (j == 1) ? jm : j - 1;
+                    const double pc = p64[at(i, j, k)];
+                    const double pe = (i == im) ? pc : p64[at(i + 1, j, k)];
+                    const double pw = (i == 1) ? pc : p64[at(i - 1, j, k)];
+                    const double pn = p64[at(i, jn, k)], ps = p64[at(i, js, k)];
+                    const double pu = (k == km) ? pc : p64[at(i, j, k + 1)];
+                    const double pd = (k == 1) ? pc : p64[at(i, j, k - 1)];
+                    const double diag = 1.0 / (double)cn1(i, j, k);
+                    double s = (double)cn2l(i) * pe;
+                    s = s + (double)cn2s(i) * pw;
+                    s = s + (double)cn3l(j) * pn;
+                    s = s + (double)cn3s(j) * ps;
+                    s = s + (double)cn4l(k) * pu;
+                    s = s + (double)cn4s(k) * pd;
+                    const double ap = s - pc * diag;
+                    const double b = (double)rraw[at(i, j, k)] - rav;
+                    const double r = b - ap;
+                    er(i, j, k) = (float)r;
+                    r2 += r * r;
+                    b2 += b * b;
+                }
+        if (m == 0) bnorm2 = b2;
+        rel = bnorm2 > 0.0 ? std::sqrt(r2 / bnorm2) : 0.0;
+        if (m == 0) g_ref_out[2] = rel;
+        g_ref_out[3] = rel;
+        if (rel <= g_ref_tol) stop = true;
+        if (stop || m == g_ref_outer) break;
+        std::fill(e_.begin(), e_.end(), 0.0f);
+        for (int l = 1; l <= g_ref_inner; ++l) {
+            for (int nrd = 0; nrd <= 1; ++nrd) {
+                for (int k = 1; k <= km; ++k)
+                    for (int j = 1; j <= jm; ++j)
+                        for (int i = 1 + (k + j + nrd) % 2; i <= im; i += 2) {
+                            const float reltmp =
+                                omega * (cn1(i, j, k) * (cn2l(i) * e(i + 1, j, k) + cn2s(i) * e(i - 1, j, k) +
+                                                         cn3l(j) * e(i, j + 1, k) + cn3s(j) * e(i, j - 1, k) +
+                                                         cn4l(k) * e(i, j, k + 1) + cn4s(k) * e(i, j, k - 1) -
+                                                         er(i, j, k)) -
+                                         e(i, j, k));
+                            e(i, j, k) = e(i, j, k) + reltmp;
+                        }
+                oracle_boundp1(km, jm, e_.data(), im);
+            }
+            oracle_boundp2(jm, im, e_.data(), km);
+        }
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) p64[at(i, j, k)] = p64[at(i, j, k)] + (double)e(i, j, k);
+        ++g_ref_done;
+    }
+    double num = 0.0, den = 0.0;
+    for (int k = 1; k <= km; ++k)
+        for (int j = 1; j <= jm; ++j)
+            for (int i = 1; i <= im; ++i) {
+                const double w = (double)dx1(i) * (double)dy1(j) * (double)dzn(k);
+                num += p64[at(i, j, k)] * w;
+                den += w;
+            }
+    const double pav = num / den;
+    g_ref_out[0] = rav;
+    g_ref_out[1] = pav;
+    for (int k = 1; k <= km; ++k)
+        for (int j = 1; j <= jm; ++j)
+            for (int i = 1; i <= im; ++i) p(i, j, k) = (float)(p64[at(i, j, k)] - pav);
+    oracle_boundp1(km, jm, p_, im);
+    oracle_boundp2(jm, im, p_, km);
+    return (float)pav;
+}
+
 int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const float *dx1_,
                     const float *v_, const float *dy1_, const float *w_, const float *dzn_,
                     float *f_, float *g_, float *h_, float dt, const float *cn1_,
@@ -1073,12 +1188,22 @@ int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const 
                                (h(i, j, k) - h(i, j, k - 1)) / dzn(k) + rhs(i, j, k) / dt;
             }
     float rhsav;
+    double rhsav64 = 0.0;
+    const bool refine = canon && g_ref_outer > 0;
+    std::vector<float> rraw;  // rhs before the rhsav subtraction (refined press)
+    if (refine) {
+        rraw.resize((size_t)im * jm * km);
+        for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+                for (int i = 1; i <= im; ++i) rraw[(i - 1) + (size_t)im * ((j - 1) + (size_t)jm * (k - 1))] = rhs(i, j, k);
+    }
     if (canon) {
         const double num = canonical_sum3(
             im, jm, km, [&](int i, int j, int k) { return dx1(i) * dy1(j) * dzn(k) * rhs(i, j, k); });
         const double den =
             canonical_sum3(im, jm, km, [&](int i, int j, int k) { return dx1(i) * dy1(j) * dzn(k); });
-        rhsav = (float)(num / den);
+        rhsav64 = num / den;
+        rhsav = (float)rhsav64;
     } else {
         float s = 0.0f, area = 0.0f;
         for (int k = 1; k <= km; ++k)
@@ -1133,6 +1258,14 @@ int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const 
         if (sor < pjuge) break;
     }
 
+    if (refine) {
+        const float pav = oracle_refine_tail(km, jm, im, p_, rraw.data(), rhsav64, dx1_, dy1_, dzn_, cn1_, cn2l_,
+                                             cn2s_, cn3l_, cn3s_, cn4l_, cn4s_, omega);
+        if (sor_out) *sor_out = sor;
+        if (rhsav_out) *rhsav_out = rhsav;
+        if (pav_out) *pav_out = pav;
+        return l_exec;
+    }
     float pav;
     if (canon) {
         const double num = canonical_sum3(

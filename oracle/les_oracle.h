@@ -34,6 +34,11 @@ enum { ORACLE_RED_CANONICAL = 0, ORACLE_RED_FAITHFUL = 1 };
 
 void oracle_set_reduction_mode(int mode);
 int oracle_get_reduction_mode(void);
+/* FP64-refined press (the CUDA path's les_press_refine_fp64): outer = 0 is
+ * the plain press.  oracle_last_refine fills rhsav, pav, rel_initial,
+ * rel_final of the last press and returns the corrections applied. */
+void oracle_set_press_refine(int outer, int inner, double tol);
+int oracle_last_refine(double *out4);
 
 /* set.f95:76-82 physical constants (vn computed as the Fortran does). */
 void oracle_constants(float *ro, float *vn, float *alpha, float *beta);
