@@ -23,7 +23,9 @@ enum { V_D1 = 0, V_C1 = 9, NV = 18 };
 // around the tile per plane, five plane slots (k-1..k+2 in use, k+3 loading).
 // Band row b holds real row jwrap(jb2 + b); a real row j is found by moving
 // it by +-jm into the band.  Valid when the band is not taller than jm.
-constexpr int kBW = kMX + 4, kBH = kMY + 4, kBA = kBW * kBH, kBS = 5;
+// band: 36 x 12 positions per plane, four plane slots (three read by a fill,
+// one arriving)
+constexpr int kBW = kMX + 4, kBH = kMY + 4, kBA = kBW * kBH, kBS = 4;
 struct UVWBand : DivIEEE {
     const float *base;  // slot s, field f at base + (s*3 + f)*kBA
     int ib2, jb2;       // real (i, j) of band position (0, 0)
@@ -453,8 +455,8 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
             tile_plane<DIU_ONLY, false>(g, qg, dst, prv7, prv8, ib, jb, k, save);
     };
     const BandCopies bc = BAND ? BandCopies(g, F, i0 - 2, j0 - 2) : BandCopies();
-    if (BAND) {  // planes -1..1 and 0..2 fill the first two face planes; 3 is needed at k=1
-        for (int k = -1; k <= 3; ++k) bc.load(band, k);
+    if (BAND) {  // planes -1..1 and 0..2 fill the first two face planes
+        for (int k = -1; k <= 2; ++k) bc.load(band, k);
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
@@ -501,6 +503,15 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
     fill(s0, 0, false);
     fill(s1, 1, false);
     __syncthreads();
+    if (BAND) {  // plane 3 (needed at k = 1) takes the slot of plane -1, free after the fills
+        bc.load(band, 3);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+    }
+    // In the march, plane k+3 goes into the slot of plane k-1, whose last
+    // reader (the fill of plane k at step k-1) finished before the barrier
+    // that ends step k-1.
     for (int k = 1; k <= g.km; ++k) {
         pre(k);
         if (BAND) {  // plane k+3 streams in while plane k+1 is filled from k..k+2
