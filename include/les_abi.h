@@ -440,6 +440,30 @@ typedef struct les_refine_metrics {
 les_status les_press_refine_fp64(les_ctx *ctx, int outer, int inner, double rel_tol);
 les_status les_last_refine_metrics(les_ctx *ctx, les_refine_metrics *m);
 
+/* ---- NetCDF output: src/OpenCL/module_LES_write_netcdf.f95 ------------------
+ * les_netcdf_open is init_netcdf_file (:105-322): it creates
+ * <prefix>LES_output.nc and LES_output_p.nc (pressure, hPa), LES_output_u/_v/_w.nc
+ * (velocity_x/_y/_z, m/s) and LES_output_uvwsum.nc (velocity_sum_x/_y/_z),
+ * each with dimensions level, latitude, longitude (the full Fortran extents of
+ * its arrays, ghosts included: p (ip+3,jp+3,kp+2), u and v (ip+2,jp+3,kp+2),
+ * w (ip+2,jp+3,kp+3), usum.. (ip+1,jp+1,kp+1)) and a time dimension of
+ * `ntimes` slots (NTIMESTEPS = 20 in the reference), the coordinate variables
+ * latitude, longitude (1..n) and time (1..ntimes) and their units.  prefix is
+ * prepended to the file names (NULL: "./").  les_netcdf_write puts time slot t
+ * (1-based; the reference passes n/1000) of the context's p, u, v, w, usum,
+ * vsum, wsum (write_to_netcdf_file, :324-357); les_netcdf_write_host does the
+ * same from host arrays with those Fortran bounds.  les_netcdf_close
+ * (close_netcdf_file, :359-386) fills the slots never written with the
+ * default float fill value and closes.  Classic format, 64-bit offsets when a
+ * file reaches 2 GiB. */
+typedef struct les_netcdf les_netcdf;
+les_status les_netcdf_open(const char *prefix, int ip, int jp, int kp, int ntimes, les_netcdf **nc);
+les_status les_netcdf_write(les_netcdf *nc, les_ctx *ctx, int t);
+les_status les_netcdf_write_host(les_netcdf *nc, int t, const float *p, const float *u, const float *v,
+                                 const float *w, const float *usum, const float *vsum,
+                                 const float *wsum);
+les_status les_netcdf_close(les_netcdf *nc);
+
 /* ---- Batched ensemble: many domains, one graph launch per step -------------
  * The reference advances one domain per run (main_ocl.f95:232-317); an
  * ensemble of uneven domains is this library's addition.  Members are

@@ -131,6 +131,10 @@ _SIGS = {
     "les_ensemble_launch_count": (C.c_uint64, [_P]),
     "les_ensemble_destroy": (C.c_int, [_P]),
     "les_press_refine_fp64": (C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
+    "les_netcdf_open": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "les_netcdf_write": (C.c_int, [_P, _P, C.c_int]),
+    "les_netcdf_write_host": (C.c_int, [_P, C.c_int] + [_P] * 7),
+    "les_netcdf_close": (C.c_int, [_P]),
     "les_last_refine_metrics": (C.c_int, [_P, C.POINTER(LesRefineMetrics)]),
 }
 

@@ -15,7 +15,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liblesb200.so"
-SOURCES = ["les_lib.cu", "les_setup.cu", "les_noalloc.cu"]
+SOURCES = ["les_lib.cu", "les_setup.cu", "les_noalloc.cu", "les_netcdf.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 NVCC_FLAGS = [

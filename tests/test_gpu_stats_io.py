@@ -164,3 +164,23 @@ def test_restart_reader_rejects_bad_files(require_gpu, tmp_path):
     assert st == abi.LES_ERR_IO and "fghold" in L.les_last_error_string().decode()
     assert L.les_read_restart(g.ctx, str(d30).encode(), str(d31).encode(), None, None, None) == abi.LES_OK
     g.close()
+
+
+def test_netcdf_from_the_device_state(require_gpu, tmp_path):
+    from scipy.io import netcdf_file
+    ip, jp, kp = 20, 14, 9
+    _, dev = _pair(ip, jp, kp, seed=12)
+    g = GpuLes(dev)
+    g.warmup(1)
+    g.step(1, 2)
+    L = abi.lib()
+    h = C.c_void_p()
+    abi.check(L.les_netcdf_open(f"{tmp_path}/".encode(), ip, jp, kp, 3, C.byref(h)))
+    abi.check(L.les_netcdf_write(h, g.ctx, 2))
+    abi.check(L.les_netcdf_close(h))
+    st = g.download(["p", "u", "w", "usum"])
+    for fname, var, src in (("LES_output_p.nc", "pressure", "p"), ("LES_output_u.nc", "velocity_x", "u"),
+                            ("LES_output_w.nc", "velocity_z", "w"), ("LES_output_uvwsum.nc", "velocity_sum_x", "usum")):
+        with netcdf_file(str(tmp_path / fname), "r", mmap=False) as f:
+            assert np.array_equal(f.variables[var][1].copy(), st[src].T)
+    g.close()
