@@ -15,8 +15,12 @@
 namespace les {
 namespace {  // kernels get internal linkage: each .cu has its own copy
 
-constexpr int kMX = 32, kMY = 8, kMNT = 256;
+// tile 32 x 8 cells; 352 threads (11 warps): one per ring position of the
+// 34 x 10 face-value planes, so a plane fills in one pass; the first 256
+// own the tile's cells
+constexpr int kMX = 32, kMY = 8, kMNT = 352;
 constexpr int kMEX = kMX + 2, kMEY = kMY + 2, kMPOS = kMEX * kMEY;
+static_assert(kMNT % 32 == 0 && kMNT >= kMPOS && kMNT >= kMX * kMY, "one thread per ring position");
 enum { V_D1 = 0, V_C1 = 9, NV = 18 };
 
 // u, v, w staged in shared memory: a band of (32+4) x (8+4) columns/rows
@@ -566,7 +570,7 @@ __device__ __forceinline__ bool tile_interior_b(const Geo &g) {
 template <bool BAND, bool P2>
 __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
-    const bool mine = (i <= g.im && j <= g.jm);
+    const bool mine = threadIdx.x < kMX * kMY && i <= g.im && j <= g.jm;
     // the cell's own inputs of plane k (feedbf.f95:38-66, velFG's h), loaded
     // ahead by pre(k); only this thread writes them
     float h0 = 0, u0 = 0, v0 = 0, w0 = 0, us0 = 0, vs0 = 0, ws0 = 0, bm0 = 0, cm0 = 0, dm0 = 0;
@@ -613,7 +617,7 @@ __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
 template <bool ADAM, bool BAND, bool P2>
 __global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
-    const bool mine = (i <= g.im && j <= g.jm);
+    const bool mine = threadIdx.x < kMX * kMY && i <= g.im && j <= g.jm;
     // the cell's f, g, h (and fold, gold, hold) of plane k, loaded ahead by
     // pre(k); only this thread writes them
     float f0 = 0, g0 = 0, hh0 = 0, fo0 = 0, go0 = 0, ho0 = 0;
