@@ -33,11 +33,28 @@ struct FixPart {
 
 LES_HD i128 fix_term(float x, int &bad) {
 #if defined(__CUDA_ARCH__)
-    const uint32_t b = __float_as_uint(x);
+    // The same integer without a variable 128-bit shift: |x| = t + f with
+    // t = trunc(|x|) and f = |x| - t, both exact in FP32, so
+    // trunc(|x| * 2^64) = t * 2^64 + trunc(f * 2^64), each part one
+    // truncating conversion (f * 2^64 is a power-of-two scaling, exact).
+    const float a = fabsf(x);
+    if (!(a < 4.611686018427388e18f)) {  // NaN, inf or >= 2^62
+        bad = 1;
+        return 0;
+    }
+    unsigned long long ip = 0ull, fr;
+    if (a < 1.0f) {
+        fr = __float2ull_rz(a * 18446744073709551616.0f);
+    } else {
+        const float t = truncf(a);
+        ip = __float2ull_rz(t);
+        fr = __float2ull_rz((a - t) * 18446744073709551616.0f);
+    }
+    const i128 m = (i128)(((unsigned __int128)ip << 64) | (unsigned __int128)fr);
+    return signbit(x) ? -m : m;
 #else
     uint32_t b;
     memcpy(&b, &x, 4);
-#endif
     const int e = (int)((b >> 23) & 0xffu);
     if (e == 255) {
         bad = 1;
@@ -59,6 +76,7 @@ LES_HD i128 fix_term(float x, int &bad) {
     else
         m = 0;
     return (b >> 31) ? -m : m;
+#endif
 }
 
 LES_HD double fix_finish(i128 t, int bad) {
