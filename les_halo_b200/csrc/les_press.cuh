@@ -25,6 +25,8 @@ __global__ void __launch_bounds__(kRedNT) k_rhs(Geo g, Fields F, int kchunk, Fix
     int bad = 0;
     if (i <= g.im && j <= g.jm) {
         const float *dx1 = g.dx1, *dy1 = g.dy1, *dzn = g.dzn;
+        // RN(1/dt) for kdiv; 0 (IEEE division) outside [2^-30, 2^30]
+        const float rdt = (g.dt >= 0x1p-30f && g.dt <= 0x1p30f) ? 1.0f / g.dt : 0.0f;
         for (int k = k0; k <= k1; ++k) {
             // every load first (no store below writes a location any thread
             // reads), then the bondfg ghost writes, then rhs
@@ -45,8 +47,13 @@ __global__ void __launch_bounds__(kRedNT) k_rhs(Geo g, Fields F, int kchunk, Fix
                 hc = 0.0f;
             }
             if (k == 1) F.h[IX(g, i, j, 0)] = 0.0f;
-            float r = (-um + uc) / dx1[i] + (-vm + vc) / dy1[j] + (-wm + wc) / dzn[k];
-            r = (fc - fm) / dx1[i] + (gc - gm) / dy1[j] + (hc - hm) / dzn[k] + r / g.dt;
+            // the quotients of press.f95:59-70 with the IEEE bits: by an x/y
+            // spacing, a multiplication when its reciprocal is an exact power
+            // of two (fdiv); by dzn(k) and dt, Markstein's corrected quotient
+            // from the rounded reciprocal (kdiv)
+            const float rdx = g.rdx1[i], rdy = g.rdy1[j], dz = dzn[k], rdz = g.rdzn[k];
+            float r = fdiv(-um + uc, dx1[i], rdx) + fdiv(-vm + vc, dy1[j], rdy) + kdiv(-wm + wc, dz, rdz);
+            r = fdiv(fc - fm, dx1[i], rdx) + fdiv(gc - gm, dy1[j], rdy) + kdiv(hc - hm, dz, rdz) + kdiv(r, g.dt, rdt);
             F.rhs[c] = r;
             acc += fix_term(dx1[i] * dy1[j] * dzn[k] * r, bad);
         }
