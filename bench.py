@@ -204,59 +204,107 @@ REFINE = dict(outer=2, inner=50, tol=1e-9)
 ENSEMBLE = dict(members=64, size_lo=96, size_hi=256, kp=80, ustar_lo=0.2, ustar_hi=0.5, seed=2024)
 
 
-def ensemble_bench(steps, warmup):
+def ensemble_members():
+    """The ensemble's domains, the same on every rank: (ip, jp, u*, seed)."""
+    E = ENSEMBLE
+    rng = np.random.default_rng(E["seed"])
+    out = []
+    for m in range(E["members"]):
+        ip, jp = (int(x) for x in rng.integers(E["size_lo"], E["size_hi"] + 1, size=2))
+        out.append((ip, jp, float(rng.uniform(E["ustar_lo"], E["ustar_hi"])), E["seed"] + 1 + m))
+    return out
+
+
+def shard_members(cells, ws):
+    """Greedy balance of independent members over ws ranks: largest first,
+    each onto the least-loaded rank (ties: lower rank).  Returns each rank's
+    member indices in increasing order."""
+    load, out = [0] * ws, [[] for _ in range(ws)]
+    for m in sorted(range(len(cells)), key=lambda q: (-cells[q], q)):
+        r = min(range(ws), key=lambda q: (load[q], q))
+        out[r].append(m)
+        load[r] += cells[m]
+    return [sorted(x) for x in out]
+
+
+def ensemble_job(ms, cells, failed, dist=None, device="cpu"):
+    """Max-over-ranks ensemble time, total cells of all ranks, and whether
+    any rank failed (the same collectives on every rank, failed or not)."""
+    import torch
+    t = torch.tensor([ms, float(failed)], dtype=torch.float64, device=device)
+    c = torch.tensor([float(cells)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t[0]), int(c[0]), bool(t[1] > 0)
+
+
+def ensemble_bench(steps, warmup, ws=1, rank=0, dist=None):
     """64 uneven domains (ip, jp ~ U{96..256}, kp=80, own terrain seed, u* ~
-    U[0.2, 0.5]) advanced `steps` steps by one graph launch per step, and the
-    same members advanced one after another with les_step (64 sequential
-    runs); CUDA events on the launching streams."""
+    U[0.2, 0.5]) advanced `steps` steps by one graph launch per step; under
+    torchrun the members are sharded over the ranks (shard_members, no
+    collective on the data path) and the time is the slowest rank's.  On one
+    GPU the same members are also advanced one after another with les_step
+    (64 sequential runs).  CUDA events on the launching streams."""
     import torch
     import les_halo_b200 as lh
     E = ENSEMBLE
-    rng = np.random.default_rng(E["seed"])
-    members, cells = [], 0
-    for m in range(E["members"]):
-        ip, jp = (int(x) for x in rng.integers(E["size_lo"], E["size_hi"] + 1, size=2))
-        ustar = float(rng.uniform(E["ustar_lo"], E["ustar_hi"]))
-        case = lh.synthetic_case(ip, jp, E["kp"], seed=E["seed"] + 1 + m, dt=0.05, nmaxp=50,
-                                 ustar=ustar)
-        g = lh.GpuLes(case)
-        g.warmup(1)
-        members.append(g)
-        cells += ip * jp * E["kp"]
-    ens = lh.Ensemble(members)
-    ens.step(1, warmup)
-    ens.sync()
-    st = torch.cuda.ExternalStream(ens.stream())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    l0 = ens.launches()
-    e0.record(st)
-    ens.step(1 + warmup, steps)
-    e1.record(st)
-    torch.cuda.synchronize()
-    ens_ms = e0.elapsed_time(e1)
-    launches = ens.launches() - l0
-    n = 1 + warmup + steps
-    seq_ms = 0.0
-    for g in members:  # one run after another
-        ms = torch.cuda.ExternalStream(g.stream())
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(ms)
-        g.step(n, steps)
-        b.record(ms)
+    doms = ensemble_members()
+    mine = shard_members([ip * jp * E["kp"] for ip, jp, _, _ in doms], ws)[rank]
+    err, ens_ms, cells, launches, seq_ms = None, float("nan"), 0, 0, None
+    members, ens = [], None
+    try:
+        for m in mine:
+            ip, jp, ustar, seed = doms[m]
+            case = lh.synthetic_case(ip, jp, E["kp"], seed=seed, dt=0.05, nmaxp=50, ustar=ustar)
+            g = lh.GpuLes(case)
+            g.warmup(1)
+            members.append(g)
+            cells += ip * jp * E["kp"]
+        ens = lh.Ensemble(members)
+        ens.step(1, warmup)
+        ens.sync()
+        st = torch.cuda.ExternalStream(ens.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ens.launches()
+        e0.record(st)
+        ens.step(1 + warmup, steps)
+        e1.record(st)
         torch.cuda.synchronize()
-        seq_ms += a.elapsed_time(b)
-    ens.close()
-    for g in members:
-        g.close()
-    return {"members": E["members"], "cells": cells, "kp": E["kp"], "steps": steps,
-            "ensemble_mpts": round(cells * steps / (ens_ms / 1e3) / 1e6, 1),
-            "ensemble_ms_per_step": round(ens_ms / steps, 3),
-            "sequential_mpts": round(cells * steps / (seq_ms / 1e3) / 1e6, 1),
-            "sequential_ms_per_step": round(seq_ms / steps, 3),
-            "speedup": round(seq_ms / ens_ms, 3), "graph_launches_per_step": 1,
-            "kernels_per_step": int(launches // max(steps, 1)),
-            "config": f"ip,jp ~ U{{{E['size_lo']}..{E['size_hi']}}}, kp={E['kp']}, u* ~ "
-                      f"U[{E['ustar_lo']},{E['ustar_hi']}], seed {E['seed']}"}
+        ens_ms = e0.elapsed_time(e1)
+        launches = ens.launches() - l0
+        if ws == 1:
+            n, seq_ms = 1 + warmup + steps, 0.0
+            for g in members:  # one run after another
+                ms = torch.cuda.ExternalStream(g.stream())
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(ms)
+                g.step(n, steps)
+                b.record(ms)
+                torch.cuda.synchronize()
+                seq_ms += a.elapsed_time(b)
+    except Exception as exc:  # reported, never fatal to the headline line
+        err = f"{type(exc).__name__}: {exc}"[:300]
+    finally:
+        if ens is not None:
+            ens.close()
+        for g in members:
+            g.close()
+    ens_ms, cells_all, failed = ensemble_job(ens_ms if err is None else float("inf"), cells, err is not None,
+                                             dist, "cuda" if dist is not None else "cpu")
+    if failed:
+        return {"error": err or "failed on another rank"}
+    out = {"members": E["members"], "cells": cells_all, "kp": E["kp"], "steps": steps, "ranks": ws,
+           "sharding": "greedy cell-count balance, no collective on the data path",
+           "ensemble_mpts": round(cells_all * steps / (ens_ms / 1e3) / 1e6, 1),
+           "ensemble_ms_per_step": round(ens_ms / steps, 3), "graph_launches_per_step": 1,
+           "kernels_per_step_rank0": int(launches // max(steps, 1)),
+           "config": f"ip,jp ~ U{{{E['size_lo']}..{E['size_hi']}}}, kp={E['kp']}, u* ~ "
+                     f"U[{E['ustar_lo']},{E['ustar_hi']}], seed {E['seed']}"}
+    if seq_ms is not None:
+        out.update(sequential_mpts=round(cells_all * steps / (seq_ms / 1e3) / 1e6, 1),
+                   sequential_ms_per_step=round(seq_ms / steps, 3), speedup=round(seq_ms / ens_ms, 3))
+    return out
 
 
 def run_ours(args):
@@ -406,6 +454,10 @@ def run_ours(args):
             traffic = json.loads(tf.read_text()).get("bytes_per_launch")
         except Exception:
             traffic = None
+    # every rank takes part (its shard of the members, and the collectives)
+    ens_line = None
+    if not args.profile and not args.no_ensemble:
+        ens_line = ensemble_bench(args.steps, args.warmup, ws, rank, dist)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mpts/s", "n_gpus": ws,
@@ -443,11 +495,8 @@ def run_ours(args):
                         "frac": round(AVE_BYTES_PER_CELL * cells / (ave_ms / 1e3) / 1e9 / peak, 4),
                         "bytes_per_cell": AVE_BYTES_PER_CELL, "calls": ave_k},
         }
-        if ws == 1 and not args.profile and not args.no_ensemble:
-            try:
-                line["ensemble"] = ensemble_bench(args.steps, args.warmup)
-            except Exception as exc:  # reported, never fatal to the headline line
-                line["ensemble"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+        if ens_line is not None:
+            line["ensemble"] = ens_line
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
