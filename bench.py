@@ -489,7 +489,8 @@ def run_ours(args):
             "clocks": clocks,
             "refined_press": dict(refined, time_vs_plain=round(refined["ms_per_step"] / ms_step, 3))
             if refined and "ms_per_step" in refined else refined,
-            "aveflow": {"kernel": "k_ave_accum", "ms_per_call": round(ave_ms, 4),
+            "aveflow": {"kernel": "k_ave_accum4" if case.ip % 4 == 0 else "k_ave_accum",
+                        "ms_per_call": round(ave_ms, 4),
                         "achieved": round(AVE_BYTES_PER_CELL * cells / (ave_ms / 1e3) / 1e9, 1),
                         "peak": peak, "unit": "GB/s",
                         "frac": round(AVE_BYTES_PER_CELL * cells / (ave_ms / 1e3) / 1e9 / peak, 4),

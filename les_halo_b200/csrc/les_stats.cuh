@@ -64,6 +64,58 @@ __global__ void k_ave_accum(Geo g, Fields F, AveBuf A, int first) {
     if (first) A.cell(AV_L)[t] = 0.0f;
 }
 
+// k_ave_accum for four consecutive i per thread (ip a multiple of 4): the
+// box rows start on 128-byte boundaries at i = 1 and the dense (ip,jp,kp)
+// rows on 16-byte ones, so every access is a 16-byte vector except the
+// fifth w(i+4,j,k-1).  Same per-element expressions.
+__global__ void k_ave_accum4(Geo g, Fields F, AveBuf A, int first) {
+    const int ip = g.im, jp = g.jm;
+    const int i = 4 * (blockIdx.x * blockDim.x + threadIdx.x) + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    if (i > ip) return;
+    const long long t = (long long)(i - 1) + (long long)ip * ((j - 1) + (long long)jp * (k - 1));
+    if (first && j == 1) {
+        const long long tc = (long long)(i - 1) + (long long)ip * (k - 1);
+        for (int a = AV_SU; a <= AV_SWW; ++a)
+            *reinterpret_cast<float4 *>(A.col(a) + tc) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    const int c = IX(g, i, j, k), cm = IX(g, i, j, k - 1);
+    auto ld = [](const float *p) { return *reinterpret_cast<const float4 *>(p); };
+    const float4 u4 = ld(F.u + c), v4 = ld(F.v + c), w4 = ld(F.w + c), p4 = ld(F.p + c), s4 = ld(F.sm + c);
+    const float4 um4 = ld(F.u + cm), wm4 = ld(F.w + cm);
+    const float wm5 = F.w[cm + 4];
+    const float u[4] = {u4.x, u4.y, u4.z, u4.w}, v[4] = {v4.x, v4.y, v4.z, v4.w};
+    const float w[4] = {w4.x, w4.y, w4.z, w4.w}, p[4] = {p4.x, p4.y, p4.z, p4.w};
+    const float sm[4] = {s4.x, s4.y, s4.z, s4.w}, um[4] = {um4.x, um4.y, um4.z, um4.w};
+    const float wm[5] = {wm4.x, wm4.y, wm4.z, wm4.w, wm5};
+    auto add = [&](int a, const float *x) {
+        float4 *q = reinterpret_cast<float4 *>(A.cell(a) + t);
+        const float4 o = first ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : *q;
+        *q = make_float4(o.x + x[0], o.y + x[1], o.z + x[2], o.w + x[3]);
+    };
+    float x[4];
+    add(AV_U, u);
+    add(AV_V, v);
+    add(AV_W, w);
+    add(AV_P, p);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) x[e] = u[e] * u[e];
+    add(AV_UU, x);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) x[e] = v[e] * v[e];
+    add(AV_VV, x);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) x[e] = w[e] * w[e];
+    add(AV_WW, x);
+    add(AV_SM, sm);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) x[e] = sm[e] * sm[e];
+    add(AV_SMSM, x);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) x[e] = 0.5f * (um[e] + u[e]) * 0.5f * (wm[e] + wm[e + 1]);
+    add(AV_UWFX, x);
+    if (first) *reinterpret_cast<float4 *>(A.cell(AV_L) + t) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
 // aveflow.f95:92-108: the ten time means (avel included).
 __global__ void k_ave_divide(AveBuf A, float cnt) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
