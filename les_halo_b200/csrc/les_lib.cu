@@ -191,6 +191,8 @@ struct les_ctx {
     bool force_exact_sor = false;    // testing: always the per-colour path
     bool sor_fp32_test = true;       // LES_SOR_SUMS=exact clears it: every pass sums exactly
     float *d_ave = nullptr;          // aveflow statistics (les_stats.cuh), allocated on first use
+    TbKCoef kq{};                    // per-plane SOR coefficients (build_tables), a pass kernel's parameter
+    unsigned table_gen = 0;          // bumped whenever build_tables runs (captured graphs are dropped)
     // FP64-refined press (les_refine.cuh): corrections per step, inner sweeps, tolerance
     int ref_outer = 0, ref_inner = 0;
     double ref_tol = 0.0;
@@ -213,6 +215,25 @@ namespace {
 float *field_ptr(les_ctx *c, int f) { return c->d_fields + (size_t)f * c->box_elems; }
 les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, float pjuge, int itmax,
                          bool tuning = false, const SorBufs *bufs = nullptr);
+
+// The SOR of the next step runs one colour sweep at a time (press.f95's own
+// sequence with materialised ghosts) instead of the temporal-blocked passes:
+// on request, for odd jp (same-colour periodic partners), for a just-uploaded
+// p whose ghosts are not boundary-consistent, and for km >= kTbKMax.
+bool sor_per_colour(const les_ctx *c) {
+    return c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok || c->prm.kp >= kTbKMax;
+}
+
+void drop_step_graphs(les_ctx *c) {
+    for (int gi = 0; gi < 4; ++gi) {
+        if (c->graph[gi]) cudaGraphExecDestroy(c->graph[gi]);
+        if (c->graph_src[gi]) cudaGraphDestroy(c->graph_src[gi]);
+        c->graph[gi] = nullptr;
+        c->graph_src[gi] = nullptr;
+        c->tnode[gi].clear();
+        c->tnode_idx[gi].clear();
+    }
+}
 les_status enqueue_refine(les_ctx *c);
 bool tb_fast_ok(const les_ctx *c, const TbShape &sh);
 
@@ -287,6 +308,16 @@ les_status build_tables(les_ctx *c, const les_host_fields *hf, bool require_infl
         c->cn1_by_k = uni && hf->dxs && hf->dys && hf->dzs;
         for (int k = 1; k <= kp; ++k) h[t.cn1k + k] = 1.0f / (h[t.cnA] + h[t.cnB] + h[t.cnC + k - 1]);
     }
+    c->kq = TbKCoef{};
+    for (int k = 1; k <= kp && k < kTbKMax; ++k) {
+        c->kq.c4l[k] = h[t.cn4l + k - 1];
+        c->kq.c4s[k] = h[t.cn4s + k - 1];
+        c->kq.cnk[k] = c->cn1_by_k ? h[t.cn1k + k] : 0.0f;
+    }
+    // graphs captured before hold the old tables' kernel choices and
+    // parameters: capture again at the next step
+    drop_step_graphs(c);
+    ++c->table_gen;
     // exact reciprocals of power-of-two x/y divisors (0 otherwise)
     auto recip = [](float d) -> float {
         int e = 0;
@@ -552,7 +583,7 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
         a.sc = bufs->sc;
     }
     const Geo &g = c->geo;
-#define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a)
+#define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a, c->kq)
     switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
         case 2: TBL(1, false); break;
         case 3: TBL(1, true); break;
@@ -1009,7 +1040,7 @@ les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *nch) {
 
 float les_ctx_sor_iters_per_launch(les_ctx *c) {
     if (!c) return 0.0f;
-    const bool exact = c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok;
+    const bool exact = sor_per_colour(c);
     return exact ? 0.5f : (float)(c->tb.T ? c->tb.T : 2);
 }
 
@@ -1033,7 +1064,7 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
     if (nsteps < 0) return fail(LES_ERR_BAD_ARG, "nsteps < 0");
     for (int s = 0; s < nsteps; ++s) {
         const int n = n0 + s;
-        const bool exact = c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok;
+        const bool exact = sor_per_colour(c);
         const int gi = ((n == 1 && c->prm.ical == 0) ? 1 : 0) + (exact ? 2 : 0);
         if ((!exact || c->ref_outer > 0) && c->tb.T == 0) {  // the refined press uses the passes too
             les_status st = autotune_sor(c);

@@ -83,6 +83,16 @@ struct TbArgs {
     Scal *sc;
 };
 
+// Per-plane coefficients of the SOR update, passed by value as a
+// __grid_constant__ kernel parameter: a warp-uniform plane index reads them
+// from the constant bank without address arithmetic or a global load.
+// Index q = 1..km; grids with km >= kTbKMax use the per-colour sweeps.
+constexpr int kTbKMax = 1024;
+struct TbKCoef {
+    float c4l[kTbKMax], c4s[kTbKMax];  // cn4l(q), cn4s(q)
+    float cnk[kTbKMax];                // cn1 by plane when it depends on k only (CN1K)
+};
+
 // Exact Q63.64 term (les_fix.h) of a non-negative float below 2^62: the
 // integer part and the fraction scaled by 2^64, both exact in FP64.  A term
 // below 1 is the fraction alone, and x * 2^64 is then exact in FP32 (a
@@ -224,7 +234,7 @@ __device__ void tb_finish_fast(const FixPart *part, int nblocks, float pjuge, Sc
 // CN1K: cn1 depends on k only (uniform dx and dy), read from cn1k[k].
 // blockDim.x = 32 * tb_rh(T, ty): warp y owns region row y.
 template <int T, bool CN1K>
-__global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a) {
+__global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a, const __grid_constant__ TbKCoef kq) {
     extern __shared__ float4 smem4[];
     Scal *sc = a.sc;
     const bool redo = (a.mode == 1);
@@ -336,8 +346,8 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a)
                 const float4 nn = Pq[RW4], ss = Pq[-RW4], bb = Bs[sq * RA4 + d0];
                 const float pn4[kTbCW] = {nn.x, nn.y, nn.z, nn.w}, ps4[kTbCW] = {ss.x, ss.y, ss.z, ss.w};
                 const float b4[kTbCW] = {bb.x, bb.y, bb.z, bb.w};
-                const float c4l = g.cn4l[q], c4s = g.cn4s[q];
-                const float cnq = CN1K ? a.cn1k[q] : 0.0f;
+                const float c4l = kq.c4l[q], c4s = kq.c4s[q];
+                const float cnq = CN1K ? kq.cnk[q] : 0.0f;
                 const float cC = CN1K ? 0.0f : g.cnC[q];
                 const bool top = (q == km), bottom = (q == 1);
                 const bool acc = acc_cells && q >= k0 && q <= k1;

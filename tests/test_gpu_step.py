@@ -275,3 +275,28 @@ def _sor_shape(gpu):
     v = [C.c_int() for _ in range(4)]
     abi.check(abi.lib().les_ctx_sor_shape(gpu.ctx, *[C.byref(x) for x in v]))
     return tuple(x.value for x in v)
+
+
+def test_reupload_with_other_spacings_recaptures_the_step(require_gpu):
+    # the step graph bakes in kernel choices and parameters taken from the
+    # grid tables (power-of-two x/y spacing, per-plane SOR coefficients): an
+    # upload of other tables must make the next step capture again
+    import ctypes as C
+    from les_halo_b200 import abi
+    ip, jp, kp = 40, 24, 14
+    a = synthetic_case(ip, jp, kp, seed=5, dx=4.0, dy=4.0, masks_and_poisson=oracle.masks_and_poisson)
+    b = synthetic_case(ip, jp, kp, seed=6, dx=3.0, dy=5.0, dz0=1.5, masks_and_poisson=oracle.masks_and_poisson)
+    g = GpuLes(a.copy())
+    g.warmup(1)
+    g.step(1, 2)
+    hb = b.host_fields()
+    abi.check(abi.lib().les_ctx_upload(g.ctx, C.byref(hb)))
+    g.warmup(1)
+    g.step(1, 2)
+    fresh = GpuLes(b.copy())
+    fresh.warmup(1)
+    fresh.step(1, 2)
+    assert_bitexact(g.download(ALL), fresh.download(ALL), ip, jp, kp, ALL)
+    assert g.metrics()["sor_iters"] == fresh.metrics()["sor_iters"]
+    g.close()
+    fresh.close()
