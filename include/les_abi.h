@@ -423,13 +423,20 @@ les_status les_read_restart(les_ctx *ctx, const char *data30, const char *data31
 
 /* ---- FP64-refined pressure solve (no counterpart in the reference) -------
  * outer > 0 turns it on for the following steps: after the plain FP32 SOR
- * of press.f95:87-115, `outer` FP64 defect corrections follow, each
- * r = b - A p64 in FP64 (b = rhs - rhsav with rhsav in FP64; A the operator
- * the sweeps relax, cn1 included), A e = r by `inner` FP32 SOR iterations
- * from e = 0, p64 += e; a correction is skipped once ||r||2/||b||2 <= rel_tol.
- * pav (press.f95:123-133) is then formed in FP64 and p = (float)(p64 - pav)
- * with its boundp1/boundp2 copies.  outer = 0 restores the plain press.
- * Needs even jp (the inner sweeps are the temporal-blocked passes).
+ * of press.f95:87-115, up to `outer` FP64 defect corrections follow, each
+ * r = b - A p64 in FP64 and A e = r, p64 += e, until ||r||2/||b||2 <= rel_tol.
+ * A is the operator the sweeps relax with its diagonal the sum of its six
+ * coefficients (exactly singular, like the Neumann/periodic problem), and
+ * b = rhs minus the mean of rhs weighted by A's left null vector (so A e = b
+ * is solvable; on a stretched grid the reference's rhsav weights are not that
+ * vector).  inner > 0: A e = r by `inner` FP32 SOR iterations from e = 0
+ * (needs even jp); inner = 0: an FP64 spectral solve (DCT-II in i, DFT in j,
+ * tridiagonal in k; needs even ip and jp and uniform x and y spacing), which
+ * solves A e = r to FP64 rounding, issued after the captured step graph with
+ * one host synchronisation per correction (such contexts cannot join an
+ * ensemble).  pav (press.f95:123-133) is then formed in FP64 and
+ * p = (float)(p64 - pav) with its boundp1/boundp2 copies.  outer = 0
+ * restores the plain press.
  * les_last_refine_metrics reports the last step's FP64 rhsav and pav, the
  * relative residual before the first and after the last correction, and
  * the corrections applied. */

@@ -25,6 +25,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
     "-Xptxas", "-v",
     "-shared",
+    "-lcufft",
 ]
 
 
@@ -37,6 +38,7 @@ def _stale(target: Path, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + \
+        list(CSRC.glob("*.inc")) + \
         list((ROOT / "include").glob("*.h")) + [Path(__file__)]
     if force or _stale(LIB, deps):
         cmd = [NVCC, *NVCC_FLAGS, "-I", str(ROOT / "include"), "-I", str(CSRC),

@@ -1,6 +1,7 @@
 // les_lib.cu -- host side of liblesb200.so: contexts, the host boundary,
 // the graph-captured time step and the setup routines (les_abi.h).
 #include <cuda_runtime.h>
+#include <cufft.h>
 
 #include <algorithm>
 #include <climits>
@@ -23,6 +24,7 @@
 #include "les_sor_tb.cuh"
 #include "les_stats.cuh"
 #include "les_refine.cuh"
+#include "les_spectral.cuh"
 #include "les_step.cuh"
 
 using namespace les;
@@ -148,6 +150,9 @@ struct TbShape {
     int T = 0, ty = 0, nch = 1;
 };
 
+struct SpecState;  // spectral solve of the refined press (les_refine.inc)
+void spec_release(SpecState *s);
+
 struct les_ctx {
     les_params prm{};
     Geo geo{};
@@ -201,6 +206,8 @@ struct les_ctx {
     Scal *d_scal2 = nullptr;              // scalars of the inner sweeps
     Ref64 *d_ref = nullptr;
     double2 *d_dpart = nullptr;           // FP64 per-block partial sums
+    double *d_refw = nullptr;             // left null vector weights wx, wy, wz
+    SpecState *spec = nullptr;            // spectral inner solve (inner = 0)
 };
 
 // Buffers of an SOR pass other than the context's p / second p / rhs / scalars.
@@ -220,6 +227,12 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
 // sequence with materialised ghosts) instead of the temporal-blocked passes:
 // on request, for odd jp (same-colour periodic partners), for a just-uploaded
 // p whose ghosts are not boundary-consistent, and for km >= kTbKMax.
+// The refined press with the spectral inner solve (inner = 0) runs after
+// the captured step graph, issued directly on the stream: its cuFFT
+// executions captured into the step graph faulted (misaligned address) on a
+// B200 where the same sequence issued directly ran correctly.
+bool spec_eager(const les_ctx *c) { return c->ref_outer > 0 && c->ref_inner == 0; }
+
 bool sor_per_colour(const les_ctx *c) {
     return c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok || c->prm.kp >= kTbKMax;
 }
@@ -497,6 +510,7 @@ les_status enqueue_press(les_ctx *c, bool exact) {
         }
     }
     MARK(c, EV_SOR_END);
+    if (c->ref_outer > 0 && spec_eager(c)) return LES_OK;  // the tail runs after the graph (les_step)
     if (c->ref_outer > 0) {
         les_status st = enqueue_refine(c);
         MARK(c, EV_PAV);
@@ -518,6 +532,7 @@ les_status enqueue_step(les_ctx *c, int n, bool exact_sor) {
     MARK(c, EV_BONDV1);
     if ((s = enqueue_velfg_les(c, true)) != LES_OK) return s;
     if ((s = enqueue_press(c, exact_sor)) != LES_OK) return s;
+    if (c->ref_outer > 0 && spec_eager(c)) return LES_OK;  // probe after the eager tail
     LAUNCH(c, k_probe, dim3(1), dim3(1), c->geo, c->F, c->d_scal);
     return LES_OK;
 }
@@ -907,6 +922,8 @@ les_status les_ctx_destroy(les_ctx *c) {
     cudaFree(c->d_scal2);
     cudaFree(c->d_ref);
     cudaFree(c->d_dpart);
+    cudaFree(c->d_refw);
+    spec_release(c->spec);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return ok();
@@ -1124,6 +1141,11 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
         LAUNCH(c, k_step_begin, dim3(1), dim3(1), c->d_scal, n);
         CK(cudaGraphLaunch(c->graph[gi], c->stream));
         c->launches += c->graph_kernels[gi];
+        if (c->ref_outer > 0 && spec_eager(c)) {  // the refined press's tail, issued directly
+            les_status st = enqueue_refine(c);
+            if (st != LES_OK) return st;
+            LAUNCH(c, k_probe, dim3(1), dim3(1), c->geo, c->F, c->d_scal);
+        }
         c->last_n = n;
         c->rhs_raw = true;
         c->p_ghosts_ok = true;  // press ends with boundp1/boundp2

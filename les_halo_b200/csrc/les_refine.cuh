@@ -1,14 +1,23 @@
 // les_refine.cuh -- FP64 defect correction of the pressure solve.
 //
-// The plain press (press.f95:49-146) solves, by FP32 red-black SOR,
-//     A p = b,   (A p)(c) = cn2l p_e + cn2s p_w + cn3l p_n + cn3s p_s + cn4l p_u + cn4s p_d - p / cn1,
-// with b = rhs - rhsav and the neighbours of the boundary cells given by
-// boundp1/boundp2 (i and k Neumann: the cell itself; j periodic).  The
-// refined press keeps those FP32 sweeps and wraps them in an FP64 outer
-// loop: p64 = p; then repeatedly r = b - A p64 in FP64, A e = r by the same
-// FP32 sweeps from e = 0, p64 += e.  rhsav, the residual norms and pav are
-// FP64.  Every pointwise expression below has a fixed operand order, the
-// same in the oracle's restatement (oracle_press_refine).
+// The plain press (press.f95:49-146) relaxes, by FP32 red-black SOR,
+//     cn2l p_e + cn2s p_w + cn3l p_n + cn3s p_s + cn4l p_u + cn4s p_d - p / cn1 = rhs - rhsav,
+// with the neighbours of the boundary cells given by boundp1/boundp2 (i and
+// k Neumann: the cell itself; j periodic).  The refined press solves the
+// same operator in FP64 with its diagonal the sum of the six coefficients,
+//     (A p)(c) = cn2l p_e + cn2s p_w + cn3l p_n + cn3s p_s + cn4l p_u + cn4s p_d - (cn2l+cn2s+cn3l+cn3s+cn4l+cn4s) p,
+// which makes A exactly singular with the constants as its null space, as
+// the continuous Neumann/periodic problem is.  A e = b then has a solution
+// only if b is orthogonal to A's left null vector w = wx(i) wy(j) wz(k)
+// (wz(k+1) cn4s(k+1) = wz(k) cn4l(k), likewise in x and y); on a stretched
+// grid the reference's rhsav weights (dx1 dy1 dzn) are not w, so b = rhs - mu
+// with mu the w-weighted mean of rhs (the reference's rhsav cancels).  The
+// FP32 sweeps are kept, then an FP64 outer loop: p64 = p; repeatedly
+// r = b - A p64 in FP64, A e = r by the inner solve from e = 0, p64 += e.
+// The inner solve is either `inner` FP32 SOR iterations (the same passes) or,
+// for uniform x and y spacing, the FP64 spectral solve of les_spectral.cuh.
+// Every pointwise expression below has a fixed operand order, the same in
+// the oracle's restatement (oracle_refine_tail).
 #pragma once
 
 #include "les_press.cuh"
@@ -17,7 +26,8 @@ namespace les {
 
 // FP64 scalars of the refined press.
 struct Ref64 {
-    double rhsav;        // FP64 mean of rhs
+    double rhsav;        // FP64 mean of rhs (press.f95:138, dx1 dy1 dzn weights)
+    double bshift;       // mean of rhs with the weights of A's left null vector
     double pav;          // FP64 mean of the refined p
     double bnorm2;       // sum of b^2
     double rel_initial;  // ||b - A p||2 / ||b||2 after the FP32 sweeps
@@ -58,13 +68,50 @@ __global__ void __launch_bounds__(1024) k_ref_rhsav(const FixPart *part, int n, 
     }
 }
 
-// r = b - A p64 on the interior (FP64), r32 = (float) r for the inner
-// sweeps, and per-block sums of r^2 and b^2.  FIRST: p64 is the FP32 SOR
-// result (read from the buffer Scal::pbuf names) and is stored.
-template <bool FIRST>
+// Sums of w*rhs and w over the interior (w = wx wy wz, FP64).
+__global__ void __launch_bounds__(kRedNT) k_ref_wmean(Geo g, const float *rhs, const double *wx, const double *wy,
+                                                       const double *wz, int kchunk, double2 *part) {
+    const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
+    const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
+    const int k0 = 1 + blockIdx.z * kchunk;
+    const int k1 = min(g.km, k0 + kchunk - 1);
+    double2 acc = make_double2(0.0, 0.0);
+    if (i <= g.im && j <= g.jm) {
+        const double wxy = wx[i - 1] * wy[j - 1];
+        for (int k = k0; k <= k1; ++k) {
+            const double w = wxy * wz[k - 1];
+            acc.x += w * (double)rhs[IX(g, i, j, k)];
+            acc.y += w;
+        }
+    }
+    const double2 v = block_sum_d2(acc);
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = v;
+}
+
+__global__ void __launch_bounds__(1024) k_ref_wmean_final(const double2 *part, int n, Ref64 *R) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) acc.x += part[t].x, acc.y += part[t].y;
+    const double2 v = block_sum_d2(acc);
+    if (threadIdx.x == 0) R->bshift = v.x / v.y;
+}
+
+// Position of i (1-based) in the even-then-reversed-odd order of a line of
+// n (even) values that turns a DCT-II into one real FFT (Makhoul 1980).
+__host__ __device__ __forceinline__ int makhoul_pos(int i, int n) {
+    const int i0 = i - 1;
+    return (i0 & 1) ? n - 1 - (i0 >> 1) : (i0 >> 1);
+}
+
+// r = b - A p64 on the interior (FP64) and per-block sums of r^2 and b^2.
+// SPEC: r goes to the dense FP64 lines (k, j) of the spectral solve, in
+// makhoul_pos order; else r32 = (float) r in the box for the inner sweeps.
+// FIRST: p64 is the FP32 SOR result (read from the buffer Scal::pbuf
+// names) and is stored.
+template <bool FIRST, bool SPEC>
 __global__ void __launch_bounds__(kRedNT) k_ref_defect(Geo g, const float *rhs, const float *p0, const float *p1,
-                                                        const Scal *sc, double *p64, float *r32, int kchunk,
-                                                        const Ref64 *R, double2 *part) {
+                                                        const Scal *sc, double *p64, float *r32, double *rline,
+                                                        int kchunk, const Ref64 *R, double2 *part) {
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
     const int k0 = 1 + blockIdx.z * kchunk;
@@ -74,7 +121,7 @@ __global__ void __launch_bounds__(kRedNT) k_ref_defect(Geo g, const float *rhs, 
         const float *p32 = sc->pbuf ? p1 : p0;
         const int jn = (j == g.jm) ? 1 : j + 1, js = (j == 1) ? g.jm : j - 1;
         const double c2l = g.cn2l[i], c2s = g.cn2s[i], c3l = g.cn3l[j], c3s = g.cn3s[j];
-        const double rav = R->rhsav;
+        const double bsh = R->bshift;
         for (int k = k0; k <= k1; ++k) {
             auto P = [&](int ii, int jj, int kk) -> double {
                 const int c = IX(g, ii, jj, kk);
@@ -87,18 +134,21 @@ __global__ void __launch_bounds__(kRedNT) k_ref_defect(Geo g, const float *rhs, 
             const double pn = P(i, jn, k), ps = P(i, js, k);
             const double pu = (k == g.km) ? pc : P(i, j, k + 1);
             const double pd = (k == 1) ? pc : P(i, j, k - 1);
-            const float cn1 = 1.0f / (g.cnA[i] + g.cnB[j] + g.cnC[k]);
-            const double diag = 1.0 / (double)cn1;
+            const double c4l = g.cn4l[k], c4s = g.cn4s[k];
+            const double diag = ((((c2l + c2s) + c3l) + c3s) + c4l) + c4s;
             double s = c2l * pe;
             s = s + c2s * pw;
             s = s + c3l * pn;
             s = s + c3s * ps;
-            s = s + (double)g.cn4l[k] * pu;
-            s = s + (double)g.cn4s[k] * pd;
+            s = s + c4l * pu;
+            s = s + c4s * pd;
             const double ap = s - pc * diag;
-            const double b = (double)rhs[c] - rav;
+            const double b = (double)rhs[c] - bsh;
             const double r = b - ap;
-            r32[c] = (float)r;
+            if (SPEC)
+                rline[((size_t)(k - 1) * g.jm + (j - 1)) * g.im + makhoul_pos(i, g.im)] = r;
+            else
+                r32[c] = (float)r;
             acc.x += r * r;
             if (FIRST) acc.y += b * b;
         }

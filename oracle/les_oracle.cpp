@@ -1061,12 +1061,102 @@ void oracle_boundp1(int km, int jm, float *p_, int im) {
 
 // press.f95:49-146
 // FP64-refined press after the FP32 SOR (the CUDA path's les_refine.cuh):
-// p64 = p; for m = 0..M: r = b - A p64 (FP64, b = rhs_raw - rhsav64, A the
-// operator the sweeps relax with the boundp1/boundp2 neighbours), the
+// p64 = p; for m = 0..M: r = b - A p64 in FP64, A the operator the sweeps
+// relax (boundp1/boundp2 neighbours) with its diagonal the sum of the six
+// coefficients, b = rhs_raw - mu with mu the mean of rhs weighted by A's
+// left null vector w = wx wy wz (w(q+1) cs(q+1) = w(q) cl(q) per axis); the
 // relative residual and the stop test; if m < M and not stopped: A e = r by
 // `inner` FP32 SOR iterations from e = 0 (press.f95:87-115 with rhs = (float)
 // r, no rhsav, no stop test), p64 += e.  Then pav in FP64 and
 // p = (float)(p64 - pav) with boundp1/boundp2.  Returns (float) pav.
+// The spectral inner solve (inner = 0) for uniform x and y spacing, by
+// direct sums: DCT-II along i, real DFT along j, one tridiagonal solve in k
+// per mode (the (0,0) mode drops its last equation, e(km) = 0), then the
+// inverse sums.  r and e are (im, jm, km) arrays, i fastest.
+static void oracle_spectral_solve(int im, int jm, int km, double c2, double c3, const std::vector<double> &zsub,
+                                  const std::vector<double> &zdiag, const std::vector<double> &zsup,
+                                  const std::vector<double> &r, std::vector<double> &e) {
+    const double pi = 3.14159265358979323846;
+    const int jh = jm / 2 + 1;
+    auto R = [&](int i, int j, int k) { return r[(size_t)i + (size_t)im * (j + (size_t)jm * k)]; };
+    std::vector<double> X((size_t)im * jm * km);  // [k][j][m]
+    for (int k = 0; k < km; ++k)
+        for (int j = 0; j < jm; ++j)
+            for (int m = 0; m < im; ++m) {
+                double s = 0.0;
+                for (int i = 0; i < im; ++i) s += R(i, j, k) * std::cos(pi * m * (2 * i + 1) / (2.0 * im));
+                X[(size_t)m + (size_t)im * (j + (size_t)jm * k)] = s;
+            }
+    std::vector<double> Yr((size_t)im * jh * km), Yi(Yr.size());  // [k][n][m]
+    for (int k = 0; k < km; ++k)
+        for (int n = 0; n < jh; ++n)
+            for (int m = 0; m < im; ++m) {
+                double sr = 0.0, si = 0.0;
+                for (int j = 0; j < jm; ++j) {
+                    const double x = X[(size_t)m + (size_t)im * (j + (size_t)jm * k)];
+                    sr += x * std::cos(2.0 * pi * n * j / jm);
+                    si -= x * std::sin(2.0 * pi * n * j / jm);
+                }
+                Yr[(size_t)m + (size_t)im * (n + (size_t)jh * k)] = sr;
+                Yi[(size_t)m + (size_t)im * (n + (size_t)jh * k)] = si;
+            }
+    for (int n = 0; n < jh; ++n)
+        for (int m = 0; m < im; ++m) {
+            const double lam = 2.0 * c2 * (std::cos(pi * m / im) - 1.0) + 2.0 * c3 * (std::cos(2.0 * pi * n / jm) - 1.0);
+            const int kn = (m == 0 && n == 0) ? km - 1 : km;
+            std::vector<double> cp(km), dr(km), di(km);
+            for (int k = 0; k < kn; ++k) {
+                const double a = k > 0 ? zsub[k] : 0.0, b = zdiag[k] + lam, c = (k < kn - 1) ? zsup[k] : 0.0;
+                const double den = b - a * (k > 0 ? cp[k - 1] : 0.0);
+                const size_t q = (size_t)m + (size_t)im * (n + (size_t)jh * k);
+                cp[k] = c / den;
+                dr[k] = (Yr[q] - a * (k > 0 ? dr[k - 1] : 0.0)) / den;
+                di[k] = (Yi[q] - a * (k > 0 ? di[k - 1] : 0.0)) / den;
+            }
+            double xr = 0.0, xi = 0.0;
+            for (int k = kn - 1; k >= 0; --k) {
+                if (k < kn - 1) {
+                    xr = dr[k] - cp[k] * xr;
+                    xi = di[k] - cp[k] * xi;
+                } else {
+                    xr = dr[k];
+                    xi = di[k];
+                }
+                const size_t q = (size_t)m + (size_t)im * (n + (size_t)jh * k);
+                Yr[q] = xr;
+                Yi[q] = xi;
+            }
+            if (kn < km) {
+                const size_t q = (size_t)m + (size_t)im * (n + (size_t)jh * (km - 1));
+                Yr[q] = 0.0;
+                Yi[q] = 0.0;
+            }
+        }
+    for (int k = 0; k < km; ++k)  // inverse real DFT along j (Hermitian extension)
+        for (int j = 0; j < jm; ++j)
+            for (int m = 0; m < im; ++m) {
+                double s = 0.0;
+                for (int n = 0; n < jh; ++n) {
+                    const size_t q = (size_t)m + (size_t)im * (n + (size_t)jh * k);
+                    const double w = (n == 0 || 2 * n == jm) ? 1.0 : 2.0;
+                    const double re = (n == 0 || 2 * n == jm) ? Yr[q] * std::cos(2.0 * pi * n * j / jm)
+                                                              : Yr[q] * std::cos(2.0 * pi * n * j / jm) -
+                                                                    Yi[q] * std::sin(2.0 * pi * n * j / jm);
+                    s += w * re;
+                }
+                X[(size_t)m + (size_t)im * (j + (size_t)jm * k)] = s / jm;
+            }
+    e.assign((size_t)im * jm * km, 0.0);
+    for (int k = 0; k < km; ++k)  // inverse DCT-II along i
+        for (int j = 0; j < jm; ++j)
+            for (int i = 0; i < im; ++i) {
+                double s = X[(size_t)im * (j + (size_t)jm * k)];
+                for (int m = 1; m < im; ++m)
+                    s += 2.0 * X[(size_t)m + (size_t)im * (j + (size_t)jm * k)] * std::cos(pi * m * (2 * i + 1) / (2.0 * im));
+                e[(size_t)i + (size_t)im * (j + (size_t)jm * k)] = s / im;
+            }
+}
+
 static float oracle_refine_tail(int km, int jm, int im, float *p_, const float *rraw, double rav,
                                 const float *dx1_, const float *dy1_, const float *dzn_, const float *cn1_,
                                 const float *cn2l_, const float *cn2s_, const float *cn3l_, const float *cn3s_,
@@ -1078,6 +1168,21 @@ static float oracle_refine_tail(int km, int jm, int im, float *p_, const float *
        cn4l = mk1(cn4l_, 1), cn4s = mk1(cn4s_, 1);
     const size_t n = (size_t)im * jm * km;
     auto at = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)); };
+    auto weights = [](const A1 &cl, const A1 &cs, int nq) {
+        std::vector<double> w(nq, 1.0);
+        for (int q = 1; q < nq; ++q) w[q] = w[q - 1] * (double)cl(q) / (double)cs(q + 1);
+        return w;
+    };
+    const std::vector<double> wx = weights(cn2l, cn2s, im), wy = weights(cn3l, cn3s, jm), wz = weights(cn4l, cn4s, km);
+    double sw = 0.0, swr = 0.0;
+    for (int k = 1; k <= km; ++k)
+        for (int j = 1; j <= jm; ++j)
+            for (int i = 1; i <= im; ++i) {
+                const double w = wx[i - 1] * wy[j - 1] * wz[k - 1];
+                swr += w * (double)rraw[at(i, j, k)];
+                sw += w;
+            }
+    const double mu = swr / sw;
     std::vector<double> p64(n);
     for (int k = 1; k <= km; ++k)
         for (int j = 1; j <= jm; ++j)
@@ -1099,15 +1204,17 @@ static float oracle_refine_tail(int km, int jm, int im, float *p_, const float *
                     const double pn = p64[at(i, jn, k)], ps = p64[at(i, js, k)];
                     const double pu = (k == km) ? pc : p64[at(i, j, k + 1)];
                     const double pd = (k == 1) ? pc : p64[at(i, j, k - 1)];
-                    const double diag = 1.0 / (double)cn1(i, j, k);
-                    double s = (double)cn2l(i) * pe;
-                    s = s + (double)cn2s(i) * pw;
-                    s = s + (double)cn3l(j) * pn;
-                    s = s + (double)cn3s(j) * ps;
-                    s = s + (double)cn4l(k) * pu;
-                    s = s + (double)cn4s(k) * pd;
+                    const double c2l = cn2l(i), c2s = cn2s(i), c3l = cn3l(j), c3s = cn3s(j), c4l = cn4l(k),
+                                 c4s = cn4s(k);
+                    const double diag = ((((c2l + c2s) + c3l) + c3s) + c4l) + c4s;
+                    double s = c2l * pe;
+                    s = s + c2s * pw;
+                    s = s + c3l * pn;
+                    s = s + c3s * ps;
+                    s = s + c4l * pu;
+                    s = s + c4s * pd;
                     const double ap = s - pc * diag;
-                    const double b = (double)rraw[at(i, j, k)] - rav;
+                    const double b = (double)rraw[at(i, j, k)] - mu;
                     const double r = b - ap;
                     er(i, j, k) = (float)r;
                     r2 += r * r;
@@ -1119,6 +1226,43 @@ static float oracle_refine_tail(int km, int jm, int im, float *p_, const float *
         g_ref_out[3] = rel;
         if (rel <= g_ref_tol) stop = true;
         if (stop || m == g_ref_outer) break;
+        if (g_ref_inner == 0) {  // spectral: r in FP64, then p64 += e
+            std::vector<double> rr(n), ee;
+            for (int k = 1; k <= km; ++k)
+                for (int j = 1; j <= jm; ++j)
+                    for (int i = 1; i <= im; ++i) {
+                        const int jn = (j == jm) ? 1 : j + 1, js = (j == 1) ? jm : j - 1;
+                        const double pc = p64[at(i, j, k)];
+                        const double pe = (i == im) ? pc : p64[at(i + 1, j, k)];
+                        const double pw = (i == 1) ? pc : p64[at(i - 1, j, k)];
+                        const double pn = p64[at(i, jn, k)], ps = p64[at(i, js, k)];
+                        const double pu = (k == km) ? pc : p64[at(i, j, k + 1)];
+                        const double pd = (k == 1) ? pc : p64[at(i, j, k - 1)];
+                        const double c2l = cn2l(i), c2s = cn2s(i), c3l = cn3l(j), c3s = cn3s(j), c4l = cn4l(k),
+                                     c4s = cn4s(k);
+                        const double diag = ((((c2l + c2s) + c3l) + c3s) + c4l) + c4s;
+                        double s = c2l * pe;
+                        s = s + c2s * pw;
+                        s = s + c3l * pn;
+                        s = s + c3s * ps;
+                        s = s + c4l * pu;
+                        s = s + c4s * pd;
+                        rr[at(i, j, k)] = ((double)rraw[at(i, j, k)] - mu) - (s - pc * diag);
+                    }
+            std::vector<double> zsub(km), zdiag(km), zsup(km);
+            for (int k = 1; k <= km; ++k) {
+                zsub[k - 1] = cn4s(k);
+                zsup[k - 1] = cn4l(k);
+                double d = -((double)cn4l(k) + (double)cn4s(k));
+                if (k == 1) d += cn4s(k);
+                if (k == km) d += cn4l(k);
+                zdiag[k - 1] = d;
+            }
+            oracle_spectral_solve(im, jm, km, cn2l(1), cn3l(1), zsub, zdiag, zsup, rr, ee);
+            for (size_t q = 0; q < n; ++q) p64[q] = p64[q] + ee[q];
+            ++g_ref_done;
+            continue;
+        }
         std::fill(e_.begin(), e_.end(), 0.0f);
         for (int l = 1; l <= g_ref_inner; ++l) {
             for (int nrd = 0; nrd <= 1; ++nrd) {

@@ -1,5 +1,6 @@
 """FP64-refined pressure solve (les_press_refine_fp64) against the oracle's
-restatement of the same algorithm.
+restatement of the same algorithm, with SOR inner sweeps and with the
+spectral inner solve.
 
 The plain FP32 sweeps and every pointwise FP64 expression are bit-identical
 on both sides; the FP64 sums (residual norms, pav) are reduced in different
@@ -78,4 +79,30 @@ def test_refine_rejects_odd_jp(require_gpu):
     g = GpuLes(case)
     st = abi.lib().les_press_refine_fp64(g.ctx, 2, 10, 0.0)
     assert st == abi.LES_ERR_DIMS
+    st = abi.lib().les_press_refine_fp64(g.ctx, 2, 0, 0.0)  # spectral: even ip and jp
+    assert st == abi.LES_ERR_DIMS
     g.close()
+
+
+@pytest.mark.parametrize("outer", [1, 2])
+def test_spectral_refined_press_matches_oracle(require_gpu, outer):
+    # inner = 0: the FP64 spectral solve (cuFFT on the GPU, direct sums in
+    # the oracle) solves the FP64 system in one correction; both agree to
+    # FP64 rounding, so p after its FP32 rounding differs by at most an ulp
+    ref, gpu, got, want_m, m = _run(outer, 0, 0.0)
+    ip, jp, kp = ref.ip, ref.jp, ref.kp
+    assert_bitexact(got, {k: ref.a(k) for k in NOT_P}, ip, jp, kp, NOT_P)
+    assert _ulps(got["p"], ref.a("p")) <= 1
+    assert m["outer"] == want_m["outer"] == outer
+    assert m["rel_final"] <= 1e-12 and want_m["rel_final"] <= 1e-12
+    assert abs(m["rel_initial"] - want_m["rel_initial"]) <= 1e-10 * want_m["rel_initial"]
+    assert abs(m["pav"] - want_m["pav"]) <= 1e-10 * abs(want_m["pav"])
+    gpu.close()
+
+
+def test_spectral_refine_stops_after_one_correction(require_gpu):
+    # with a 1e-9 tolerance the second correction is skipped
+    ref, gpu, got, want_m, m = _run(3, 0, 1e-9)
+    assert m["outer"] == want_m["outer"] == 1
+    assert m["rel_final"] <= 1e-9
+    gpu.close()
