@@ -1333,7 +1333,7 @@ int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const 
             }
     float rhsav;
     double rhsav64 = 0.0;
-    const bool refine = canon && g_ref_outer > 0;
+    const bool refine = g_ref_outer > 0;
     std::vector<float> rraw;  // rhs before the rhsav subtraction (refined press)
     if (refine) {
         rraw.resize((size_t)im * jm * km);
@@ -1357,6 +1357,7 @@ int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const 
                     area = area + dx1(i) * dy1(j) * dzn(k);
                 }
         rhsav = s / area;
+        rhsav64 = (double)rhsav;
     }
 #pragma omp parallel for schedule(static)
     for (int k = 1; k <= km; ++k)
