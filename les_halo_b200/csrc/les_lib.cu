@@ -518,8 +518,7 @@ les_status enqueue_press(les_ctx *c, bool exact) {
     }
     LAUNCH(c, k_pav_reduce, rg, rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, c->red_kchunk, c->d_part, c->d_scal);
     LAUNCH(c, k_final_pav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
-    LAUNCH(c, k_pav_adjust, dim3(c->red_gx, c->red_gy, g.km), rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p,
-           c->d_scal);
+    LAUNCH(c, k_pav_adjust, rg, rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, c->d_scal, c->red_kchunk);
     MARK(c, EV_PAV);
     return LES_OK;
 }

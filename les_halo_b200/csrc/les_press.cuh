@@ -12,6 +12,7 @@ namespace les {
 namespace {  // kernels get internal linkage: each .cu has its own copy
 
 constexpr int kRedBX = 32, kRedBY = 8, kRedNT = kRedBX * kRedBY;
+constexpr int kRedKMax = 8;  // planes per thread of the reduction grids (red_kchunk <= 8)
 
 // bondFG.f95:15-31 fused with the rhs of press.f95:114-125 and the partial
 // sums of press.f95:128-137.  rhs is stored before the rhsav subtraction
@@ -244,8 +245,13 @@ __global__ void __launch_bounds__(kRedNT) k_pav_reduce(Geo g, const float *p0, c
     i128 acc = 0;
     int bad = 0;
     if (i <= g.im && j <= g.jm) {
-        for (int k = k0; k <= k1; ++k)
-            acc += fix_term(p[IX(g, i, j, k)] * g.dx1[i] * g.dy1[j] * g.dzn[k], bad);
+        // the chunk's loads first (kchunk <= kRedKMax), then the sums
+        float pv[kRedKMax];
+#pragma unroll
+        for (int q = 0; q < kRedKMax; ++q) pv[q] = (k0 + q <= k1) ? p[IX(g, i, j, k0 + q)] : 0.0f;
+#pragma unroll
+        for (int q = 0; q < kRedKMax; ++q)
+            if (k0 + q <= k1) acc += fix_term(pv[q] * g.dx1[i] * g.dy1[j] * g.dzn[k0 + q], bad);
     }
     block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
 }
@@ -261,28 +267,32 @@ __global__ void __launch_bounds__(1024) k_final_pav(const FixPart *part, int n, 
 // The interior thread writes its new value and every ghost whose final
 // source it is: ghost (i,j,k) <- (clamp(i), periodic(j), clamp(k)).  The
 // SOR result may sit in the second buffer (s->pbuf); the state p is written.
-__global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *p, const float *p1, const Scal *s) {
+__global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *p, const float *p1, const Scal *s, int kchunk) {
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
-    const int k = 1 + blockIdx.z;
+    const int k0 = 1 + blockIdx.z * kchunk;
+    const int k1 = min(g.km, k0 + kchunk - 1);
     if (i > g.im || j > g.jm) return;
     const float *src = s->pbuf ? p1 : p;
-    const float val = src[IX(g, i, j, k)] - s->pav;
-    // the cell and its boundp1/boundp2 copies: at most one extra i, j and k
-    // (im, jm >= 2, km >= 3)
-    const int ie = (i == 1) ? 0 : (i == g.im ? g.im + 1 : -9);
-    const int je = (j == g.jm) ? 0 : (j == 1 ? g.jm + 1 : -9);
-    const int ke = (k == 1) ? 0 : (k == g.km ? g.km + 1 : -9);
-    auto put = [&](int kk) {
-        p[IX(g, i, j, kk)] = val;
-        if (ie != -9) p[IX(g, ie, j, kk)] = val;
-        if (je != -9) {
-            p[IX(g, i, je, kk)] = val;
-            if (ie != -9) p[IX(g, ie, je, kk)] = val;
-        }
-    };
-    put(k);
-    if (ke != -9) put(ke);
+    const float pav = s->pav;
+    for (int k = k0; k <= k1; ++k) {
+        const float val = src[IX(g, i, j, k)] - pav;
+        // the cell and its boundp1/boundp2 copies: at most one extra i, j and k
+        // (im, jm >= 2, km >= 3)
+        const int ie = (i == 1) ? 0 : (i == g.im ? g.im + 1 : -9);
+        const int je = (j == g.jm) ? 0 : (j == 1 ? g.jm + 1 : -9);
+        const int ke = (k == 1) ? 0 : (k == g.km ? g.km + 1 : -9);
+        auto put = [&](int kk) {
+            p[IX(g, i, j, kk)] = val;
+            if (ie != -9) p[IX(g, ie, j, kk)] = val;
+            if (je != -9) {
+                p[IX(g, i, je, kk)] = val;
+                if (ie != -9) p[IX(g, ie, je, kk)] = val;
+            }
+        };
+        put(k);
+        if (ke != -9) put(ke);
+    }
 }
 
 // Per-step scalars reset and the centre probe of press.f95:183-187.
