@@ -17,7 +17,9 @@ constexpr int kRedKMax = 8;  // planes per thread of the reduction grids (red_kc
 // bondFG.f95:15-31 fused with the rhs of press.f95:114-125 and the partial
 // sums of press.f95:128-137.  rhs is stored before the rhsav subtraction
 // (every reader subtracts the scalar itself).  Threads loop over a k chunk.
-__global__ void __launch_bounds__(kRedNT) k_rhs(Geo g, Fields F, int kchunk, FixPart *part) {
+// 6 CTAs per SM (at most 42 registers): the loads of more warps in flight hide
+// the memory latency that bounds this kernel
+__global__ void __launch_bounds__(kRedNT, 6) k_rhs(Geo g, Fields F, int kchunk, FixPart *part) {
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
     const int k0 = 1 + blockIdx.z * kchunk;
