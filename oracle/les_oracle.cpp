@@ -1078,28 +1078,40 @@ static void oracle_spectral_solve(int im, int jm, int km, double c2, double c3, 
                                   const std::vector<double> &r, std::vector<double> &e) {
     const double pi = 3.14159265358979323846;
     const int jh = jm / 2 + 1;
+    // cos(pi m (2i+1) / 2im), cos and sin(2 pi n j / jm)
+    std::vector<double> cx((size_t)im * im), cy((size_t)jh * jm), sy((size_t)jh * jm);
+    for (int m = 0; m < im; ++m)
+        for (int i = 0; i < im; ++i) cx[(size_t)m * im + i] = std::cos(pi * m * (2 * i + 1) / (2.0 * im));
+    for (int n = 0; n < jh; ++n)
+        for (int j = 0; j < jm; ++j) {
+            cy[(size_t)n * jm + j] = std::cos(2.0 * pi * n * j / jm);
+            sy[(size_t)n * jm + j] = std::sin(2.0 * pi * n * j / jm);
+        }
     auto R = [&](int i, int j, int k) { return r[(size_t)i + (size_t)im * (j + (size_t)jm * k)]; };
     std::vector<double> X((size_t)im * jm * km);  // [k][j][m]
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < km; ++k)
         for (int j = 0; j < jm; ++j)
             for (int m = 0; m < im; ++m) {
                 double s = 0.0;
-                for (int i = 0; i < im; ++i) s += R(i, j, k) * std::cos(pi * m * (2 * i + 1) / (2.0 * im));
+                for (int i = 0; i < im; ++i) s += R(i, j, k) * cx[(size_t)m * im + i];
                 X[(size_t)m + (size_t)im * (j + (size_t)jm * k)] = s;
             }
     std::vector<double> Yr((size_t)im * jh * km), Yi(Yr.size());  // [k][n][m]
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < km; ++k)
         for (int n = 0; n < jh; ++n)
             for (int m = 0; m < im; ++m) {
                 double sr = 0.0, si = 0.0;
                 for (int j = 0; j < jm; ++j) {
                     const double x = X[(size_t)m + (size_t)im * (j + (size_t)jm * k)];
-                    sr += x * std::cos(2.0 * pi * n * j / jm);
-                    si -= x * std::sin(2.0 * pi * n * j / jm);
+                    sr += x * cy[(size_t)n * jm + j];
+                    si -= x * sy[(size_t)n * jm + j];
                 }
                 Yr[(size_t)m + (size_t)im * (n + (size_t)jh * k)] = sr;
                 Yi[(size_t)m + (size_t)im * (n + (size_t)jh * k)] = si;
             }
+#pragma omp parallel for schedule(static)
     for (int n = 0; n < jh; ++n)
         for (int m = 0; m < im; ++m) {
             const double lam = 2.0 * c2 * (std::cos(pi * m / im) - 1.0) + 2.0 * c3 * (std::cos(2.0 * pi * n / jm) - 1.0);
@@ -1132,27 +1144,28 @@ static void oracle_spectral_solve(int im, int jm, int km, double c2, double c3, 
                 Yi[q] = 0.0;
             }
         }
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < km; ++k)  // inverse real DFT along j (Hermitian extension)
         for (int j = 0; j < jm; ++j)
             for (int m = 0; m < im; ++m) {
                 double s = 0.0;
                 for (int n = 0; n < jh; ++n) {
                     const size_t q = (size_t)m + (size_t)im * (n + (size_t)jh * k);
-                    const double w = (n == 0 || 2 * n == jm) ? 1.0 : 2.0;
-                    const double re = (n == 0 || 2 * n == jm) ? Yr[q] * std::cos(2.0 * pi * n * j / jm)
-                                                              : Yr[q] * std::cos(2.0 * pi * n * j / jm) -
-                                                                    Yi[q] * std::sin(2.0 * pi * n * j / jm);
-                    s += w * re;
+                    const bool edge = (n == 0 || 2 * n == jm);
+                    const double re = edge ? Yr[q] * cy[(size_t)n * jm + j]
+                                           : Yr[q] * cy[(size_t)n * jm + j] - Yi[q] * sy[(size_t)n * jm + j];
+                    s += (edge ? 1.0 : 2.0) * re;
                 }
                 X[(size_t)m + (size_t)im * (j + (size_t)jm * k)] = s / jm;
             }
     e.assign((size_t)im * jm * km, 0.0);
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < km; ++k)  // inverse DCT-II along i
         for (int j = 0; j < jm; ++j)
             for (int i = 0; i < im; ++i) {
                 double s = X[(size_t)im * (j + (size_t)jm * k)];
                 for (int m = 1; m < im; ++m)
-                    s += 2.0 * X[(size_t)m + (size_t)im * (j + (size_t)jm * k)] * std::cos(pi * m * (2 * i + 1) / (2.0 * im));
+                    s += 2.0 * X[(size_t)m + (size_t)im * (j + (size_t)jm * k)] * cx[(size_t)m * im + i];
                 e[(size_t)i + (size_t)im * (j + (size_t)jm * k)] = s / im;
             }
 }
