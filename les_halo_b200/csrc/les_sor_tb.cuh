@@ -280,16 +280,6 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a,
     // the tile's columns come in whole lanes (RX and TX are multiples of 4)
     const bool lane_tile = (fl[0] & 8) != 0;
     const bool acc_cells = !redo && ytile && lane_tile;  // this lane's updates enter the residual
-    // bit 4s+c: column c of this lane is updated by half-sweep s (inside the
-    // region shrunk by s+1 and inside 1..im)
-    unsigned vmask = 0u;
-#pragma unroll
-    for (int s = 0; s < 2 * T; ++s)
-#pragma unroll
-        for (int c = 0; c < kTbCW; ++c) {
-            const int x = kTbCW * lane + c;
-            if (x >= s + 1 && x < kTbRW - s - 1 && (fl[c] & 1)) vmask |= 1u << (kTbCW * s + c);
-        }
     // x parity of the colour updated at step tau: (pbase + tau) & 1 for every
     // half-sweep (q = tau - s and nrd = s & 1 move together)
     const int pbase = (jr0 + y + 1 - ir0) & 1;
@@ -317,98 +307,126 @@ __global__ void __launch_bounds__(T == 1 ? 1024 : 768) k_sor_tb(Geo g, TbArgs a,
 
 #pragma unroll
     for (int k = 0; k < D; ++k) request(kb + k, (kb + k) % NS);
-    int st1 = kb % NS;  // slot of plane tau+1
     const int tau_end = k1 + 2 * T - 1;  // plane k1 is stored at this step
-    for (int tau = kb - 1; tau <= tau_end; ++tau) {
-        request(tau + 1 + D, st1 + D >= NS ? st1 + D - NS : st1 + D);
-        tb_cp_wait<D>();  // plane tau+1 has landed (this thread's copies)
-        __syncthreads();  // ... and everyone's
+
+    // The plane loop, compiled for each stop test (FAST: the FP32 sum) and
+    // for blocks whose region reaches i = 1 or i = im (EDGE).  A half-sweep
+    // updates every column of its rows and planes, the ring columns
+    // included.  A ring column's update may read a value from outside the
+    // region (the lane shuffles wrap around); such values move inward by at
+    // most one column per half-sweep, 2T columns in all, and the x ring has
+    // RX >= 2T columns, so the tile is exact.  Columns outside 1..im are
+    // updated the same way and no cell inside reads them: the ghost
+    // neighbour of i = 1 and of i = im is the cell itself (boundp1,
+    // press.f95:87-115).  Only tile cells inside the grid enter the residual.
+    static_assert(tb_ringx(T) >= 2 * T && tb_ringx(T) % kTbCW == 0 && tb_tx(T) % kTbCW == 0,
+                  "the ring must hold 2T columns, and i = 1 must fall on column 0 of a lane");
+    const bool edge = ir0 <= 1 || ir0 + kTbRW - 1 >= im;
+    auto sweep = [&](auto FASTc, auto EDGEc) {
+        constexpr bool FAST = decltype(FASTc)::value, EDGE = decltype(EDGEc)::value;
+        int st1 = kb % NS;  // slot of plane tau+1
+        for (int tau = kb - 1; tau <= tau_end; ++tau) {
+            request(tau + 1 + D, st1 + D >= NS ? st1 + D - NS : st1 + D);
+            tb_cp_wait<D>();  // plane tau+1 has landed (this thread's copies)
+            __syncthreads();  // ... and everyone's
 #pragma unroll
-        for (int c = 0; c < kTbCW; ++c)
+            for (int c = 0; c < kTbCW; ++c)
 #pragma unroll
-            for (int m = W - 1; m > 0; --m) w[c][m] = w[c][m - 1];
-        if (tau + 1 <= ke) {
-            const float4 v = P[st1 * RA4 + d0];
-            w[0][0] = v.x;
-            w[1][0] = v.y;
-            w[2][0] = v.z;
-            w[3][0] = v.w;
-        }
+                for (int m = W - 1; m > 0; --m) w[c][m] = w[c][m - 1];
+            if (tau + 1 <= ke) {
+                const float4 v = P[st1 * RA4 + d0];
+                w[0][0] = v.x;
+                w[1][0] = v.y;
+                w[2][0] = v.z;
+                w[3][0] = v.w;
+            }
 #pragma unroll
-        for (int s = 0; s < 2 * T; ++s) {
-            const int q = tau - s;
-            const int qlo = (kb == 1) ? 1 : kb + s + 1, qhi = (ke == km) ? km : ke - s - 1;  // hoisted by the compiler
-            const int lo = s + 1;
-            if (s < nhs && q >= qlo && q <= qhi && y >= lo && y < RH - lo) {
-                int sq = st1 - 1 - s;
-                if (sq < 0) sq += NS;
-                float4 *Pq = P + sq * RA4 + d0;
-                const float4 nn = Pq[RW4], ss = Pq[-RW4], bb = Bs[sq * RA4 + d0];
-                const float pn4[kTbCW] = {nn.x, nn.y, nn.z, nn.w}, ps4[kTbCW] = {ss.x, ss.y, ss.z, ss.w};
-                const float b4[kTbCW] = {bb.x, bb.y, bb.z, bb.w};
-                const float c4l = kq.c4l[q], c4s = kq.c4s[q];
-                const float cnq = CN1K ? kq.cnk[q] : 0.0f;
-                const float cC = CN1K ? 0.0f : g.cnC[q];
-                const bool top = (q == km), bottom = (q == 1);
-                const bool acc = acc_cells && q >= k0 && q <= k1;
-                // update column C (of this half-sweep's colour) given its x neighbours
-                auto upd = [&](auto Cc, float west, float east) {
-                    constexpr int C = decltype(Cc)::value;
-                    // computed on every lane; kept where the cell is in the
-                    // half-sweep's region (no divergent branch)
-                    const bool ok = (vmask >> (kTbCW * s + C)) & 1u;
-                    const float pc = w[C][s + 1];
-                    const float pe = (fl[C] & 4) ? pc : east;
-                    const float pw = (fl[C] & 2) ? pc : west;
-                    const float pu = top ? pc : w[C][s];
-                    const float pd = bottom ? pc : w[C][s + 2];
-                    const float cn1 = CN1K ? cnq : 1.0f / (cA[C] + cB + cC);
-                    const float reltmp = omega * (cn1 * (c2l[C] * pe + c2s[C] * pw + c3l * pn4[C] + c3s * ps4[C] +
-                                                         c4l * pu + c4s * pd - (b4[C] - rhsav)) -
-                                                  pc);
-                    w[C][s + 1] = ok ? pc + reltmp : pc;
-                    if (acc && ok) {
-                        const float t2 = reltmp * reltmp;
-                        if (fast)
-                            fsum += t2;
-                        else if (s < 2)
-                            fix_add_nonneg(t2, h0, l0, bad);
-                        else if (s < 4)
-                            fix_add_nonneg(t2, h1, l1, bad);
-                        else
-                            fix_add_nonneg(t2, h2, l2, bad);
+            for (int s = 0; s < 2 * T; ++s) {
+                const int q = tau - s;
+                const int qlo = (kb == 1) ? 1 : kb + s + 1, qhi = (ke == km) ? km : ke - s - 1;  // hoisted by the compiler
+                const int lo = s + 1;
+                if (s < nhs && q >= qlo && q <= qhi && y >= lo && y < RH - lo) {
+                    int sq = st1 - 1 - s;
+                    if (sq < 0) sq += NS;
+                    float4 *Pq = P + sq * RA4 + d0;
+                    const float4 nn = Pq[RW4], ss = Pq[-RW4], bb = Bs[sq * RA4 + d0];
+                    const float pn4[kTbCW] = {nn.x, nn.y, nn.z, nn.w}, ps4[kTbCW] = {ss.x, ss.y, ss.z, ss.w};
+                    const float b4[kTbCW] = {bb.x, bb.y, bb.z, bb.w};
+                    const float c4l = kq.c4l[q], c4s = kq.c4s[q];
+                    const float cnq = CN1K ? kq.cnk[q] : 0.0f;
+                    const float cC = CN1K ? 0.0f : g.cnC[q];
+                    const bool top = (q == km), bottom = (q == 1);
+                    const bool acc = acc_cells && q >= k0 && q <= k1;
+                    // update column C (of this half-sweep's colour) given its x neighbours
+                    auto upd = [&](auto Cc, float west, float east) {
+                        constexpr int C = decltype(Cc)::value;
+                        const float pc = w[C][s + 1];
+                        const float pe = (EDGE && (fl[C] & 4)) ? pc : east;
+                        const float pw = (EDGE && C == 0 && (fl[0] & 2)) ? pc : west;
+                        const float pu = top ? pc : w[C][s];
+                        const float pd = bottom ? pc : w[C][s + 2];
+                        const float cn1 = CN1K ? cnq : 1.0f / (cA[C] + cB + cC);
+                        const float reltmp = omega * (cn1 * (c2l[C] * pe + c2s[C] * pw + c3l * pn4[C] + c3s * ps4[C] +
+                                                             c4l * pu + c4s * pd - (b4[C] - rhsav)) -
+                                                      pc);
+                        w[C][s + 1] = pc + reltmp;
+                        if (acc && (!EDGE || (fl[C] & 1))) {
+                            const float t2 = reltmp * reltmp;
+                            if constexpr (FAST)
+                                fsum += t2;
+                            else if (s < 2)
+                                fix_add_nonneg(t2, h0, l0, bad);
+                            else if (s < 4)
+                                fix_add_nonneg(t2, h1, l1, bad);
+                            else
+                                fix_add_nonneg(t2, h2, l2, bad);
+                        }
+                    };
+                    // x parity of this colour's cells on the row
+                    if (((pbase + tau) & 1) == 0) {
+                        // cells 4l, 4l+2; the west neighbour of 4l is column 3 of lane-1
+                        const float nb = __shfl_sync(0xffffffffu, w[3][s + 1], lane - 1);
+                        upd(std::integral_constant<int, 0>(), nb, w[1][s + 1]);
+                        upd(std::integral_constant<int, 2>(), w[1][s + 1], w[3][s + 1]);
+                    } else {
+                        // cells 4l+1, 4l+3; the east neighbour of 4l+3 is column 0 of lane+1
+                        const float nb = __shfl_sync(0xffffffffu, w[0][s + 1], lane + 1);
+                        upd(std::integral_constant<int, 1>(), w[0][s + 1], w[2][s + 1]);
+                        upd(std::integral_constant<int, 3>(), w[2][s + 1], nb);
                     }
-                };
-                // x parity of this colour's cells on the row
-                if (((pbase + tau) & 1) == 0) {
-                    // cells 4l, 4l+2; the west neighbour of 4l is column 3 of lane-1
-                    const float nb = __shfl_sync(0xffffffffu, w[3][s + 1], lane - 1);
-                    upd(std::integral_constant<int, 0>(), nb, w[1][s + 1]);
-                    upd(std::integral_constant<int, 2>(), w[1][s + 1], w[3][s + 1]);
-                } else {
-                    // cells 4l+1, 4l+3; the east neighbour of 4l+3 is column 0 of lane+1
-                    const float nb = __shfl_sync(0xffffffffu, w[0][s + 1], lane + 1);
-                    upd(std::integral_constant<int, 1>(), w[0][s + 1], w[2][s + 1]);
-                    upd(std::integral_constant<int, 3>(), w[2][s + 1], nb);
+                    // publish the row's four columns (the other colour's two are
+                    // unchanged, so concurrent readers of those see the same bits)
+                    *Pq = make_float4(w[0][s + 1], w[1][s + 1], w[2][s + 1], w[3][s + 1]);
                 }
-                // publish the row's four columns (the other colour's two are
-                // unchanged, so concurrent readers of those see the same bits)
-                *Pq = make_float4(w[0][s + 1], w[1][s + 1], w[2][s + 1], w[3][s + 1]);
             }
-        }
-        // plane tau+1-2T is final: store the tile part of the row
-        const int qs = tau + 1 - 2 * T;
-        if (ytile && lane_tile && qs >= k0 && qs <= k1) {
-            float *dst = pout + (coff + pstride * qs);
-            if ((fl[3] & 1))  // all four columns inside the grid: one 16-byte store
-                *reinterpret_cast<float4 *>(dst) = make_float4(w[0][2 * T], w[1][2 * T], w[2][2 * T], w[3][2 * T]);
-            else {
+            // plane tau+1-2T is final: store the tile part of the row
+            const int qs = tau + 1 - 2 * T;
+            if (ytile && lane_tile && qs >= k0 && qs <= k1) {
+                float *dst = pout + (coff + pstride * qs);
+                if (!EDGE || (fl[3] & 1))  // all four columns inside the grid: one 16-byte store
+                    *reinterpret_cast<float4 *>(dst) =
+                        make_float4(w[0][2 * T], w[1][2 * T], w[2][2 * T], w[3][2 * T]);
+                else {
 #pragma unroll
-                for (int c = 0; c < kTbCW; ++c)
-                    if (fl[c] & 1) dst[c] = w[c][2 * T];
+                    for (int c = 0; c < kTbCW; ++c)
+                        if (fl[c] & 1) dst[c] = w[c][2 * T];
+                }
             }
+            st1 = (st1 + 1 == NS) ? 0 : st1 + 1;
         }
-        st1 = (st1 + 1 == NS) ? 0 : st1 + 1;
+    };
+    using True = std::true_type;
+    using False = std::false_type;
+    if (T == 1 && fast) {
+        if (edge)
+            sweep(True(), True());
+        else
+            sweep(True(), False());
+    } else {
+        if (edge)
+            sweep(False(), True());
+        else
+            sweep(False(), False());
     }
     tb_cp_wait<0>();  // only empty groups can be left
 
