@@ -336,6 +336,36 @@ les_status les_press_residual_(const int *km, const int *jm, const int *im, cons
                                const float *cn4s, float *sor);
 les_status les_press_pav_adj_(const int *km, const int *jm, const int *im, float *p, const float *dx1,
                               const float *dy1, const float *dzn, float *pav);
+/* Adjoint (reverse mode) of press.f95:49-146 run with *niter SOR iterations
+ * and relaxation factor *omega (the count les_press_ reported; with it fixed
+ * press is linear in u, v, w, f, g, h and the initial p).  No counterpart in
+ * the reference.  On entry rhsb, pb, fb, gb, hb hold the adjoints of press's
+ * outputs rhs, p, f, g, h (same Fortran bounds as those arrays); on return
+ * pb, fb, gb, hb hold the adjoints of its inputs p, f, g, h, rhsb that of its
+ * input rhs (0 on the interior press overwrites), and the adjoints of u, v, w
+ * are ADDED to ub, vb, wb.  dx1, dy1, dzn, dt, cn1..cn4s as given to press. */
+les_status les_press_b_(const int *km, const int *jm, const int *im, float *rhsb, const float *dx1,
+                        const float *dy1, const float *dzn, float *fb, float *gb, float *hb,
+                        const float *dt, const float *cn1, const float *cn2l, float *pb,
+                        const float *cn2s, const float *cn3l, const float *cn3s, const float *cn4l,
+                        const float *cn4s, const int *niter, const float *omega, float *ub,
+                        float *vb, float *wb);
+/* Adjoints of velnw.f95:5, feedbf.f95:5 and adam.f95:5, same argument order
+ * as the forward entries with each state array replaced by its adjoint (no
+ * counterpart in the reference).  On entry an array holds the adjoint of the
+ * routine's output of that name; on return the adjoint of its input.
+ * Arrays that are inputs only (velnw: p, f, g, h; feedbf: u, v, w) have the
+ * adjoint ADDED.  fxb..fzb may be NULL (no seed). */
+les_status les_velnw_b_(const int *km, const int *jm, const int *im, float *pb, const float *ro,
+                        const float *dxs, float *ub, const float *dt, float *fb, const float *dys,
+                        float *vb, float *gb, const float *dzs, float *wb, float *hb);
+les_status les_feedbf_b_(const int *km, const int *jm, const int *im, float *usumb, float *ub,
+                         const float *bmask1, float *vsumb, float *vb, const float *cmask1,
+                         float *wsumb, float *wb, const float *dmask1, const float *alpha,
+                         const float *dt, const float *beta, float *fxb, float *fyb, float *fzb,
+                         float *fb, float *gb, float *hb);
+les_status les_adam_b_(const int *n, const int *nmax, float *foldb, const int *im, const int *jm,
+                       const int *km, float *goldb, float *holdb, float *fb, float *gb, float *hb);
 /* bondFG.f95:5 */
 les_status les_bondfg_(const int *km, const int *jm, float *f, const int *im, float *g, float *h);
 /* boundp.f95:36 */

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "les_abi.h"
+#include "les_adjoint.cuh"
 #include "les_halo.cuh"
 #include "les_mom.cuh"
 #include "les_press.cuh"
@@ -1294,3 +1295,4 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 #include "les_stats_io.inc"
 #include "les_ensemble.inc"
 #include "les_refine.inc"
+#include "les_adjoint.inc"
