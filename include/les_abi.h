@@ -366,6 +366,19 @@ les_status les_feedbf_b_(const int *km, const int *jm, const int *im, float *usu
                          float *fb, float *gb, float *hb);
 les_status les_adam_b_(const int *n, const int *nmax, float *foldb, const int *im, const int *jm,
                        const int *km, float *goldb, float *holdb, float *fb, float *gb, float *hb);
+/* Adjoint of les.f95:98 at the forward state given by diu1..9 (no counterpart
+ * in the reference): smb, fb, gb, hb hold the adjoints of les's outputs sm,
+ * f, g, h; on return smb holds that of its input sm (0 where les overwrites
+ * it), the adjoints of diu1..9 are ADDED to diu1b..diu9b, and those of f, g, h
+ * equal fb, gb, hb (unchanged).  Where a cell's strain invariant is 0 no
+ * derivative passes through its sqrt. */
+les_status les_les_b_(const int *km, const float *dx1, const float *dy1, const float *dzn,
+                      const int *jm, const int *im, const float *diu1, const float *diu2,
+                      const float *diu3, const float *diu4, const float *diu5, const float *diu6,
+                      const float *diu7, const float *diu8, const float *diu9, float *diu1b,
+                      float *diu2b, float *diu3b, float *diu4b, float *diu5b, float *diu6b,
+                      float *diu7b, float *diu8b, float *diu9b, float *smb, const float *fb,
+                      const float *gb, const float *hb);
 /* bondFG.f95:5 */
 les_status les_bondfg_(const int *km, const int *jm, float *f, const int *im, float *g, float *h);
 /* boundp.f95:36 */

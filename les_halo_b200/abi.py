@@ -145,7 +145,7 @@ ROUTINES = {
     "les_bondfg_": 6, "les_boundp1_": 4, "les_boundp2_": 4,
     "les_press_rhsav_": 15, "les_press_sor_sweep_": 14, "les_press_residual_": 13, "les_press_pav_adj_": 8,
     "les_aveflow_": 32, "les_press_b_": 24,
-    "les_velnw_b_": 15, "les_feedbf_b_": 21, "les_adam_b_": 11,
+    "les_velnw_b_": 15, "les_feedbf_b_": 21, "les_adam_b_": 11, "les_les_b_": 28,
 }
 
 

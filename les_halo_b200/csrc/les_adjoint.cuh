@@ -1,6 +1,7 @@
-// les_adjoint.cuh -- reverse-mode (adjoint) kernels of the routines whose
-// map is linear: press.f95:49-146 run with a fixed number of SOR iterations
-// (the count a forward call executed), velnw, feedbf (masks fixed), adam.
+// les_adjoint.cuh -- reverse-mode (adjoint) kernels: of the routines whose
+// map is linear, press.f95:49-146 run with a fixed number of SOR iterations
+// (the count a forward call executed), velnw, feedbf (masks fixed), adam;
+// and of les (at the forward state, below).
 //
 // With that count fixed the routine is a linear map of its inputs: bondfg
 // (bondFG.f95:15-31) copies and clears ghost faces of f, g, h; rhs is the
@@ -291,6 +292,190 @@ __global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_adam(Geo g, Fields F) {
         cur[a][c] = 1.5f * b + ob;
         old[a][c] = -0.5f * b;
     }
+}
+
+// ---- les.f95:31-182 (Smagorinsky sm, boundsm, viscous terms) ------------
+// Nonlinear: the adjoint is taken at the forward state (the caller's diu and
+// the sm they give).  Contributions are scattered with atomic adds, so the
+// adjoint's last bits depend on the order the adds land in.
+struct LesAdj {
+    Geo g;
+    const float *d[9];  // diu1..9 (forward values)
+    float *db[9];       // their adjoints (accumulated)
+    const float *sm;    // sm of the forward, boundsm included
+    float *smb;         // sm's adjoint
+};
+
+// The viscous terms transposed (les.f95:170-274): f, g, h gain
+// vf = sum sgn * evs * D / div per cell, evs a value of sm or a two-axis
+// weighted average of four, D = 2 diu or the sum of two diu values; each
+// term sends vb * D (vb = sgn * seed / div) to the sm points of evs, with
+// their weights, and vb * evs to the diu entries of D.
+__global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_les_visc(LesAdj a, const float *fb, const float *gb,
+                                                                 const float *hb) {
+    const int i = 1 + blockIdx.x * kAdjBX + threadIdx.x, j = 1 + blockIdx.y * kAdjBY + threadIdx.y;
+    const int k = 1 + blockIdx.z;
+    const Geo &g = a.g;
+    if (i > g.im || j > g.jm) return;
+    const int c = IX(g, i, j, k);
+    const float sf = fb[c], sg = gb[c], sh = hb[c];
+    auto X = [&](int q) { return g.dx1[q]; };
+    auto Y = [&](int q) { return g.dy1[q]; };
+    auto Z = [&](int q) { return g.dzn[q]; };
+    auto S = [&](int x, int y, int z) { return a.sm[IX(g, x, y, z)]; };
+    auto sadd = [&](int x, int y, int z, float v) { atomicAdd(&a.smb[IX(g, x, y, z)], v); };
+    auto dv = [&](int n, int x, int y, int z) { return a.d[n][IX(g, x, y, z)]; };
+    auto dadd = [&](int n, int x, int y, int z, float v) { atomicAdd(&a.db[n][IX(g, x, y, z)], v); };
+    // evs = sm(px,py,pz), D = 2 diu_n(qx,qy,qz)
+    auto pt = [&](float seed, float sgn, float div, int px, int py, int pz, int n, int qx, int qy, int qz) {
+        const float vb = sgn * seed / div;
+        sadd(px, py, pz, vb * (2.0f * dv(n, qx, qy, qz)));
+        dadd(n, qx, qy, qz, vb * S(px, py, pz) * 2.0f);
+    };
+    // evs = (A*((d(p+1) s(p,q0) + d(p) s(p+1,q0))/Sin) + B*(... at q0+1))/Sd,
+    // inner axis ax (0 x, 1 y) over p, p+1, outer axis bx (1 y, 2 z) over
+    // q0, q0+1; D = diu_n1(..) + diu_n2(..)
+    auto av = [&](float seed, float sgn, float div, int ax, int p, int bx, int q0, float A, float B, float Sd,
+                  int n1, int x1, int y1, int z1, int n2, int x2, int y2, int z2) {
+        const float dp = ax == 0 ? X(p) : Y(p), dp1 = ax == 0 ? X(p + 1) : Y(p + 1);
+        const float Sin = dp + dp1;
+        int px[4], py[4], pz[4];
+        float w[4], evs = 0.0f;
+#pragma unroll
+        for (int o = 0; o < 2; ++o)
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const int q = 2 * o + t;
+                px[q] = i;
+                py[q] = j;
+                pz[q] = k;
+                if (ax == 0) px[q] = p + t;
+                else py[q] = p + t;
+                if (bx == 1) py[q] = q0 + o;
+                else pz[q] = q0 + o;
+                w[q] = (o ? B : A) * (t ? dp : dp1) / Sin / Sd;
+                evs += w[q] * S(px[q], py[q], pz[q]);
+            }
+        const float D = dv(n1, x1, y1, z1) + dv(n2, x2, y2, z2);
+        const float vb = sgn * seed / div;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sadd(px[q], py[q], pz[q], vb * D * w[q]);
+        dadd(n1, x1, y1, z1, vb * evs);
+        dadd(n2, x2, y2, z2, vb * evs);
+    };
+    // f (les.f95:170-204)
+    pt(sf, 1.0f, X(i), i + 1, j, k, 0, i + 1, j, k);
+    pt(sf, -1.0f, X(i), i, j, k, 0, i, j, k);
+    av(sf, 1.0f, Y(j), 0, i, 1, j, Y(j + 1), Y(j), Y(j) + Y(j + 1), 1, i, j + 1, k, 3, i + 1, j, k);
+    av(sf, -1.0f, Y(j), 0, i, 1, j - 1, Y(j + 1), Y(j), Y(j) + Y(j + 1), 1, i, j, k, 3, i + 1, j - 1, k);
+    av(sf, 1.0f, Z(k), 0, i, 2, k, Z(k + 1), Z(k), Z(k) + Z(k + 1), 2, i, j, k + 1, 6, i + 1, j, k);
+    av(sf, -1.0f, Z(k), 0, i, 2, k - 1, Z(k), Z(k - 1), Z(k - 1) + Z(k), 2, i, j, k, 6, i + 1, j, k - 1);
+    // g (les.f95:205-239)
+    av(sg, 1.0f, X(i), 0, i, 1, j, Y(j + 1), Y(j), Y(j) + Y(j + 1), 1, i, j + 1, k, 3, i + 1, j, k);
+    av(sg, -1.0f, X(i), 0, i - 1, 1, j, Y(j + 1), Y(j), Y(j) + Y(j + 1), 1, i - 1, j + 1, k, 3, i, j, k);
+    pt(sg, 1.0f, Y(j), i, j + 1, k, 4, i, j + 1, k);
+    pt(sg, -1.0f, Y(j), i, j, k, 4, i, j, k);
+    av(sg, 1.0f, Z(k), 0, i, 2, k, Z(k + 1), Z(k), Z(k) + Z(k + 1), 5, i, j, k + 1, 7, i, j + 1, k);
+    av(sg, -1.0f, Z(k), 0, i, 2, k - 1, Z(k), Z(k - 1), Z(k - 1) + Z(k), 5, i, j, k, 7, i, j + 1, k - 1);
+    // h (les.f95:240-274)
+    av(sh, 1.0f, X(i), 0, i, 2, k, Z(k + 1), Z(k), Z(k) + Z(k + 1), 2, i, j, k + 1, 6, i + 1, j, k);
+    av(sh, -1.0f, X(i), 0, i - 1, 2, k, Z(k + 1), Z(k), Z(k) + Z(k + 1), 2, i - 1, j, k + 1, 6, i, j, k);
+    av(sh, 1.0f, Y(j), 1, j, 2, k, Z(k + 1), Z(k), Z(k) + Z(k + 1), 5, i, j, k + 1, 7, i, j + 1, k);
+    av(sh, -1.0f, Y(j), 1, j - 1, 2, k, Z(k + 1), Z(k), Z(k) + Z(k + 1), 5, i, j - 1, k + 1, 7, i, j, k);
+    pt(sh, 1.0f, Z(k), i, j, k + 1, 8, i, j, k + 1);
+    pt(sh, -1.0f, Z(k), i, j, k, 8, i, j, k);
+}
+
+// boundsm transposed (boundsm.f95:13-32), its three loops last first:
+// k ghosts sm(.,.,0) = -sm(.,.,1), sm(.,.,km+1) = sm(.,.,km) over
+// j = -1..jm+1, i = 0..im+1 (stage 3); j ghosts sm(.,jm+1,.) = sm(.,jm,.),
+// sm(.,0,.) = sm(.,1,.) over k = 0..km+1, i = 0..im+1 (stage 2); i ghosts
+// sm(0,.,.) = sm(1,.,.), sm(im+1,.,.) = sm(im,.,.) over k = 0..km+1,
+// j = -1..jm+1 (stage 1).
+__global__ void k_adj_boundsm(Geo g, float *smb, int stage) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int im = g.im, jm = g.jm, km = g.km;
+    auto at = [&](int x, int y, int z) -> float & { return smb[IX(g, x, y, z)]; };
+    if (stage == 3) {
+        const int ni = im + 2;
+        if (t >= ni * (jm + 3)) return;
+        const int i = t % ni, j = t / ni - 1;
+        at(i, j, km) += at(i, j, km + 1);
+        at(i, j, km + 1) = 0.0f;
+        at(i, j, 1) += -at(i, j, 0);
+        at(i, j, 0) = 0.0f;
+    } else if (stage == 2) {
+        const int ni = im + 2;
+        if (t >= ni * (km + 2)) return;
+        const int i = t % ni, k = t / ni;
+        at(i, 1, k) += at(i, 0, k);
+        at(i, 0, k) = 0.0f;
+        at(i, jm, k) += at(i, jm + 1, k);
+        at(i, jm + 1, k) = 0.0f;
+    } else {
+        const int nj = jm + 3;
+        if (t >= nj * (km + 2)) return;
+        const int j = t % nj - 1, k = t / nj;
+        at(im, j, k) += at(im + 1, j, k);
+        at(im + 1, j, k) = 0.0f;
+        at(1, j, k) += at(0, j, k);
+        at(0, j, k) = 0.0f;
+    }
+}
+
+// sm = smc(k) sqrt(Q) transposed (les.f95:132-152), Q = 2(d1^2 + d5^2 +
+// d9^2) + a^2 + b^2 + c^2 of the cell's averaged gradients; at Q = 0 (all
+// gradients zero, e.g. inside buildings) sqrt has no derivative and none is
+// propagated.  The forward overwrites sm here: its input adjoint is 0.
+__global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_les_sm(LesAdj a) {
+    const int i = 1 + blockIdx.x * kAdjBX + threadIdx.x, j = 1 + blockIdx.y * kAdjBY + threadIdx.y;
+    const int k = 1 + blockIdx.z;
+    const Geo &g = a.g;
+    if (i > g.im || j > g.jm) return;
+    auto dv = [&](int n, int x, int y, int z) { return a.d[n][IX(g, x, y, z)]; };
+    auto dadd = [&](int n, int x, int y, int z, float v) { atomicAdd(&a.db[n][IX(g, x, y, z)], v); };
+    float &sb = a.smb[IX(g, i, j, k)];
+    const float b0 = sb;
+    sb = 0.0f;
+    const float d1 = dv(0, i, j, k), d5 = dv(4, i, j, k), d9 = dv(8, i, j, k);
+    const float uy = (dv(1, i - 1, j, k) + dv(1, i - 1, j + 1, k) + dv(1, i, j, k) + dv(1, i, j + 1, k)) * 0.25f;
+    const float uz = (dv(2, i - 1, j, k) + dv(2, i - 1, j, k + 1) + dv(2, i, j, k) + dv(2, i, j, k + 1)) * 0.25f;
+    const float vx = (dv(3, i, j, k) + dv(3, i, j - 1, k) + dv(3, i + 1, j, k) + dv(3, i + 1, j - 1, k)) * 0.25f;
+    const float vz = (dv(5, i, j - 1, k) + dv(5, i, j - 1, k + 1) + dv(5, i, j, k) + dv(5, i, j, k + 1)) * 0.25f;
+    const float wx = (dv(6, i, j, k) + dv(6, i, j, k - 1) + dv(6, i + 1, j, k) + dv(6, i + 1, j, k - 1)) * 0.25f;
+    const float wy = (dv(7, i, j, k) + dv(7, i, j, k - 1) + dv(7, i, j + 1, k) + dv(7, i, j + 1, k - 1)) * 0.25f;
+    const float ab = uy + vx, bb = wy + vz, cb = uz + wx;
+    const float q = 2.0f * (d1 * d1 + d5 * d5 + d9 * d9) + ab * ab + bb * bb + cb * cb;
+    if (!(q > 0.0f)) return;
+    const float qb = b0 * g.smc[k] * 0.5f / sqrtf(q);
+    dadd(0, i, j, k, qb * 4.0f * d1);
+    dadd(4, i, j, k, qb * 4.0f * d5);
+    dadd(8, i, j, k, qb * 4.0f * d9);
+    const float a4 = 0.5f * ab * qb, b4 = 0.5f * bb * qb, c4 = 0.5f * cb * qb;  // 2 x * qb / 4
+    dadd(1, i - 1, j, k, a4);
+    dadd(1, i - 1, j + 1, k, a4);
+    dadd(1, i, j, k, a4);
+    dadd(1, i, j + 1, k, a4);
+    dadd(3, i, j, k, a4);
+    dadd(3, i, j - 1, k, a4);
+    dadd(3, i + 1, j, k, a4);
+    dadd(3, i + 1, j - 1, k, a4);
+    dadd(2, i - 1, j, k, c4);
+    dadd(2, i - 1, j, k + 1, c4);
+    dadd(2, i, j, k, c4);
+    dadd(2, i, j, k + 1, c4);
+    dadd(6, i, j, k, c4);
+    dadd(6, i, j, k - 1, c4);
+    dadd(6, i + 1, j, k, c4);
+    dadd(6, i + 1, j, k - 1, c4);
+    dadd(5, i, j - 1, k, b4);
+    dadd(5, i, j - 1, k + 1, b4);
+    dadd(5, i, j, k, b4);
+    dadd(5, i, j, k + 1, b4);
+    dadd(7, i, j, k, b4);
+    dadd(7, i, j, k - 1, b4);
+    dadd(7, i, j + 1, k, b4);
+    dadd(7, i, j + 1, k - 1, b4);
 }
 
 }  // namespace

@@ -194,3 +194,43 @@ def test_adam_adjoint_dot_products(require_gpu, case):
         P = lambda n: a[n].ctypes.data
         L.oracle_adam(3, 10, P("fold"), IP, JP, KP, P("gold"), P("hold"), P("f"), P("g"), P("h"))
         check_dot(a, y, x, b, ADAM, ADAM)
+
+
+DIU = [f"diu{n}" for n in range(1, 10)]
+LES_OUT = ["sm", "f", "g", "h"]
+
+
+def les64(case, x):
+    """The FP64 oracle's les on float64 copies; returns sm, f, g, h."""
+    L = fp64.lib()
+    i, p = C.c_int, C.c_void_p
+    L.oracle_les.argtypes = [i, p, p, p, p, i, i] + [p] * 13
+    a = {n: np.asfortranarray(np.asarray(x[n], dtype=np.float64)) for n in DIU + LES_OUT}
+    co = {n: f64(case.arrays[n]) for n in ("dx1", "dy1", "dzn")}
+    delx1 = np.zeros(KP)
+    L.oracle_les(KP, delx1.ctypes.data, co["dx1"].ctypes.data, co["dy1"].ctypes.data, co["dzn"].ctypes.data, JP,
+                 IP, *[a[n].ctypes.data for n in DIU + LES_OUT])
+    return {n: a[n] for n in LES_OUT}
+
+
+def test_les_adjoint_against_fp64_differences(require_gpu, case):
+    """les is nonlinear: <J d, y> by central differences of the FP64 oracle
+    (step 1e-5, error ~1e-10) against <d, J^T y> from les_les_b_ at the
+    same state; random diu keep every strain invariant positive."""
+    A = case.arrays
+    x0 = rand_fields(DIU + LES_OUT, 300)
+    y = rand_fields(LES_OUT, 301)
+    b = {n: FL.alloc(n, IP, JP, KP) for n in DIU}
+    b.update({n: y[n].copy(order="F") for n in LES_OUT})
+    Fp = FL.ptr
+    abi.check(abi.lib().les_les_b_(I(KP), Fp(A["dx1"]), Fp(A["dy1"]), Fp(A["dzn"]), I(JP), I(IP),
+                                   *[Fp(x0[n]) for n in DIU], *[Fp(b[n]) for n in DIU],
+                                   *[Fp(b[n]) for n in LES_OUT]))
+    h = 1e-5
+    for s in range(2):
+        d = rand_fields(DIU + LES_OUT, 310 + s)
+        xp = {n: x0[n].astype(np.float64) + h * d[n] for n in DIU + LES_OUT}
+        xm = {n: x0[n].astype(np.float64) - h * d[n] for n in DIU + LES_OUT}
+        fp, fm = les64(case, xp), les64(case, xm)
+        jd = {n: (fp[n] - fm[n]) / (2 * h) for n in LES_OUT}
+        check_dot(jd, y, d, b, LES_OUT, DIU + LES_OUT)
