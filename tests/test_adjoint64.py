@@ -1,0 +1,61 @@
+"""The FP64 reference adjoints of oracle/adjoint64.py against central
+differences of the FP64 oracle (no GPU).
+
+velfg (vel2.f95:48-188 + velFG.f95:56-105) is quadratic in (u, v, w): for
+random (u, v, w), directions d and output seeds y on f, g, h and diu1..9,
+<(F(x + h d) - F(x - h d)) / 2h, y> must equal <d, J^T y> from velfg_b to the
+differences' accuracy (exact for a quadratic map up to FP64 rounding)."""
+import ctypes as C
+
+import numpy as np
+
+import oracle
+from oracle import adjoint64, fp64
+from les_halo_b200 import fields as FL, synthetic_case
+
+IP, JP, KP = 12, 10, 7
+WORK = [f"{a}{n}" for n in range(1, 10) for a in ("nou", "diu", "cov")] + ["dfu1", "dfv1", "dfw1"]
+
+
+def rnd(name, seed):
+    a = FL.alloc(name, IP, JP, KP)
+    a[...] = np.random.default_rng(seed).standard_normal(a.shape)
+    return np.asfortranarray(a.astype(np.float64))
+
+
+def velfg64(case, u, v, w):
+    """FP64 oracle velfg from zeroed work arrays; returns f, g, h, diu1..9."""
+    L = fp64.lib()
+    i, d, p = C.c_int, C.c_double, C.c_void_p
+    L.oracle_velfg.argtypes = [i, i, i] + [p] * 10 + [d] + [p] * 30
+    a = {n: np.asfortranarray(np.zeros(FL.alloc(n, IP, JP, KP).shape)) for n in WORK + ["f", "g", "h"]}
+    a.update({"u": np.asfortranarray(u), "v": np.asfortranarray(v), "w": np.asfortranarray(w)})
+    co = {n: np.asfortranarray(case.arrays[n].astype(np.float64)) for n in ("dx1", "dy1", "dzn", "dzs")}
+    P = lambda n: (a[n] if n in a else co[n]).ctypes.data
+    order = ["dx1", "cov1", "cov2", "cov3", "dfu1", "diu1", "diu2", "dy1", "diu3", "dzn"]
+    order2 = ["f", "cov4", "cov5", "cov6", "dfv1", "diu4", "diu5", "diu6", "g", "cov7", "cov8", "cov9", "dfw1",
+              "diu7", "diu8", "diu9", "dzs", "h", "nou1", "u", "nou5", "v", "nou9", "w", "nou2", "nou3", "nou4",
+              "nou6", "nou7", "nou8"]
+    L.oracle_velfg(KP, JP, IP, *[P(n) for n in order], float(np.float32(case.params.vn)), *[P(n) for n in order2])
+    return a
+
+
+def test_velfg_reference_adjoint_against_fp64_differences():
+    case = synthetic_case(IP, JP, KP, seed=3, masks_and_poisson=oracle.masks_and_poisson)
+    x = {n: rnd(n, s) for s, n in enumerate(("u", "v", "w"))}
+    outs = ["f", "g", "h"] + [f"diu{n}" for n in range(1, 10)]
+    y = {n: rnd(n, 20 + s) for s, n in enumerate(outs)}
+    metrics = {n: case.arrays[n].astype(np.float64) for n in ("dx1", "dy1", "dzn", "dzs")}
+    (ub, vb, wb), _ = adjoint64.velfg_b(IP, JP, KP, metrics, float(np.float32(case.params.vn)), x["u"], x["v"],
+                                        x["w"], y["f"], y["g"], y["h"], {n: y[f"diu{n}"] for n in range(1, 10)})
+    adj = {"u": ub, "v": vb, "w": wb}
+    h = 1e-4
+    for s in range(2):
+        d = {n: rnd(n, 40 + 3 * s + t) for t, n in enumerate(("u", "v", "w"))}
+        fp = velfg64(case, *[x[n] + h * d[n] for n in ("u", "v", "w")])
+        fm = velfg64(case, *[x[n] - h * d[n] for n in ("u", "v", "w")])
+        lhs = sum(float(np.sum((fp[n] - fm[n]) / (2 * h) * y[n])) for n in outs)
+        terms = [d[n] * adj[n] for n in ("u", "v", "w")]
+        rhs = sum(float(t.sum()) for t in terms)
+        scale = sum(float(np.abs(t).sum()) for t in terms)
+        assert abs(lhs - rhs) <= 1e-9 * scale, (s, lhs, rhs, scale)
