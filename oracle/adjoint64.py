@@ -6,6 +6,9 @@ that the CUDA adjoint entries are checked against, itself checked against
 central differences of the FP64 oracle (oracle/fp64.py) in
 tests/test_adjoint64.py.
 
+bondv1_ext_b: bondv1_ext_wind_profile.f95:27-127 (inflow from the external
+profile, n == 1 broadcast, outflow with uout, periodic, top and ground).
+
 velfg_b: vel2.f95:48-188 + velFG.f95:56-105, the face quantities of (u, v,
 w) and the advection/diffusion terms f, g, h.  The map is quadratic (cov =
 nou * diu); its adjoint is taken at the given (u, v, w).  Outputs whose
@@ -222,3 +225,82 @@ def velfg_b(ip, jp, kp, metrics, vn, u, v, w, fb, gb, hb, diub):
     wb[I, sh(J, -1), K1] -= 2.0 * b / sy
     wb[I, J, K1] += 2.0 * b / sy
     return (ub.arr, vb.arr, wb.arr), {n: db[n].arr for n in range(1, 10)}
+
+
+def bondv1_ext_b(ip, jp, kp, dxs, dt, n, wp, u, v, w, ub, vb, wb):
+    """Adjoint of bondv1_ext_wind_profile.f95:27-127 at the state (u, v, w)
+    and wind profile wp(j, k) it is called with.  ub, vb, wb: adjoints of its
+    outputs u, v, w.
+    Returns (ub, vb, wb, wpb): the adjoints of its inputs u, v, w and of the
+    wind profile wp(j, k).  Piecewise linear: uout = (max(0, u(im,.,.)) +
+    min(0, u(im,.,.)))/2 passes its derivative to the first maximal (and
+    minimal) element in the reference's loop order (k outer, j inner), as
+    amax1/amin1 pick it; a tie or a zero extreme has no derivative there."""
+    im, jm, km = ip, jp, kp
+    U, V, W = (FA(nm, ip, jp, kp, np.asarray(a, dtype=np.float64).copy()) for nm, a in (("u", u), ("v", v), ("w", w)))
+    Ub, Vb, Wb = (FA(nm, ip, jp, kp, np.asarray(a, dtype=np.float64).copy()) for nm, a in (("u", ub), ("v", vb), ("w", wb)))
+    J, K = (1, jm), (1, km)
+    ds = float(np.asarray(dxs, dtype=np.float64)[im])  # dxs(0:ip)
+    # forward up to the tail: inflow (bondv1_ext_wind_profile.f95:27-34) is
+    # overwritten data; the n == 1 broadcast (bondv1.f95:47-59) copies i = 1
+    U[(0, 1), J, K] = np.asarray(wp, dtype=np.float64)[np.newaxis, :, :]
+    V[(0, 1), J, K] = 0.0
+    W[(0, 1), J, K] = 0.0
+    if n == 1:
+        for A in (U, V, W):
+            A[(2, im), J, K] = A[1, J, K][np.newaxis, :, :]
+    # primal values the tail reads (before its updates)
+    u_im = U[im, J, K].copy()
+    du = U[im, J, K] - U[im - 1, J, K]
+    dvv = V[im + 1, J, K] - V[im, J, K]
+    dww = W[im + 1, J, K] - W[im, J, K]
+    aaa = max(0.0, float(u_im.max()))
+    bbb = min(0.0, float(u_im.min()))
+    uout = (aaa + bbb) / 2.0
+    c = dt * uout / ds
+
+    # w(., ., 0) = w(., ., km) = 0 for i = -1..im+1, j = -1..jm+1; i = -1 is
+    # w(ip+1, j-1, .) in the column-major layout (j = -1: w(ip+1, jp+1, k-1))
+    Wb[(0, im + 1), (-1, jm + 1), 0] = 0.0
+    Wb[(0, im + 1), (-1, jm + 1), km] = 0.0
+    Wb[ip + 1, (-1, jm), 0] = 0.0
+    Wb[ip + 1, (-1, jm), km] = 0.0
+    Wb[ip + 1, jp + 1, -1] = 0.0
+    Wb[ip + 1, jp + 1, km - 1] = 0.0
+    # top and ground, v then u: x(.,.,0) = -x(.,.,1); x(.,.,km+1) = x(.,.,km)
+    for A in (Vb, Ub):
+        A[(0, im + 1), (0, jm + 1), km] += A[(0, im + 1), (0, jm + 1), km + 1]
+        A[(0, im + 1), (0, jm + 1), km + 1] = 0.0
+        A[(0, im + 1), (0, jm + 1), 1] -= A[(0, im + 1), (0, jm + 1), 0]
+        A[(0, im + 1), (0, jm + 1), 0] = 0.0
+    # periodic j, w (k = 0..km) then v, u (k = 0..km+1)
+    for A, kr in ((Wb, (0, km)), (Vb, (0, km + 1)), (Ub, (0, km + 1))):
+        A[(0, im + 1), 1, kr] += A[(0, im + 1), jm + 1, kr]
+        A[(0, im + 1), jm + 1, kr] = 0.0
+        A[(0, im + 1), jm, kr] += A[(0, im + 1), 0, kr]
+        A[(0, im + 1), 0, kr] = 0.0
+    # outflow, w then v then u: x(e) = x(e) - (dt*uout)*(x(e) - x(e-1))/dxs(im)
+    uoutb = 0.0
+    for A, e, dx in ((Wb, im + 1, dww), (Vb, im + 1, dvv), (Ub, im, du)):
+        ob = A[e, J, K].copy()
+        uoutb += float(np.sum(-dt / ds * dx * ob))
+        A[e - 1, J, K] += c * ob
+        A[e, J, K] = (1.0 - c) * ob
+    # uout = (aaa + bbb)/2 over u(im, 1..jm, 1..km), first extreme in k-major order
+    order = u_im.T  # [k, j]
+    if aaa > 0.0:
+        kk, jj = np.unravel_index(int(np.argmax(order)), order.shape)
+        Ub[im, 1 + jj, 1 + kk] += uoutb / 2.0
+    if bbb < 0.0:
+        kk, jj = np.unravel_index(int(np.argmin(order)), order.shape)
+        Ub[im, 1 + jj, 1 + kk] += uoutb / 2.0
+    # n == 1 broadcast: x(i, j, k) = x(1, j, k), i = 2..im
+    if n == 1:
+        for A in (Ub, Vb, Wb):
+            A[1, J, K] += A[(2, im), J, K].sum(axis=0)
+            A[(2, im), J, K] = 0.0
+    # inflow: u(0:1, j, k) = wp(j, k); v = w = 0 there
+    wpb = Ub[0, J, K] + Ub[1, J, K]
+    for A in (Ub, Vb, Wb):
+        A[(0, 1), J, K] = 0.0
+    return Ub.arr, Vb.arr, Wb.arr, wpb

@@ -8,6 +8,7 @@ differences' accuracy (exact for a quadratic map up to FP64 rounding)."""
 import ctypes as C
 
 import numpy as np
+import pytest
 
 import oracle
 from oracle import adjoint64, fp64
@@ -59,3 +60,45 @@ def test_velfg_reference_adjoint_against_fp64_differences():
         rhs = sum(float(t.sum()) for t in terms)
         scale = sum(float(np.abs(t).sum()) for t in terms)
         assert abs(lhs - rhs) <= 1e-9 * scale, (s, lhs, rhs, scale)
+
+
+def bondv1_ext64(case, n, wp, u, v, w):
+    L = fp64.lib()
+    i, d, p = C.c_int, C.c_double, C.c_void_p
+    L.oracle_bondv1_ext_wind_profile.argtypes = [i, p, p, p, p, p, i, i, i, d, p, p]
+    a = {"u": np.asfortranarray(u.copy()), "v": np.asfortranarray(v.copy()), "w": np.asfortranarray(w.copy())}
+    co = {nm: np.asfortranarray(case.arrays[nm].astype(np.float64)) for nm in ("z2", "dzn", "dxs")}
+    wpa = np.asfortranarray(wp)
+    L.oracle_bondv1_ext_wind_profile(JP, a["u"].ctypes.data, co["z2"].ctypes.data, co["dzn"].ctypes.data,
+                                     a["v"].ctypes.data, a["w"].ctypes.data, KP, n, IP,
+                                     float(np.float32(case.params.dt)), co["dxs"].ctypes.data, wpa.ctypes.data)
+    return a
+
+
+
+
+
+@pytest.mark.parametrize("n", [1, 5])
+def test_bondv1_reference_adjoint_against_fp64_differences(n):
+    """bondv1 (external inflow profile) is piecewise linear; random states
+    keep the max/min of u(im, ., .) unique and away from the kinks, so
+    central differences of the FP64 oracle are exact to rounding."""
+    case = synthetic_case(IP, JP, KP, seed=4, masks_and_poisson=oracle.masks_and_poisson)
+    x = {nm: rnd(nm, 60 + s) for s, nm in enumerate(("u", "v", "w"))}
+    x["wp"] = rnd("wind_profile", 63)
+    y = {nm: rnd(nm, 70 + s) for s, nm in enumerate(("u", "v", "w"))}
+    dt = float(np.float32(case.params.dt))
+    ub, vb, wb, wpb = adjoint64.bondv1_ext_b(IP, JP, KP, case.arrays["dxs"].astype(np.float64), dt, n, x["wp"],
+                                             x["u"], x["v"], x["w"], y["u"], y["v"], y["w"])
+    adj = {"u": ub, "v": vb, "w": wb, "wp": wpb}
+    h = 1e-6
+    for s in range(2):
+        d = {nm: rnd(nm if nm != "wp" else "wind_profile", 80 + 4 * s + t)
+             for t, nm in enumerate(("u", "v", "w", "wp"))}
+        fp = bondv1_ext64(case, n, x["wp"] + h * d["wp"], *[x[nm] + h * d[nm] for nm in ("u", "v", "w")])
+        fm = bondv1_ext64(case, n, x["wp"] - h * d["wp"], *[x[nm] - h * d[nm] for nm in ("u", "v", "w")])
+        lhs = sum(float(np.sum((fp[nm] - fm[nm]) / (2 * h) * y[nm])) for nm in ("u", "v", "w"))
+        terms = [d[nm] * adj[nm] for nm in ("u", "v", "w", "wp")]
+        rhs = sum(float(t.sum()) for t in terms)
+        scale = sum(float(np.abs(t).sum()) for t in terms)
+        assert abs(lhs - rhs) <= 1e-8 * scale, (n, s, lhs, rhs, scale)
