@@ -1,5 +1,5 @@
-"""FP64 reference adjoints (reverse mode) for routines whose CUDA adjoint is
-still to come, in vectorised NumPy.
+"""FP64 reference adjoints (reverse mode) of the time step's routines and of
+the whole step, in NumPy.
 
 TEST INFRASTRUCTURE ONLY, like the rest of oracle/: the reference gradient
 that the CUDA adjoint entries are checked against, itself checked against
@@ -8,6 +8,12 @@ tests/test_adjoint64.py.
 
 bondv1_ext_b: bondv1_ext_wind_profile.f95:27-127 (inflow from the external
 profile, n == 1 broadcast, outflow with uout, periodic, top and ground).
+
+velnw_b, feedbf_b, adam_b, press_b, les_b restate in FP64 the transposes the
+CUDA entries les_velnw_b_ .. les_les_b_ compute, and Step64 composes all of
+them into the adjoint of one whole time step (the sequence of
+oracle_run_steps, main_ocl.f95:264-299, with the external inflow profile
+and a fixed SOR iteration count): the FP64 reference gradient of a step.
 
 velfg_b: vel2.f95:48-188 + velFG.f95:56-105, the face quantities of (u, v,
 w) and the advection/diffusion terms f, g, h.  The map is quadratic (cov =
@@ -304,3 +310,431 @@ def bondv1_ext_b(ip, jp, kp, dxs, dt, n, wp, u, v, w, ub, vb, wb):
     for A in (Ub, Vb, Wb):
         A[(0, 1), J, K] = 0.0
     return Ub.arr, Vb.arr, Wb.arr, wpb
+
+
+# ---- routines whose CUDA adjoint exists (les_adjoint.cuh), restated in FP64
+# for the step-level reference below.  Each takes and returns full arrays
+# with the routine's Fortran bounds; elements the routine never touches keep
+# their adjoint.
+
+def velnw_b(ip, jp, kp, dxs, dys, dzs, ro, dt, ub, vb, wb):
+    """velnw.f95:27-59: u, v (all k), w (k <= km-1) += dt*(f - (p(+1) - p)/ro/ds).
+    Returns the adjoint contributions (pb, fb, gb, hb); u, v, w keep theirs."""
+    im, jm, km = ip, jp, kp
+    Ub, Vb, Wb = (FA(n, ip, jp, kp, np.asarray(a, dtype=np.float64)) for n, a in (("u", ub), ("v", vb), ("w", wb)))
+    Pb, Fb, Gb, Hb = FA("p", ip, jp, kp), FA("f", ip, jp, kp), FA("g", ip, jp, kp), FA("h", ip, jp, kp)
+    I, J, K, K1 = (1, im), (1, jm), (1, km), (1, km - 1)
+    sh = lambda r, d: (r[0] + d, r[1] + d)
+    XS = _m1(dxs, 0, I, 0)
+    YS = _m1(dys, 0, J, 1)
+    ZS = _m1(dzs, -1, K1, 2)
+    a = dt * Ub[I, J, K] / ro / XS
+    Pb[sh(I, 1), J, K] -= a
+    Pb[I, J, K] += a
+    Fb[I, J, K] += dt * Ub[I, J, K]
+    a = dt * Vb[I, J, K] / ro / YS
+    Pb[I, sh(J, 1), K] -= a
+    Pb[I, J, K] += a
+    Gb[I, J, K] += dt * Vb[I, J, K]
+    a = dt * Wb[I, J, K1] / ro / ZS
+    Pb[I, J, sh(K1, 1)] -= a
+    Pb[I, J, K1] += a
+    Hb[I, J, K1] += dt * Wb[I, J, K1]
+    return Pb.arr, Fb.arr, Gb.arr, Hb.arr
+
+
+def feedbf_b(ip, jp, kp, masks, alpha, dt, beta, usumb, vsumb, wsumb, fb, gb, hb):
+    """feedbf.f95:38-67 on the interior: sum' = (sum + v) m; fx = (alpha sum')
+    dt + (beta v) m; f' = f + fx (fx a work array).  Returns the new
+    (usumb, vsumb, wsumb) and the contributions (ub, vb, wb); f, g, h keep
+    their adjoints."""
+    I, J, K = (1, ip), (1, jp), (1, kp)
+    out_s, out_v = [], []
+    for sname, vname, mname, sb, xb in (("usum", "u", "bmask1", usumb, fb), ("vsum", "v", "cmask1", vsumb, gb),
+                                        ("wsum", "w", "dmask1", wsumb, hb)):
+        S = FA(sname, ip, jp, kp, np.asarray(sb, dtype=np.float64).copy())
+        Vb = FA(vname, ip, jp, kp)
+        M = FA(mname, ip, jp, kp, np.asarray(masks[mname], dtype=np.float64))
+        X = FA("f", ip, jp, kp, np.asarray(xb, dtype=np.float64))
+        m = M[I, J, K]
+        t = X[I, J, K]
+        s = S[I, J, K] + (alpha * dt) * t
+        Vb[I, J, K] += (beta * m) * t + m * s
+        S[I, J, K] = m * s
+        out_s.append(S.arr)
+        out_v.append(Vb.arr)
+    return tuple(out_s), tuple(out_v)
+
+
+def adam_b(ip, jp, kp, fb, gb, hb, foldb, goldb, holdb):
+    """adam.f95:32-46: f' = 1.5 f - 0.5 fold, fold' = f on the interior."""
+    I, J, K = (1, ip), (1, jp), (1, kp)
+    res = []
+    for nm, xb, ob in (("f", fb, foldb), ("g", gb, goldb), ("h", hb, holdb)):
+        X = FA("f", ip, jp, kp, np.asarray(xb, dtype=np.float64).copy())
+        O = FA("fold", ip, jp, kp, np.asarray(ob, dtype=np.float64).copy())
+        x, o = X[I, J, K].copy(), O[I, J, K].copy()
+        X[I, J, K] = 1.5 * x + o
+        O[I, J, K] = -0.5 * x
+        res.append((X.arr, O.arr))
+    return res
+
+
+def press_b(ip, jp, kp, co, dt, omega, niter, rhsb, pb, fb, gb, hb):
+    """press.f95:49-146 with niter SOR iterations (the map is linear).  co:
+    dx1, dy1, dzn, cn1, cn2l..cn4s (Fortran layout).  Takes the adjoints of
+    the outputs rhs, p, f, g, h; returns those of the inputs (rhsb, pb, fb,
+    gb, hb) and the contributions (ub, vb, wb)."""
+    im, jm, km = ip, jp, kp
+    R = FA("rhs", ip, jp, kp, np.asarray(rhsb, dtype=np.float64).copy())
+    P = FA("p", ip, jp, kp, np.asarray(pb, dtype=np.float64).copy())
+    Fb, Gb, Hb = (FA("f", ip, jp, kp, np.asarray(a, dtype=np.float64).copy()) for a in (fb, gb, hb))
+    Ub, Vb, Wb = FA("u", ip, jp, kp), FA("v", ip, jp, kp), FA("w", ip, jp, kp)
+    d = {n: np.asarray(co[n], dtype=np.float64) for n in co}
+    X1, Y1, Z1 = (lambda i: d["dx1"][i + 1]), (lambda j: d["dy1"][j]), (lambda k: d["dzn"][k + 1])
+    cn1 = lambda i, j, k: d["cn1"][i - 1, j - 1, k - 1]
+    c1d = {n: (lambda arr: (lambda q: arr[q - 1]))(d[n]) for n in ("cn2l", "cn2s", "cn3l", "cn3s", "cn4l", "cn4s")}
+    c2l, c2s, c3l, c3s, c4l, c4s = (c1d[n] for n in ("cn2l", "cn2s", "cn3l", "cn3s", "cn4l", "cn4s"))
+    area = sum(X1(i) * Y1(j) * Z1(k) for i in range(1, im + 1) for j in range(1, jm + 1) for k in range(1, km + 1))
+
+    def bp2(A):  # boundp.f95:5-21 transposed
+        for i in range(0, im + 2):
+            for j in range(0, jm + 2):
+                A[i, j, km] += A[i, j, km + 1]
+                A[i, j, km + 1] = 0.0
+                A[i, j, 1] += A[i, j, 0]
+                A[i, j, 0] = 0.0
+
+    def bp1(A):  # boundp.f95:23-44 transposed (its j loop first)
+        for k in range(0, km + 2):
+            for i in range(0, im + 2):
+                A[i, 1, k] += A[i, jm + 1, k]
+                A[i, jm + 1, k] = 0.0
+                A[i, jm, k] += A[i, 0, k]
+                A[i, 0, k] = 0.0
+        for k in range(0, km + 2):
+            for j in range(0, jm + 2):
+                A[im, j, k] += A[im + 1, j, k]
+                A[im + 1, j, k] = 0.0
+                A[1, j, k] += A[0, j, k]
+                A[0, j, k] = 0.0
+
+    def meansub(A):  # x -= (sum w x)/W transposed: x_c -= w_c (sum x)/W
+        s = float(A[(1, im), (1, jm), (1, km)].sum())
+        for i in range(1, im + 1):
+            for j in range(1, jm + 1):
+                for k in range(1, km + 1):
+                    A[i, j, k] -= X1(i) * Y1(j) * Z1(k) * s / area
+
+    bp2(P)
+    bp1(P)
+    meansub(P)
+    for _ in range(niter):
+        bp2(P)
+        for nrd in (1, 0):
+            bp1(P)
+            inn = P.arr.copy()
+            I0 = FA("p", ip, jp, kp, inn)
+            sw = lambda i, j, k: (i + j + k + nrd) % 2 == 1
+            fr = lambda i, j, k, c: omega * cn1(i, j, k) * c * I0[i, j, k]
+            for i in range(1, im + 1):
+                for j in range(1, jm + 1):
+                    for k in range(1, km + 1):
+                        v = I0[i, j, k]
+                        if sw(i, j, k):
+                            R[i, j, k] -= omega * cn1(i, j, k) * v
+                            P[i, j, k] = (1.0 - omega) * v
+                        else:
+                            r = v
+                            if i > 1: r += fr(i - 1, j, k, c2l(i - 1))
+                            if i < im: r += fr(i + 1, j, k, c2s(i + 1))
+                            if j > 1: r += fr(i, j - 1, k, c3l(j - 1))
+                            if j < jm: r += fr(i, j + 1, k, c3s(j + 1))
+                            if k > 1: r += fr(i, j, k - 1, c4l(k - 1))
+                            if k < km: r += fr(i, j, k + 1, c4s(k + 1))
+                            P[i, j, k] = r
+            for j in range(1, jm + 1):
+                for k in range(1, km + 1):
+                    if sw(1, j, k): P[0, j, k] += fr(1, j, k, c2s(1))
+                    if sw(im, j, k): P[im + 1, j, k] += fr(im, j, k, c2l(im))
+            for i in range(1, im + 1):
+                for k in range(1, km + 1):
+                    if sw(i, 1, k): P[i, 0, k] += fr(i, 1, k, c3s(1))
+                    if sw(i, jm, k): P[i, jm + 1, k] += fr(i, jm, k, c3l(jm))
+                for j in range(1, jm + 1):
+                    if sw(i, j, 1): P[i, j, 0] += fr(i, j, 1, c4s(1))
+                    if sw(i, j, km): P[i, j, km + 1] += fr(i, j, km, c4l(km))
+    meansub(R)
+    for i in range(0, im + 1):
+        for j in range(0, jm + 1):
+            for k in range(0, km + 1):
+                rb = lambda a, b, c: R[a, b, c]
+                if j >= 1 and k >= 1:
+                    x = (rb(i, j, k) / X1(i) if i >= 1 else 0.0) - (rb(i + 1, j, k) / X1(i + 1) if i < im else 0.0)
+                    Fb[i, j, k] += x
+                    Ub[i, j, k] += x / dt
+                if i >= 1 and k >= 1:
+                    x = (rb(i, j, k) / Y1(j) if j >= 1 else 0.0) - (rb(i, j + 1, k) / Y1(j + 1) if j < jm else 0.0)
+                    Gb[i, j, k] += x
+                    Vb[i, j, k] += x / dt
+                if i >= 1 and j >= 1:
+                    x = (rb(i, j, k) / Z1(k) if k >= 1 else 0.0) - (rb(i, j, k + 1) / Z1(k + 1) if k < km else 0.0)
+                    Hb[i, j, k] += x
+                    Wb[i, j, k] += x / dt
+    R[(1, im), (1, jm), (1, km)] = 0.0
+    # bondFG.f95:15-31 transposed
+    Fb[1, (1, jm), (1, km)] += Fb[0, (1, jm), (1, km)]
+    Fb[0, (1, jm), (1, km)] = 0.0
+    Gb[(1, im), jm, (1, km)] += Gb[(1, im), 0, (1, km)]
+    Gb[(1, im), 0, (1, km)] = 0.0
+    Hb[(1, im), (1, jm), km] = 0.0
+    Hb[(1, im), (1, jm), 0] = 0.0
+    return (R.arr, P.arr, Fb.arr, Gb.arr, Hb.arr), (Ub.arr, Vb.arr, Wb.arr)
+
+
+def les_b(ip, jp, kp, co, diu, smb, fb, gb, hb):
+    """les.f95:31-182 at the state diu[1..9] (the sm it computes, boundsm,
+    the viscous terms added to f, g, h).  co: dx1, dy1, dzn.  Takes the
+    adjoints of the outputs sm, f, g, h; returns that of the input sm (0
+    where les overwrites it) and those of diu1..9; f, g, h keep theirs.  No
+    derivative passes through sqrt where the strain invariant is 0."""
+    im, jm, km = ip, jp, kp
+    D = {n: FA(f"diu{n}", ip, jp, kp, np.asarray(diu[n], dtype=np.float64)) for n in range(1, 10)}
+    Db = {n: FA(f"diu{n}", ip, jp, kp) for n in range(1, 10)}
+    Sb = FA("sm", ip, jp, kp, np.asarray(smb, dtype=np.float64).copy())
+    sm = FA("sm", ip, jp, kp)
+    seed = {c: FA("f", ip, jp, kp, np.asarray(a, dtype=np.float64)) for c, a in (("f", fb), ("g", gb), ("h", hb))}
+    d = {n: np.asarray(co[n], dtype=np.float64) for n in ("dx1", "dy1", "dzn")}
+    X, Y, Z = (lambda i: d["dx1"][i + 1]), (lambda j: d["dy1"][j]), (lambda k: d["dzn"][k + 1])
+    smc = lambda k: (0.1 * (X(0) * Y(0) * Z(k)) ** (1.0 / 3.0)) ** 2
+
+    def grads(i, j, k):
+        g = lambda n, a, b, c: D[n][a, b, c]
+        return dict(
+            d1=g(1, i, j, k), d5=g(5, i, j, k), d9=g(9, i, j, k),
+            uy=(g(2, i - 1, j, k) + g(2, i - 1, j + 1, k) + g(2, i, j, k) + g(2, i, j + 1, k)) * 0.25,
+            uz=(g(3, i - 1, j, k) + g(3, i - 1, j, k + 1) + g(3, i, j, k) + g(3, i, j, k + 1)) * 0.25,
+            vx=(g(4, i, j, k) + g(4, i, j - 1, k) + g(4, i + 1, j, k) + g(4, i + 1, j - 1, k)) * 0.25,
+            vz=(g(6, i, j - 1, k) + g(6, i, j - 1, k + 1) + g(6, i, j, k) + g(6, i, j, k + 1)) * 0.25,
+            wx=(g(7, i, j, k) + g(7, i, j, k - 1) + g(7, i + 1, j, k) + g(7, i + 1, j, k - 1)) * 0.25,
+            wy=(g(8, i, j, k) + g(8, i, j, k - 1) + g(8, i, j + 1, k) + g(8, i, j + 1, k - 1)) * 0.25)
+
+    def inv(gr):
+        a, b, c = gr["uy"] + gr["vx"], gr["wy"] + gr["vz"], gr["uz"] + gr["wx"]
+        return 2 * (gr["d1"] ** 2 + gr["d5"] ** 2 + gr["d9"] ** 2) + a * a + b * b + c * c, a, b, c
+
+    # the forward's sm (les.f95:132-152) and boundsm (boundsm.f95:13-32)
+    for i in range(1, im + 1):
+        for j in range(1, jm + 1):
+            for k in range(1, km + 1):
+                sm[i, j, k] = smc(k) * np.sqrt(inv(grads(i, j, k))[0])
+    for k in range(0, km + 2):
+        for j in range(-1, jm + 2):
+            sm[0, j, k] = sm[1, j, k]
+            sm[im + 1, j, k] = sm[im, j, k]
+    for k in range(0, km + 2):
+        for i in range(0, im + 2):
+            sm[i, jm + 1, k] = sm[i, jm, k]
+            sm[i, 0, k] = sm[i, 1, k]
+    for j in range(-1, jm + 2):
+        for i in range(0, im + 2):
+            sm[i, j, 0] = -sm[i, j, 1]
+            sm[i, j, km + 1] = sm[i, j, km]
+
+    def avg(inner, p, outer, q0, A, B, Sd, i, j, k):
+        dd = X if inner == "x" else Y
+        win, Sin = (dd(p + 1), dd(p)), dd(p) + dd(p + 1)
+        pts = []
+        for o, wo in ((0, A), (1, B)):
+            for t, wi in ((0, win[0]), (1, win[1])):
+                ii, jj, kk = i, j, k
+                if inner == "x":
+                    ii = p + t
+                else:
+                    jj = p + t
+                if outer == "y":
+                    jj = q0 + o
+                else:
+                    kk = q0 + o
+                pts.append(((ii, jj, kk), wo * wi / Sin / Sd))
+        return pts
+
+    def terms(i, j, k):  # (component, sign, divisor, evs points, D entries) of les.f95:170-274
+        Yjs, Zks, Zkm = Y(j) + Y(j + 1), Z(k) + Z(k + 1), Z(k - 1) + Z(k)
+        yield "f", 1, X(i), [((i + 1, j, k), 1.0)], [(1, (i + 1, j, k), 2.0)]
+        yield "f", -1, X(i), [((i, j, k), 1.0)], [(1, (i, j, k), 2.0)]
+        yield "f", 1, Y(j), avg("x", i, "y", j, Y(j + 1), Y(j), Yjs, i, j, k), [(2, (i, j + 1, k), 1.0), (4, (i + 1, j, k), 1.0)]
+        yield "f", -1, Y(j), avg("x", i, "y", j - 1, Y(j + 1), Y(j), Yjs, i, j, k), [(2, (i, j, k), 1.0), (4, (i + 1, j - 1, k), 1.0)]
+        yield "f", 1, Z(k), avg("x", i, "z", k, Z(k + 1), Z(k), Zks, i, j, k), [(3, (i, j, k + 1), 1.0), (7, (i + 1, j, k), 1.0)]
+        yield "f", -1, Z(k), avg("x", i, "z", k - 1, Z(k), Z(k - 1), Zkm, i, j, k), [(3, (i, j, k), 1.0), (7, (i + 1, j, k - 1), 1.0)]
+        yield "g", 1, X(i), avg("x", i, "y", j, Y(j + 1), Y(j), Yjs, i, j, k), [(2, (i, j + 1, k), 1.0), (4, (i + 1, j, k), 1.0)]
+        yield "g", -1, X(i), avg("x", i - 1, "y", j, Y(j + 1), Y(j), Yjs, i, j, k), [(2, (i - 1, j + 1, k), 1.0), (4, (i, j, k), 1.0)]
+        yield "g", 1, Y(j), [((i, j + 1, k), 1.0)], [(5, (i, j + 1, k), 2.0)]
+        yield "g", -1, Y(j), [((i, j, k), 1.0)], [(5, (i, j, k), 2.0)]
+        yield "g", 1, Z(k), avg("x", i, "z", k, Z(k + 1), Z(k), Zks, i, j, k), [(6, (i, j, k + 1), 1.0), (8, (i, j + 1, k), 1.0)]
+        yield "g", -1, Z(k), avg("x", i, "z", k - 1, Z(k), Z(k - 1), Zkm, i, j, k), [(6, (i, j, k), 1.0), (8, (i, j + 1, k - 1), 1.0)]
+        yield "h", 1, X(i), avg("x", i, "z", k, Z(k + 1), Z(k), Zks, i, j, k), [(3, (i, j, k + 1), 1.0), (7, (i + 1, j, k), 1.0)]
+        yield "h", -1, X(i), avg("x", i - 1, "z", k, Z(k + 1), Z(k), Zks, i, j, k), [(3, (i - 1, j, k + 1), 1.0), (7, (i, j, k), 1.0)]
+        yield "h", 1, Y(j), avg("y", j, "z", k, Z(k + 1), Z(k), Zks, i, j, k), [(6, (i, j, k + 1), 1.0), (8, (i, j + 1, k), 1.0)]
+        yield "h", -1, Y(j), avg("y", j - 1, "z", k, Z(k + 1), Z(k), Zks, i, j, k), [(6, (i, j - 1, k + 1), 1.0), (8, (i, j, k), 1.0)]
+        yield "h", 1, Z(k), [((i, j, k + 1), 1.0)], [(9, (i, j, k + 1), 2.0)]
+        yield "h", -1, Z(k), [((i, j, k), 1.0)], [(9, (i, j, k), 2.0)]
+
+    for i in range(1, im + 1):
+        for j in range(1, jm + 1):
+            for k in range(1, km + 1):
+                for comp, sgn, div, pts, dl in terms(i, j, k):
+                    vb = sgn * seed[comp][i, j, k] / div
+                    evs = sum(w * sm[p] for p, w in pts)
+                    Dv = sum(fac * D[n][loc] for n, loc, fac in dl)
+                    for p, w in pts:
+                        Sb[p] += vb * Dv * w
+                    for n, loc, fac in dl:
+                        Db[n][loc] += vb * evs * fac
+    # boundsm transposed, its three loops last first
+    for j in range(-1, jm + 2):
+        for i in range(0, im + 2):
+            Sb[i, j, km] += Sb[i, j, km + 1]
+            Sb[i, j, km + 1] = 0.0
+            Sb[i, j, 1] -= Sb[i, j, 0]
+            Sb[i, j, 0] = 0.0
+    for k in range(0, km + 2):
+        for i in range(0, im + 2):
+            Sb[i, 1, k] += Sb[i, 0, k]
+            Sb[i, 0, k] = 0.0
+            Sb[i, jm, k] += Sb[i, jm + 1, k]
+            Sb[i, jm + 1, k] = 0.0
+    for k in range(0, km + 2):
+        for j in range(-1, jm + 2):
+            Sb[im, j, k] += Sb[im + 1, j, k]
+            Sb[im + 1, j, k] = 0.0
+            Sb[1, j, k] += Sb[0, j, k]
+            Sb[0, j, k] = 0.0
+    # sm = smc(k) sqrt(Q) transposed
+    for i in range(1, im + 1):
+        for j in range(1, jm + 1):
+            for k in range(1, km + 1):
+                b0 = Sb[i, j, k]
+                Sb[i, j, k] = 0.0
+                gr = grads(i, j, k)
+                q, a, b, c = inv(gr)
+                if not q > 0.0:
+                    continue
+                qb = b0 * smc(k) * 0.5 / np.sqrt(q)
+                for n, key in ((1, "d1"), (5, "d5"), (9, "d9")):
+                    Db[n][i, j, k] += qb * 4.0 * gr[key]
+                ab, bb, cb = 0.5 * a * qb, 0.5 * b * qb, 0.5 * c * qb
+                for n, val, pts in (
+                        (2, ab, ((i - 1, j, k), (i - 1, j + 1, k), (i, j, k), (i, j + 1, k))),
+                        (4, ab, ((i, j, k), (i, j - 1, k), (i + 1, j, k), (i + 1, j - 1, k))),
+                        (3, cb, ((i - 1, j, k), (i - 1, j, k + 1), (i, j, k), (i, j, k + 1))),
+                        (7, cb, ((i, j, k), (i, j, k - 1), (i + 1, j, k), (i + 1, j, k - 1))),
+                        (6, bb, ((i, j - 1, k), (i, j - 1, k + 1), (i, j, k), (i, j, k + 1))),
+                        (8, bb, ((i, j, k), (i, j, k - 1), (i, j + 1, k), (i, j + 1, k - 1)))):
+                    for p in pts:
+                        Db[n][p] += val
+    return Sb.arr, {n: Db[n].arr for n in range(1, 10)}
+
+
+# ---- one whole time step (the sequence of oracle_run_steps, main_ocl.f95:
+# 264-299, with the external inflow profile) and its reference adjoint
+
+STATE = ["u", "v", "w", "p", "usum", "vsum", "wsum", "f", "g", "h", "fold", "gold", "hold", "rhs", "sm"]
+_WORK = [f"{a}{n}" for n in range(1, 10) for a in ("nou", "diu", "cov")] + ["dfu1", "dfv1", "dfw1"]
+
+
+class Step64:
+    """One step of the FP64 oracle with niter SOR iterations (no stop test)
+    and its adjoint.  co: the case's metrics, masks and Poisson coefficients
+    (Fortran layout); prm: dt, ro, vn, alpha, beta, omega."""
+
+    def __init__(self, ip, jp, kp, co, prm, niter):
+        from oracle import fp64
+        import ctypes as C
+        self.ip, self.jp, self.kp, self.prm, self.niter = ip, jp, kp, prm, niter
+        self.co = {n: np.asfortranarray(np.asarray(a, dtype=np.float64)) for n, a in co.items()}
+        L = fp64.lib()
+        i, d, p = C.c_int, C.c_double, C.c_void_p
+        L.oracle_velnw.argtypes = [i, i, i, p, d, p, p, d, p, p, p, p, p, p, p]
+        L.oracle_bondv1_ext_wind_profile.argtypes = [i, p, p, p, p, p, i, i, i, d, p, p]
+        L.oracle_velfg.argtypes = [i, i, i] + [p] * 10 + [d] + [p] * 30
+        L.oracle_feedbf.argtypes = [i, i, i] + [p] * 9 + [d, d, d] + [p] * 6
+        L.oracle_les.argtypes = [i, p, p, p, p, i, i] + [p] * 13
+        L.oracle_adam.argtypes = [i, i, p, i, i, i, p, p, p, p, p]
+        L.oracle_press_ex.argtypes = [i, i, i] + [p] * 10 + [d] + [p] * 8 + [i, d, d, p, p, p]
+        L.oracle_press_ex.restype = C.c_int
+        self.L = L
+
+    def forward(self, n, state, wp):
+        """The step from state (dict of STATE arrays) and inflow wp(j, k);
+        returns the new state and the forward values the adjoint reads."""
+        ip, jp, kp, L, pr, c = self.ip, self.jp, self.kp, self.L, self.prm, self.co
+        a = {k: np.asfortranarray(np.array(state[k], dtype=np.float64)) for k in STATE}
+        P = lambda x: x.ctypes.data
+        wpa = np.asfortranarray(np.array(wp, dtype=np.float64))
+        L.oracle_velnw(kp, jp, ip, P(a["p"]), pr["ro"], P(c["dxs"]), P(a["u"]), pr["dt"], P(a["f"]), P(c["dys"]),
+                       P(a["v"]), P(a["g"]), P(c["dzs"]), P(a["w"]), P(a["h"]))
+        tape = {"uvw_velnw": {k: a[k].copy() for k in ("u", "v", "w")}}
+        L.oracle_bondv1_ext_wind_profile(jp, P(a["u"]), P(c["z2"]), P(c["dzn"]), P(a["v"]), P(a["w"]), kp, n, ip,
+                                         pr["dt"], P(c["dxs"]), P(wpa))
+        tape["uvw_bondv1"] = {k: a[k].copy() for k in ("u", "v", "w")}
+        s = {k: np.asfortranarray(np.zeros(FL.alloc(k, ip, jp, kp).shape)) for k in _WORK}
+        s.update({k: np.asfortranarray(np.zeros(FL.alloc("f", ip, jp, kp).shape)) for k in ("fx", "fy", "fz")})
+        A = lambda k: P(a[k]) if k in a else (P(s[k]) if k in s else P(c[k]))
+        L.oracle_velfg(kp, jp, ip, *[A(k) for k in ("dx1", "cov1", "cov2", "cov3", "dfu1", "diu1", "diu2", "dy1",
+                                                    "diu3", "dzn")], pr["vn"],
+                       *[A(k) for k in ("f", "cov4", "cov5", "cov6", "dfv1", "diu4", "diu5", "diu6", "g", "cov7",
+                                        "cov8", "cov9", "dfw1", "diu7", "diu8", "diu9", "dzs", "h", "nou1", "u",
+                                        "nou5", "v", "nou9", "w", "nou2", "nou3", "nou4", "nou6", "nou7", "nou8")])
+        tape["diu"] = {m: s[f"diu{m}"].copy() for m in range(1, 10)}
+        L.oracle_feedbf(kp, jp, ip, A("usum"), A("u"), A("bmask1"), A("vsum"), A("v"), A("cmask1"), A("wsum"),
+                        A("w"), A("dmask1"), pr["alpha"], pr["dt"], pr["beta"], A("fx"), A("fy"), A("fz"),
+                        A("f"), A("g"), A("h"))
+        delx1 = np.zeros(kp)
+        L.oracle_les(kp, P(delx1), A("dx1"), A("dy1"), A("dzn"), jp, ip, *[A(f"diu{m}") for m in range(1, 10)],
+                     A("sm"), A("f"), A("g"), A("h"))
+        L.oracle_adam(n, 1 << 20, A("fold"), ip, jp, kp, A("gold"), A("hold"), A("f"), A("g"), A("h"))
+        it = L.oracle_press_ex(kp, jp, ip, A("rhs"), A("u"), A("dx1"), A("v"), A("dy1"), A("w"), A("dzn"), A("f"),
+                               A("g"), A("h"), pr["dt"], A("cn1"), A("cn2l"), A("p"), A("cn2s"), A("cn3l"),
+                               A("cn3s"), A("cn4l"), A("cn4s"), self.niter, -1.0, pr["omega"], None, None, None)
+        assert it == self.niter
+        return a, tape
+
+    def adjoint(self, n, tape, wp, seeds):
+        """Adjoints of the step's inputs (STATE arrays and wp) from those of
+        its outputs (seeds), at the forward values in tape."""
+        ip, jp, kp, pr, c = self.ip, self.jp, self.kp, self.prm, self.co
+        b = {k: np.array(seeds[k], dtype=np.float64) for k in STATE}
+        # press (press.f95:49-146)
+        (b["rhs"], b["p"], b["f"], b["g"], b["h"]), uvw = press_b(
+            ip, jp, kp, c, pr["dt"], pr["omega"], self.niter, b["rhs"], b["p"], b["f"], b["g"], b["h"])
+        for k, x in zip(("u", "v", "w"), uvw):
+            b[k] += x
+        # adam
+        (b["f"], b["fold"]), (b["g"], b["gold"]), (b["h"], b["hold"]) = adam_b(
+            ip, jp, kp, b["f"], b["g"], b["h"], b["fold"], b["gold"], b["hold"])
+        # les (diu from velfg)
+        b["sm"], diub = les_b(ip, jp, kp, c, tape["diu"], b["sm"], b["f"], b["g"], b["h"])
+        # feedbf
+        (b["usum"], b["vsum"], b["wsum"]), uvw = feedbf_b(ip, jp, kp, c, pr["alpha"], pr["dt"], pr["beta"],
+                                                          b["usum"], b["vsum"], b["wsum"], b["f"], b["g"], b["h"])
+        for k, x in zip(("u", "v", "w"), uvw):
+            b[k] += x
+        # velfg at the state after bondv1; it overwrites f, g (k = 1..km) and h (k = 1..km-1)
+        t = tape["uvw_bondv1"]
+        uvw, _ = velfg_b(ip, jp, kp, c, pr["vn"], t["u"], t["v"], t["w"], b["f"], b["g"], b["h"], diub)
+        for k, x in zip(("u", "v", "w"), uvw):
+            b[k] += x
+        for k, kr in (("f", (1, kp)), ("g", (1, kp)), ("h", (1, kp - 1))):
+            A = FA("f", ip, jp, kp, b[k])
+            A[(1, ip), (1, jp), kr] = 0.0
+        # bondv1 (external inflow) at the state after velnw
+        t = tape["uvw_velnw"]
+        b["u"], b["v"], b["w"], wpb = bondv1_ext_b(ip, jp, kp, c["dxs"], pr["dt"], n, wp, t["u"], t["v"], t["w"],
+                                                   b["u"], b["v"], b["w"])
+        # velnw
+        pb, fb, gb, hb = velnw_b(ip, jp, kp, c["dxs"], c["dys"], c["dzs"], pr["ro"], pr["dt"], b["u"], b["v"],
+                                 b["w"])
+        for k, x in (("p", pb), ("f", fb), ("g", gb), ("h", hb)):
+            b[k] += x
+        return b, wpb

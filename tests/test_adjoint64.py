@@ -102,3 +102,34 @@ def test_bondv1_reference_adjoint_against_fp64_differences(n):
         rhs = sum(float(t.sum()) for t in terms)
         scale = sum(float(np.abs(t).sum()) for t in terms)
         assert abs(lhs - rhs) <= 1e-8 * scale, (n, s, lhs, rhs, scale)
+
+
+@pytest.mark.parametrize("n", [1, 5])
+def test_step_reference_adjoint_against_fp64_differences(n):
+    """The whole step (velnw, bondv1 with the external inflow profile,
+    velfg, feedbf, les, adam, press with 3 SOR iterations) composed from the
+    reference adjoints, against central differences of the FP64 oracle's
+    step over every state array and the inflow profile."""
+    case = synthetic_case(IP, JP, KP, seed=6, masks_and_poisson=oracle.masks_and_poisson)
+    names = ["dx1", "dy1", "dzn", "dzs", "dxs", "dys", "z2", "bmask1", "cmask1", "dmask1", "cn1", "cn2l", "cn2s",
+             "cn3l", "cn3s", "cn4l", "cn4s"]
+    co = {nm: case.arrays[nm] for nm in names}
+    pr = case.params
+    prm = {k: float(np.float32(getattr(pr, k))) for k in ("dt", "ro", "vn", "alpha", "beta", "omega")}
+    step = adjoint64.Step64(IP, JP, KP, co, prm, 3)
+    x = {nm: rnd(nm, 100 + s) for s, nm in enumerate(adjoint64.STATE)}
+    wp = rnd("wind_profile", 99)
+    y = {nm: rnd(nm, 200 + s) for s, nm in enumerate(adjoint64.STATE)}
+    _, tape = step.forward(n, x, wp)
+    adj, wpb = step.adjoint(n, tape, wp, y)
+    h = 1e-6
+    for s in range(2):
+        d = {nm: rnd(nm, 300 + 20 * s + t) for t, nm in enumerate(adjoint64.STATE)}
+        dwp = rnd("wind_profile", 399 + s)
+        fp, _ = step.forward(n, {k: x[k] + h * d[k] for k in x}, wp + h * dwp)
+        fm, _ = step.forward(n, {k: x[k] - h * d[k] for k in x}, wp - h * dwp)
+        lhs = sum(float(np.sum((fp[k] - fm[k]) / (2 * h) * y[k])) for k in adjoint64.STATE)
+        terms = [d[k] * adj[k] for k in adjoint64.STATE] + [dwp * wpb]
+        rhs = sum(float(t.sum()) for t in terms)
+        scale = sum(float(np.abs(t).sum()) for t in terms)
+        assert abs(lhs - rhs) <= 1e-7 * scale, (n, s, lhs, rhs, scale, abs(lhs - rhs) / scale)
