@@ -738,3 +738,65 @@ class Step64:
         for k, x in (("p", pb), ("f", fb), ("g", gb), ("h", hb)):
             b[k] += x
         return b, wpb
+
+
+# ---- the config-3 style objective: time- and box-mean resolved TKE with the
+# cell-centred velocities of anime.f95:45-47, and its gradient by the step
+# adjoint with checkpoints and recomputation
+
+def tke(ip, jp, kp, state, box):
+    """Mean over the cells of box ((i0, i1), (j0, j1), (k0, k1), inclusive)
+    of 0.5 (uc^2 + vc^2 + wc^2), uc = 0.5 (u(i-1) + u(i)) and alike."""
+    (i0, i1), (j0, j1), (k0, k1) = box
+    U, V, W = (FA(n, ip, jp, kp, np.asarray(state[n], dtype=np.float64)) for n in ("u", "v", "w"))
+    I, J, K = (i0, i1), (j0, j1), (k0, k1)
+    sh = lambda r, d: (r[0] + d, r[1] + d)
+    uc = 0.5 * (U[sh(I, -1), J, K] + U[I, J, K])
+    vc = 0.5 * (V[I, sh(J, -1), K] + V[I, J, K])
+    wc = 0.5 * (W[I, J, sh(K, -1)] + W[I, J, K])
+    return float(np.mean(0.5 * (uc * uc + vc * vc + wc * wc)))
+
+
+def tke_seed(ip, jp, kp, state, box, scale, bar):
+    """bar[u, v, w] += scale * d tke / d (u, v, w) at state."""
+    (i0, i1), (j0, j1), (k0, k1) = box
+    ncell = (i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1)
+    I, J, K = (i0, i1), (j0, j1), (k0, k1)
+    sh = lambda r, d: (r[0] + d, r[1] + d)
+    for n, lower in (("u", (sh(I, -1), J, K)), ("v", (I, sh(J, -1), K)), ("w", (I, J, sh(K, -1)))):
+        X = FA(n, ip, jp, kp, np.asarray(state[n], dtype=np.float64))
+        B = FA(n, ip, jp, kp, bar[n])
+        c = 0.5 * (X[lower] + X[I, J, K])  # the centred value
+        g = scale / ncell * 0.5 * c  # d(0.5 c^2)/dc * dc/dx, for each of the two x
+        B[lower] += g
+        B[I, J, K] += g
+
+
+def tke_gradient(step, n0, nt, state0, wp, box, ckpt):
+    """J = (1/nt) sum over steps n0 .. n0+nt-1 of tke after the step, and its
+    gradient with respect to the inflow profile wp (held over the steps) and
+    the initial state, by the step adjoint in reverse.  Only every ckpt-th
+    state is kept; each segment's forward values are recomputed from its
+    checkpoint before the segment is reversed."""
+    ip, jp, kp = step.ip, step.jp, step.kp
+    ckpts, s, J = {0: state0}, state0, 0.0
+    for t in range(nt):
+        s, _ = step.forward(n0 + t, s, wp)
+        J += tke(ip, jp, kp, s, box) / nt
+        if (t + 1) % ckpt == 0 and t + 1 < nt:
+            ckpts[t + 1] = s
+    bar = {k: np.zeros(FL.alloc(k, ip, jp, kp).shape) for k in STATE}
+    wpb = np.zeros(np.asarray(wp).shape)
+    for t0 in sorted(ckpts, reverse=True):
+        t1 = min(t0 + ckpt, nt)
+        s, seg = ckpts[t0], []
+        for t in range(t0, t1):
+            out, tape = step.forward(n0 + t, s, wp)
+            seg.append((tape, out))
+            s = out
+        for t in reversed(range(t0, t1)):
+            tape, out = seg[t - t0]
+            tke_seed(ip, jp, kp, out, box, 1.0 / nt, bar)
+            bar, g = step.adjoint(n0 + t, tape, wp, bar)
+            wpb += g
+    return J, wpb, bar
