@@ -646,12 +646,15 @@ _WORK = [f"{a}{n}" for n in range(1, 10) for a in ("nou", "diu", "cov")] + ["dfu
 class Step64:
     """One step of the FP64 oracle with niter SOR iterations (no stop test)
     and its adjoint.  co: the case's metrics, masks and Poisson coefficients
-    (Fortran layout); prm: dt, ro, vn, alpha, beta, omega."""
+    (Fortran layout); prm: dt, ro, vn, alpha, beta, omega.  drag: an optional
+    per-column scale s(i, j) (ip x jp) on feedbf's force, f += s fx instead
+    of f += fx (feedbf.f95:61-66; s = 1 is the reference)."""
 
-    def __init__(self, ip, jp, kp, co, prm, niter):
+    def __init__(self, ip, jp, kp, co, prm, niter, drag=None):
         from oracle import fp64
         import ctypes as C
         self.ip, self.jp, self.kp, self.prm, self.niter = ip, jp, kp, prm, niter
+        self.drag = None if drag is None else np.asarray(drag, dtype=np.float64)
         self.co = {n: np.asfortranarray(np.asarray(a, dtype=np.float64)) for n, a in co.items()}
         L = fp64.lib()
         i, d, p = C.c_int, C.c_double, C.c_void_p
@@ -687,9 +690,16 @@ class Step64:
                                         "cov8", "cov9", "dfw1", "diu7", "diu8", "diu9", "dzs", "h", "nou1", "u",
                                         "nou5", "v", "nou9", "w", "nou2", "nou3", "nou4", "nou6", "nou7", "nou8")])
         tape["diu"] = {m: s[f"diu{m}"].copy() for m in range(1, 10)}
+        f0 = {k: a[k].copy() for k in ("f", "g", "h")}
         L.oracle_feedbf(kp, jp, ip, A("usum"), A("u"), A("bmask1"), A("vsum"), A("v"), A("cmask1"), A("wsum"),
                         A("w"), A("dmask1"), pr["alpha"], pr["dt"], pr["beta"], A("fx"), A("fy"), A("fz"),
                         A("f"), A("g"), A("h"))
+        tape["fxyz"] = [s[k].copy() for k in ("fx", "fy", "fz")]
+        if self.drag is not None:  # f = f0 + s fx on the interior
+            for k, x in zip(("f", "g", "h"), ("fx", "fy", "fz")):
+                F, F0, X = (FA("f", ip, jp, kp, arr) for arr in (a[k], f0[k], s[x]))
+                F[(1, ip), (1, jp), (1, kp)] = F0[(1, ip), (1, jp), (1, kp)] + \
+                    self.drag[:, :, np.newaxis] * X[(1, ip), (1, jp), (1, kp)]
         delx1 = np.zeros(kp)
         L.oracle_les(kp, P(delx1), A("dx1"), A("dy1"), A("dzn"), jp, ip, *[A(f"diu{m}") for m in range(1, 10)],
                      A("sm"), A("f"), A("g"), A("h"))
@@ -701,8 +711,9 @@ class Step64:
         return a, tape
 
     def adjoint(self, n, tape, wp, seeds):
-        """Adjoints of the step's inputs (STATE arrays and wp) from those of
-        its outputs (seeds), at the forward values in tape."""
+        """Adjoints of the step's inputs (STATE arrays) from those of its
+        outputs (seeds), at the forward values in tape, and the gradients of
+        the parameters: {"wp": inflow profile, "drag": drag scale or None}."""
         ip, jp, kp, pr, c = self.ip, self.jp, self.kp, self.prm, self.co
         b = {k: np.array(seeds[k], dtype=np.float64) for k in STATE}
         # press (press.f95:49-146)
@@ -715,9 +726,20 @@ class Step64:
             ip, jp, kp, b["f"], b["g"], b["h"], b["fold"], b["gold"], b["hold"])
         # les (diu from velfg)
         b["sm"], diub = les_b(ip, jp, kp, c, tape["diu"], b["sm"], b["f"], b["g"], b["h"])
-        # feedbf
+        # feedbf (with the drag scale, fx's adjoint is s times f's)
+        xb = [b["f"], b["g"], b["h"]]
+        dragb = None
+        if self.drag is not None:
+            dragb = np.zeros((ip, jp))
+            for q, k in enumerate(("f", "g", "h")):
+                B, X = FA("f", ip, jp, kp, b[k]), FA("f", ip, jp, kp, tape["fxyz"][q])
+                dragb += np.sum(X[(1, ip), (1, jp), (1, kp)] * B[(1, ip), (1, jp), (1, kp)], axis=2)
+                xs = b[k].copy()
+                XS = FA("f", ip, jp, kp, xs)
+                XS[(1, ip), (1, jp), (1, kp)] = self.drag[:, :, np.newaxis] * B[(1, ip), (1, jp), (1, kp)]
+                xb[q] = xs
         (b["usum"], b["vsum"], b["wsum"]), uvw = feedbf_b(ip, jp, kp, c, pr["alpha"], pr["dt"], pr["beta"],
-                                                          b["usum"], b["vsum"], b["wsum"], b["f"], b["g"], b["h"])
+                                                          b["usum"], b["vsum"], b["wsum"], *xb)
         for k, x in zip(("u", "v", "w"), uvw):
             b[k] += x
         # velfg at the state after bondv1; it overwrites f, g (k = 1..km) and h (k = 1..km-1)
@@ -737,7 +759,7 @@ class Step64:
                                  b["w"])
         for k, x in (("p", pb), ("f", fb), ("g", gb), ("h", hb)):
             b[k] += x
-        return b, wpb
+        return b, {"wp": wpb, "drag": dragb}
 
 
 # ---- the config-3 style objective: time- and box-mean resolved TKE with the
@@ -774,8 +796,9 @@ def tke_seed(ip, jp, kp, state, box, scale, bar):
 
 def tke_gradient(step, n0, nt, state0, wp, box, ckpt):
     """J = (1/nt) sum over steps n0 .. n0+nt-1 of tke after the step, and its
-    gradient with respect to the inflow profile wp (held over the steps) and
-    the initial state, by the step adjoint in reverse.  Only every ckpt-th
+    gradients with respect to the inflow profile wp (held over the steps),
+    the drag scale (when the step has one) and the initial state, by the
+    step adjoint in reverse.  Only every ckpt-th
     state is kept; each segment's forward values are recomputed from its
     checkpoint before the segment is reversed."""
     ip, jp, kp = step.ip, step.jp, step.kp
@@ -786,7 +809,7 @@ def tke_gradient(step, n0, nt, state0, wp, box, ckpt):
         if (t + 1) % ckpt == 0 and t + 1 < nt:
             ckpts[t + 1] = s
     bar = {k: np.zeros(FL.alloc(k, ip, jp, kp).shape) for k in STATE}
-    wpb = np.zeros(np.asarray(wp).shape)
+    grads = {"wp": np.zeros(np.asarray(wp).shape), "drag": None if step.drag is None else np.zeros((ip, jp))}
     for t0 in sorted(ckpts, reverse=True):
         t1 = min(t0 + ckpt, nt)
         s, seg = ckpts[t0], []
@@ -798,5 +821,7 @@ def tke_gradient(step, n0, nt, state0, wp, box, ckpt):
             tape, out = seg[t - t0]
             tke_seed(ip, jp, kp, out, box, 1.0 / nt, bar)
             bar, g = step.adjoint(n0 + t, tape, wp, bar)
-            wpb += g
-    return J, wpb, bar
+            grads["wp"] += g["wp"]
+            if grads["drag"] is not None:
+                grads["drag"] += g["drag"]
+    return J, grads, bar

@@ -121,7 +121,8 @@ def test_step_reference_adjoint_against_fp64_differences(n):
     wp = rnd("wind_profile", 99)
     y = {nm: rnd(nm, 200 + s) for s, nm in enumerate(adjoint64.STATE)}
     _, tape = step.forward(n, x, wp)
-    adj, wpb = step.adjoint(n, tape, wp, y)
+    adj, grads = step.adjoint(n, tape, wp, y)
+    wpb = grads["wp"]
     h = 1e-6
     for s in range(2):
         d = {nm: rnd(nm, 300 + 20 * s + t) for t, nm in enumerate(adjoint64.STATE)}
@@ -150,7 +151,8 @@ def test_tke_gradient_with_checkpoints_against_fp64_differences():
     wp = rnd("wind_profile", 499)
     box = ((3, 8), (2, 7), (1, 3))
     nt = 4
-    J, wpb, bar = adjoint64.tke_gradient(step, 1, nt, x, wp, box, ckpt=2)
+    J, grads, bar = adjoint64.tke_gradient(step, 1, nt, x, wp, box, ckpt=2)
+    wpb = grads["wp"]
 
     def J_of(state, w):
         s, acc = state, 0.0
@@ -170,3 +172,40 @@ def test_tke_gradient_with_checkpoints_against_fp64_differences():
     terms = [d[k] * bar[k] for k in adjoint64.STATE]
     ad = sum(float(t.sum()) for t in terms)
     assert abs(fd - ad) <= 1e-7 * sum(float(np.abs(t).sum()) for t in terms), (fd, ad)
+
+
+def test_tke_gradient_for_the_drag_scale():
+    """The same objective with a per-column drag scale s(i, j) on feedbf's
+    force (s = 1 reproduces the reference step bit for bit in FP64): its
+    gradient with respect to s against central differences."""
+    case = synthetic_case(IP, JP, KP, seed=9, masks_and_poisson=oracle.masks_and_poisson)
+    names = ["dx1", "dy1", "dzn", "dzs", "dxs", "dys", "z2", "bmask1", "cmask1", "dmask1", "cn1", "cn2l", "cn2s",
+             "cn3l", "cn3s", "cn4l", "cn4s"]
+    co = {nm: case.arrays[nm] for nm in names}
+    pr = case.params
+    prm = {k: float(np.float32(getattr(pr, k))) for k in ("dt", "ro", "vn", "alpha", "beta", "omega")}
+    x = {nm: rnd(nm, 800 + s) for s, nm in enumerate(adjoint64.STATE)}
+    wp = rnd("wind_profile", 799)
+    one = adjoint64.Step64(IP, JP, KP, co, prm, 3, drag=np.ones((IP, JP)))
+    ref = adjoint64.Step64(IP, JP, KP, co, prm, 3)
+    a1, _ = one.forward(2, x, wp)
+    a0, _ = ref.forward(2, x, wp)
+    assert all(np.array_equal(a1[k], a0[k]) for k in adjoint64.STATE)
+    drag = 1.0 + 0.3 * np.random.default_rng(5).standard_normal((IP, JP))
+    box, nt = ((3, 8), (2, 7), (1, 3)), 3
+    step = adjoint64.Step64(IP, JP, KP, co, prm, 3, drag=drag)
+    J, grads, _ = adjoint64.tke_gradient(step, 2, nt, x, wp, box, ckpt=2)
+
+    def J_of(dr):
+        st = adjoint64.Step64(IP, JP, KP, co, prm, 3, drag=dr)
+        s, acc = x, 0.0
+        for t in range(nt):
+            s, _ = st.forward(2 + t, s, wp)
+            acc += adjoint64.tke(IP, JP, KP, s, box) / nt
+        return acc
+
+    h = 1e-6
+    dd = np.random.default_rng(6).standard_normal((IP, JP))
+    fd = (J_of(drag + h * dd) - J_of(drag - h * dd)) / (2 * h)
+    ad = float(np.sum(dd * grads["drag"]))
+    assert abs(fd - ad) <= 1e-7 * float(np.sum(np.abs(dd * grads["drag"]))), (fd, ad)
