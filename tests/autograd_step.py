@@ -1,0 +1,50 @@
+"""A time step as a torch.autograd.Function (test harness).
+
+StepFunction runs one step forward and, in backward, the step's adjoint.
+Here the step is oracle/adjoint64.Step64 (the FP64 oracle's step and the
+FP64 reference adjoint); an objective written with torch operations on the
+returned state then gets its gradients with respect to the initial state,
+the inflow profile and the drag scale from loss.backward().
+"""
+import numpy as np
+import torch
+
+from oracle import adjoint64
+
+
+class StepFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, step, n, wp, drag, *state):
+        step.drag = None if drag is None else drag.detach().numpy().copy()
+        st = {k: t.detach().numpy() for k, t in zip(adjoint64.STATE, state)}
+        out, tape = step.forward(n, st, wp.detach().numpy())
+        ctx.step, ctx.n, ctx.tape, ctx.wp = step, n, tape, wp.detach().numpy().copy()
+        ctx.drag = step.drag
+        ctx.has_drag = drag is not None
+        return tuple(torch.from_numpy(np.ascontiguousarray(out[k])) for k in adjoint64.STATE)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        seeds = {k: g.numpy() for k, g in zip(adjoint64.STATE, grads)}  # unused outputs come as zeros
+        ctx.step.drag = ctx.drag
+        b, pg = ctx.step.adjoint(ctx.n, ctx.tape, ctx.wp, seeds)
+        dg = torch.from_numpy(pg["drag"]) if ctx.has_drag else None
+        return (None, None, torch.from_numpy(pg["wp"]), dg,
+                *[torch.from_numpy(np.ascontiguousarray(b[k])) for k in adjoint64.STATE])
+
+
+def tke_torch(ip, jp, kp, state, box):
+    """adjoint64.tke written with torch operations on the state tensors."""
+    (i0, i1), (j0, j1), (k0, k1) = box
+    lo = {n: [adjoint64.FL._ev(b.split(":")[0], ip, jp, kp) for b in adjoint64.FL._BOUNDS[n]] for n in "uvw"}
+
+    def view(n, a, b, c):
+        t, (li, lj, lk) = state[n], lo[n]
+        return t[a[0] - li:a[1] - li + 1, b[0] - lj:b[1] - lj + 1, c[0] - lk:c[1] - lk + 1]
+
+    I, J, K = (i0, i1), (j0, j1), (k0, k1)
+    sh = lambda r: (r[0] - 1, r[1] - 1)
+    uc = 0.5 * (view("u", sh(I), J, K) + view("u", I, J, K))
+    vc = 0.5 * (view("v", I, sh(J), K) + view("v", I, J, K))
+    wc = 0.5 * (view("w", I, J, sh(K)) + view("w", I, J, K))
+    return torch.mean(0.5 * (uc * uc + vc * vc + wc * wc))
