@@ -209,3 +209,63 @@ def test_tke_gradient_for_the_drag_scale():
     fd = (J_of(drag + h * dd) - J_of(drag - h * dd)) / (2 * h)
     ad = float(np.sum(dd * grads["drag"]))
     assert abs(fd - ad) <= 1e-7 * float(np.sum(np.abs(dd * grads["drag"]))), (fd, ad)
+
+
+def _ref_case(seed):
+    case = synthetic_case(IP, JP, KP, seed=seed, masks_and_poisson=oracle.masks_and_poisson)
+    names = ["dx1", "dy1", "dzn", "dzs", "dxs", "dys", "z2", "bmask1", "cmask1", "dmask1", "cn1", "cn2l", "cn2s",
+             "cn3l", "cn3s", "cn4l", "cn4s"]
+    pr = case.params
+    prm = {k: float(np.float32(getattr(pr, k))) for k in ("dt", "ro", "vn", "alpha", "beta", "omega")}
+    return {nm: case.arrays[nm].astype(np.float64) for nm in names}, prm
+
+
+def _dot_check(lhs_out, y, d, adj, tol):
+    lhs = sum(float(np.sum(lhs_out[k] * y[k])) for k in y)
+    terms = [d[k] * adj[k] for k in d]
+    rhs = sum(float(t.sum()) for t in terms)
+    assert abs(lhs - rhs) <= tol * sum(float(np.abs(t).sum()) for t in terms), (lhs, rhs)
+
+
+def test_press_reference_adjoint_dot_products():
+    co, prm = _ref_case(12)
+    step = adjoint64.Step64(IP, JP, KP, co, prm, 4)  # for its bound oracle_press_ex
+    L = step.L
+    outs, ins = ["rhs", "p", "f", "g", "h"], ["rhs", "u", "v", "w", "f", "g", "h", "p"]
+    y = {k: rnd(k, 1000 + s) for s, k in enumerate(outs)}
+    (rb, pb, fb, gb, hb), (ub, vb, wb) = adjoint64.press_b(IP, JP, KP, co, prm["dt"], prm["omega"], 4, y["rhs"],
+                                                           y["p"], y["f"], y["g"], y["h"])
+    adj = {"rhs": rb, "p": pb, "f": fb, "g": gb, "h": hb, "u": ub, "v": vb, "w": wb}
+    x = {k: rnd(k, 1100 + s) for s, k in enumerate(ins)}
+    a = {k: np.asfortranarray(x[k].copy()) for k in ins}
+    c = {k: np.asfortranarray(co[k]) for k in co}
+    P = lambda k: (a[k] if k in a else c[k]).ctypes.data
+    L.oracle_press_ex(KP, JP, IP, P("rhs"), P("u"), P("dx1"), P("v"), P("dy1"), P("w"), P("dzn"), P("f"), P("g"),
+                      P("h"), prm["dt"], P("cn1"), P("cn2l"), P("p"), P("cn2s"), P("cn3l"), P("cn3s"), P("cn4l"),
+                      P("cn4s"), 4, -1.0, prm["omega"], None, None, None)
+    _dot_check({k: a[k] for k in outs}, y, x, adj, 1e-12)
+
+
+def test_les_reference_adjoint_against_fp64_differences():
+    co, prm = _ref_case(13)
+    step = adjoint64.Step64(IP, JP, KP, co, prm, 1)
+    L = step.L
+    diu = {n: rnd(f"diu{n}", 1200 + n) for n in range(1, 10)}
+    outs = ["sm", "f", "g", "h"]
+    y = {k: rnd(k, 1300 + s) for s, k in enumerate(outs)}
+    smb, diub = adjoint64.les_b(IP, JP, KP, co, diu, y["sm"], y["f"], y["g"], y["h"])
+    adj = {"sm": smb, "f": y["f"], "g": y["g"], "h": y["h"], **{f"diu{n}": diub[n] for n in range(1, 10)}}
+    base = {k: rnd(k, 1400 + s) for s, k in enumerate(outs)}
+    d = {k: rnd(k, 1500 + s) for s, k in enumerate(list(adj))}
+
+    def run(sign, h=1e-6):
+        a = {k: np.asfortranarray(base[k] + sign * h * d[k]) for k in outs}
+        a.update({f"diu{n}": np.asfortranarray(diu[n] + sign * h * d[f"diu{n}"]) for n in range(1, 10)})
+        c = {k: np.asfortranarray(co[k]) for k in ("dx1", "dy1", "dzn")}
+        dl = np.zeros(KP)
+        L.oracle_les(KP, dl.ctypes.data, c["dx1"].ctypes.data, c["dy1"].ctypes.data, c["dzn"].ctypes.data, JP, IP,
+                     *[a[f"diu{n}"].ctypes.data for n in range(1, 10)], *[a[k].ctypes.data for k in outs])
+        return a
+
+    fp, fm = run(1.0), run(-1.0)
+    _dot_check({k: (fp[k] - fm[k]) / 2e-6 for k in outs}, y, d, adj, 1e-8)
