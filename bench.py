@@ -121,63 +121,89 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_case(on_device_setup=True):
+def workload_desc(ip, jp, kp):
+    """The workload's name in both arms' config (identical strings)."""
+    W = WORKLOAD
+    return (f"LES plain FP32 step {ip}x{jp}x{kp} ({round(W['plan_area'] * 100)}% plan area, heights "
+            f"<={W['h_max']:g} m, dt={W['dt']:g}, SOR {W['nmaxp']} sweeps/step)")
+
+
+def native_libs():
+    """Shared libraries of this repository mapped into the process."""
+    out = set()
+    try:
+        for ln in Path("/proc/self/maps").read_text().splitlines():
+            f = ln.split()[-1] if ln.split() else ""
+            if f.endswith(".so") and f.startswith(str(ROOT)):
+                out.add(str(Path(f).relative_to(ROOT)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def make_case():
+    """The workload built with the library's setup routines (masks and
+    Poisson coefficients on the device)."""
     import les_halo_b200 as lh
     W = WORKLOAD
-    kw = dict(plan_area=W["plan_area"], h_max=W["h_max"])
-    if on_device_setup:
-        return lh.synthetic_case(W["ip"], W["jp"], W["kp"], seed=W["seed"], dt=W["dt"],
-                                 nmaxp=W["nmaxp"], **kw)
+    return lh.synthetic_case(W["ip"], W["jp"], W["kp"], seed=W["seed"], dt=W["dt"], nmaxp=W["nmaxp"],
+                             plan_area=W["plan_area"], h_max=W["h_max"])
+
+
+def oracle_case():
+    """The same workload built by the CPU oracle alone (no liblesb200.so)."""
     import oracle
-    return lh.synthetic_case(W["ip"], W["jp"], W["kp"], seed=W["seed"], dt=W["dt"],
-                             nmaxp=W["nmaxp"], masks_and_poisson=oracle.masks_and_poisson, **kw)
+    W = WORKLOAD
+    return oracle.synthetic_case(W["ip"], W["jp"], W["kp"], seed=W["seed"], dt=W["dt"], nmaxp=W["nmaxp"],
+                                 plan_area=W["plan_area"], h_max=W["h_max"])
 
 
-def cpu_baseline(threads: int, ip=300, jp=300, kp=120, steps=4):
-    """The oracle (CPU restatement of the reference's Fortran step) on a
-    bounded sample: `steps` full time steps of an ip x jp x kp sub-domain of
-    the workload (same kp, SOR sweeps and per-cell work), about 10 s of work
-    on a 16-core host."""
+def cpu_baseline(threads: int, steps=2):
+    """The oracle (CPU restatement of the reference's Fortran step) on the
+    workload itself: after the ifdata warm-up and one untimed step (the
+    n == 1 inflow broadcast), `steps` full time steps, timed.  About 20 s of
+    work on a 16-core host at 600 x 600 x 120."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    import les_halo_b200 as lh
     import oracle
-    W = WORKLOAD
-    case = lh.synthetic_case(ip, jp, kp, seed=W["seed"], dt=W["dt"], nmaxp=W["nmaxp"],
-                             plan_area=W["plan_area"], h_max=W["h_max"],
-                             masks_and_poisson=oracle.masks_and_poisson)
+    case = oracle_case()
     oracle.ifdata(case, 1)
     oracle.run_steps(case, 1, 1)  # untimed first step (n==1 broadcast)
     t0 = time.perf_counter()
     oracle.run_steps(case, 2, steps)
     dt = time.perf_counter() - t0
-    return {"value": round(ip * jp * kp * steps / dt / 1e6, 3), "unit": "Mpts/s", "cores": threads,
+    cells = case.ip * case.jp * case.kp
+    return {"value": round(cells * steps / dt / 1e6, 3), "unit": "Mpts/s", "cores": threads,
             "kind": "port",
-            "sample": f"{steps} full step(s) (n>=2) of a {ip}x{jp}x{kp} sub-domain of the workload, "
-                      f"oracle C++ restatement of the Fortran CPU path, OpenMP {threads} threads, "
-                      f"{dt:.2f} s"}
+            "sample": f"{steps} full time steps (n=2..{steps + 1}) of the {case.ip}x{case.jp}x{case.kp} "
+                      f"workload itself, after the warm-up and one untimed step; oracle C++ restatement "
+                      f"of the Fortran CPU path, OpenMP {threads} threads, {dt:.2f} s"}
 
 
 def run_reference(args):
+    """The reference's CPU time step on the host cores, on the same
+    workload, metric and steps as the GPU arm: W untimed steps, then K
+    timed full steps of the whole grid.  The reference's Fortran cannot be
+    built here (no Fortran compiler), so its line-by-line C++ restatement
+    (the oracle, OpenMP over all host threads) stands for it; the case is
+    built by the oracle alone, so the library under test is never loaded."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    import les_halo_b200 as lh
     import oracle
     W = WORKLOAD
-    ip, jp, kp = 120, 120, W["kp"]
-    case = lh.synthetic_case(ip, jp, kp, seed=W["seed"], dt=W["dt"], nmaxp=W["nmaxp"],
-                             plan_area=W["plan_area"], h_max=W["h_max"],
-                             masks_and_poisson=oracle.masks_and_poisson)
+    case = oracle_case()
+    ip, jp, kp = case.ip, case.jp, case.kp
     oracle.ifdata(case, 1)
     n = 1
     for _ in range(args.warmup):
         oracle.run_steps(case, n, 1)
         n += 1
+    iters = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        oracle.run_steps(case, n, 1)
+        iters += oracle.run_steps(case, n, 1)
         n += 1
     dt = time.perf_counter() - t0
     val = ip * jp * kp * args.steps / dt / 1e6
@@ -185,16 +211,17 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "Mpts/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "LES plain FP32 step 600x600x120 (35% plan area, SOR 50), per-step "
-                               f"sample {ip}x{jp}x{kp}", "sor_iters": W["nmaxp"],
-                   "l2": "CPU run"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain + log-law inflow)",
+        "config": {"workload": workload_desc(ip, jp, kp), "grid": [ip, jp, kp],
+                   "sor_iters": int(max(iters)) if iters else W["nmaxp"],
+                   "parallelism": f"host cores x{threads}", "l2": "CPU run"},
         "cpu_baseline": {"value": round(val, 3), "unit": "Mpts/s", "cores": threads, "kind": "port",
-                         "sample": f"each step: one full time step of a {ip}x{jp}x{kp} sub-domain, "
-                                   "oracle restatement of the reference Fortran (no Fortran "
-                                   "compiler here to build the reference itself)"},
+                         "sample": f"each step: one full time step of the {ip}x{jp}x{kp} workload; oracle "
+                                   "C++ restatement of the reference Fortran (no Fortran compiler here to "
+                                   f"build the reference itself), OpenMP {threads} threads"},
         "e2e": {"value": round(val, 3), "unit": "Mpts/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "native_libs": native_libs(),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -319,7 +346,7 @@ def run_ours(args):
     import les_halo_b200 as lh
     from les_halo_b200 import abi
 
-    case = make_case(on_device_setup=True)
+    case = make_case()
     cells = case.ip * case.jp * case.kp
     gpu = lh.GpuLes(case)
     gpu.warmup(1)
@@ -466,8 +493,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded terrain + log-law inflow)",
-            "config": {"workload": f"LES plain FP32 step {case.ip}x{case.jp}x{case.kp} (35% plan area, "
-                                   "heights <=120 m, dt=0.05, SOR 50 sweeps/step)",
+            "config": {"workload": workload_desc(case.ip, case.jp, case.kp),
                        "grid": [case.ip, case.jp, case.kp], "sor_iters": int(m["sor_iters"]),
                        "parallelism": f"replicas x{ws}",
                        "sor_tile": {"iters_per_pass": tT, "rows": tY, "cols": tX, "k_chunks": tK},

@@ -110,7 +110,9 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out);
 les_status les_ctx_destroy(les_ctx *ctx);
 /* initialise_LES_kernel (TEMPL:18-215): copy the model state, metrics,
  * masks and Poisson coefficients to the device.  Fields the model does not
- * read (rhs, delx1) may be NULL. */
+ * read (rhs, delx1) may be NULL.  Every array given is scanned first: a NaN
+ * or Inf anywhere returns LES_ERR_NAN naming the array and its Fortran
+ * index, before anything reaches the device. */
 les_status les_ctx_upload(les_ctx *ctx, const les_host_fields *hf);
 /* Copy the device state back; any NULL pointer is skipped.  rhs is returned
  * after the rhsav subtraction (press.f95:80-82), as the reference holds it. */
@@ -144,6 +146,19 @@ les_status les_ctx_set_timing(les_ctx *ctx, int nslots);
  * give identical results; odd jp and a just-uploaded p whose ghosts are not
  * boundary-consistent always use the per-colour sweeps. */
 les_status les_ctx_set_sor_path(les_ctx *ctx, int exact);
+/* Order of the step's global sums.  LES_RED_CANONICAL (default): rhsav, the
+ * SOR residual and pav are exact sums (each FP32 term converted exactly to
+ * fixed point, summed without rounding, finished in FP64), the same whatever
+ * the reduction tree.  Each LES_RED_F_* bit instead takes one of them as the
+ * reference's sequential FP32 loop, term for term in its Fortran order:
+ * rhsav and the volume (press.f95:66-75), the residual sum(reltmp^2) over
+ * colour 0 then colour 1 (press.f95:87-99), pav and pco (press.f95:123-133).
+ * Those sums run on one thread block (milliseconds each): a parity mode,
+ * not a fast path.  LES_RED_F_SOR runs the SOR one colour sweep at a time.
+ * Excludes the FP64-refined press (LES_ERR_STATE). */
+enum { LES_RED_CANONICAL = 0, LES_RED_F_RHSAV = 1, LES_RED_F_SOR = 2, LES_RED_F_PAV = 4,
+       LES_RED_FAITHFUL = 7 };
+les_status les_ctx_set_reduction_mode(les_ctx *ctx, int mode);
 /* SOR iterations one SOR kernel launch of the next step carries: 0.5 for a
  * colour sweep, 2 for a multi-iteration pass. */
 float les_ctx_sor_iters_per_launch(les_ctx *ctx);
@@ -179,7 +194,11 @@ enum { LES_H_P = 0, LES_H_UVW, LES_H_UVWSUM, LES_H_FGH, LES_H_FGH_OLD, LES_H_RHS
 size_t les_ctx_halo_floats(les_ctx *ctx, int which);
 /* ST_HALO_READ_*: pack the ring of the state array into buf (host). */
 les_status les_ctx_halo_read(les_ctx *ctx, int which, float *buf);
-/* ST_HALO_WRITE_*: unpack buf (host) into the ring of the state array. */
+/* ST_HALO_WRITE_*: unpack buf (host) into the ring of the state array.
+ * Components with no state behind them are ignored: the second component
+ * of p2 (p2 reads as (p, p)), the fourth of the float4 arrays, and u, v at
+ * uvw's k = -1 layer (convert_to_uvw, module_LES_conversions.f95:18-21,
+ * reads them as 0). */
 les_status les_ctx_halo_write(les_ctx *ctx, int which, const float *buf);
 
 /* ---- halo pack/unpack on caller arrays (halo_exchange.cl) -------------
@@ -399,8 +418,12 @@ les_status les_boundp2_(const int *jm, const int *im, float *p, const int *km);
  * GPU loading the library holds until exit, so ceil(im/32) * ceil(jm/8) must be
  * at most 5456 (e.g. im = jm = 1024 needs 4096); larger grids are rejected
  * with LES_ERR_DIMS before any device work.  The first call on each device
- * looks up the scratch address; make it outside any stream capture.  Calls
- * that overlap in time on one device share the scratch and race. */
+ * looks up the scratch address; make it outside any stream capture.  The
+ * address is kept for the life of the process, which assumes each device
+ * keeps one primary context: after cudaDeviceReset (which unloads the
+ * module holding the scratch) the kept address is stale, so do not call
+ * this entry again in that process.  Calls that overlap in time on one
+ * device share the scratch and race. */
 les_status les_press_rhs_noalloc(int km, int jm, int im, float *rhs, const float *u,
                                  const float *dx1, const float *v, const float *dy1,
                                  const float *w, const float *dzn, float *f, float *g, float *h,

@@ -13,6 +13,8 @@ LIB_PATH = Path(__file__).resolve().parent / "liblesb200.so"
 LES_OK, LES_ERR_BAD_ARG, LES_ERR_DIMS, LES_ERR_CUDA, LES_ERR_TIMEOUT, LES_ERR_NAN, \
     LES_ERR_NOMEM, LES_ERR_STATE, LES_ERR_IO = range(9)
 LES_INFLOW_POWER_LAW, LES_INFLOW_EXTERNAL = 0, 1
+# les_ctx_set_reduction_mode bits: sums taken in the reference's serial FP32 order
+LES_RED_CANONICAL, LES_RED_F_RHSAV, LES_RED_F_SOR, LES_RED_F_PAV, LES_RED_FAITHFUL = 0, 1, 2, 4, 7
 FIELD_IDS = ["u", "v", "w", "p", "usum", "vsum", "wsum", "f", "g", "h", "fold", "gold", "hold",
              "rhs", "sm", "amask1", "bmask1", "cmask1", "dmask1"]
 HALO_IDS = ["p", "uvw", "uvwsum", "fgh", "fgh_old", "rhs", "sm"]
@@ -96,6 +98,7 @@ _SIGS = {
     "les_ctx_launch_count": (C.c_uint64, [_P]),
     "les_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "les_ctx_set_sor_path": (C.c_int, [_P, C.c_int]),
+    "les_ctx_set_reduction_mode": (C.c_int, [_P, C.c_int]),
     "les_ctx_sor_iters_per_launch": (C.c_float, [_P]),
     "les_ctx_sor_tile": (C.c_int, [_P, _I, _I]),
     "les_ctx_sor_shape": (C.c_int, [_P, _I, _I, _I, _I]),

@@ -209,6 +209,10 @@ struct les_ctx {
     double2 *d_dpart = nullptr;           // FP64 per-block partial sums
     double *d_refw = nullptr;             // left null vector weights wx, wy, wz
     SpecState *spec = nullptr;            // spectral inner solve (inner = 0)
+    // reduction mode (les_ctx_set_reduction_mode): LES_RED_F_* bits take
+    // rhsav, the SOR residual or pav in the reference's sequential FP32 order
+    int red_mode = LES_RED_CANONICAL;
+    float *d_r2 = nullptr;                // reltmp^2 per cell (box), LES_RED_F_SOR only
 };
 
 // Buffers of an SOR pass other than the context's p / second p / rhs / scalars.
@@ -235,7 +239,8 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
 bool spec_eager(const les_ctx *c) { return c->ref_outer > 0 && c->ref_inner == 0; }
 
 bool sor_per_colour(const les_ctx *c) {
-    return c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok || c->prm.kp >= kTbKMax;
+    return c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok || c->prm.kp >= kTbKMax ||
+           (c->red_mode & LES_RED_F_SOR);
 }
 
 void drop_step_graphs(les_ctx *c) {
@@ -471,7 +476,10 @@ les_status enqueue_press(les_ctx *c, bool exact) {
     const long long n1 = 2LL * (g.jm + 2) * (g.km + 2) + 2LL * g.im * (g.km + 2);
     const long long n2 = 2LL * (g.im + 2) * (g.jm + 2);
     LAUNCH(c, k_rhs, rg, rb, g, c->F, c->red_kchunk, c->d_part);
-    LAUNCH(c, k_final_rhsav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
+    if (c->red_mode & LES_RED_F_RHSAV)
+        LAUNCH(c, k_seq_sum<0>, dim3(1), dim3(kSeqNT), g, c->F.rhs, nullptr, 0.0f, c->d_scal);
+    else
+        LAUNCH(c, k_final_rhsav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
     if (c->ref_outer > 0) LAUNCH(c, k_ref_rhsav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_ref);
     MARK(c, EV_RHS);
     if (exact) {
@@ -480,15 +488,18 @@ les_status enqueue_press(les_ctx *c, bool exact) {
                 if (l == 0 && nrd == 0) MARK(c, EV_SOR1_START);
                 if (c->cn1_box)
                     LAUNCH(c, k_sor_colour<true>, rg, rb, g, c->F.p, c->F.rhs, c->cn1_box, nrd, c->red_kchunk,
-                           c->d_part + nrd * np, c->d_scal);
+                           c->d_part + nrd * np, c->d_scal, c->d_r2);
                 else
                     LAUNCH(c, k_sor_colour<false>, rg, rb, g, c->F.p, c->F.rhs, nullptr, nrd, c->red_kchunk,
-                           c->d_part + nrd * np, c->d_scal);
+                           c->d_part + nrd * np, c->d_scal, c->d_r2);
                 if (l == 0 && nrd == 0) MARK(c, EV_SOR1_END);
                 LAUNCH(c, k_boundp1<true>, dim3(cdiv(n1, 256)), dim3(256), g, c->F.p, c->d_scal);
             }
             LAUNCH(c, k_boundp2<true>, dim3(cdiv(n2, 256)), dim3(256), g, c->F.p, c->d_scal);
-            LAUNCH(c, k_final_sor, dim3(1), dim3(1024), c->d_part, 2 * np, c->prm.pjuge, c->d_scal);
+            if (c->red_mode & LES_RED_F_SOR)
+                LAUNCH(c, k_seq_sum<1>, dim3(1), dim3(kSeqNT), g, c->d_r2, nullptr, c->prm.pjuge, c->d_scal);
+            else
+                LAUNCH(c, k_final_sor, dim3(1), dim3(1024), c->d_part, 2 * np, c->prm.pjuge, c->d_scal);
         }
     } else {
         const int nmaxp = c->prm.nmaxp;
@@ -517,8 +528,13 @@ les_status enqueue_press(les_ctx *c, bool exact) {
         MARK(c, EV_PAV);
         return st;
     }
-    LAUNCH(c, k_pav_reduce, rg, rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, c->red_kchunk, c->d_part, c->d_scal);
-    LAUNCH(c, k_final_pav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
+    if (c->red_mode & LES_RED_F_PAV) {
+        LAUNCH(c, k_seq_sum<2>, dim3(1), dim3(kSeqNT), g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, 0.0f, c->d_scal);
+    } else {
+        LAUNCH(c, k_pav_reduce, rg, rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, c->red_kchunk, c->d_part,
+               c->d_scal);
+        LAUNCH(c, k_final_pav, dim3(1), dim3(1024), c->d_part, np, c->area, c->d_scal);
+    }
     LAUNCH(c, k_pav_adjust, rg, rb, g, c->F.p, c->d_p2 ? c->d_p2 : c->F.p, c->d_scal, c->red_kchunk);
     MARK(c, EV_PAV);
     return LES_OK;
@@ -923,6 +939,7 @@ les_status les_ctx_destroy(les_ctx *c) {
     cudaFree(c->d_ref);
     cudaFree(c->d_dpart);
     cudaFree(c->d_refw);
+    cudaFree(c->d_r2);
     spec_release(c->spec);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -970,12 +987,70 @@ static les_status download_field(les_ctx *c, int f, float *host) {
     return LES_OK;
 }
 
+// Index of the first non-finite float in a[0..n), or -1.  Chunks are
+// OR-reduced without branches (vectorisable); only a hit is located.
+static long long first_non_finite(const float *a, size_t n) {
+    const uint32_t *b = reinterpret_cast<const uint32_t *>(a);
+    constexpr size_t kChunk = 4096;
+    for (size_t o = 0; o < n; o += kChunk) {
+        const size_t e = std::min(n, o + kChunk);
+        uint32_t hit = 0;
+        for (size_t t = o; t < e; ++t) hit |= (uint32_t)((b[t] & 0x7f800000u) == 0x7f800000u);
+        if (hit)
+            for (size_t t = o; t < e; ++t)
+                if ((b[t] & 0x7f800000u) == 0x7f800000u) return (long long)t;
+    }
+    return -1;
+}
+
+// Input check of les_ctx_upload: every array given must be finite (the
+// reference has no such check; a NaN or Inf would spread through the step).
+static les_status scan_inputs(les_ctx *c, const les_host_fields *hf) {
+    const int ip = c->prm.ip, jp = c->prm.jp, kp = c->prm.kp;
+    struct Arr {
+        const char *name;
+        const float *p;
+        size_t n;
+    };
+    const Arr tabs[] = {{"dx1", hf->dx1, (size_t)ip + 3},  {"dy1", hf->dy1, (size_t)jp + 2},
+                        {"dzn", hf->dzn, (size_t)kp + 4},  {"dzs", hf->dzs, (size_t)kp + 4},
+                        {"dxs", hf->dxs, (size_t)ip + 1},  {"dys", hf->dys, (size_t)jp + 1},
+                        {"cn2l", hf->cn2l, (size_t)ip},    {"cn2s", hf->cn2s, (size_t)ip},
+                        {"cn3l", hf->cn3l, (size_t)jp},    {"cn3s", hf->cn3s, (size_t)jp},
+                        {"cn4l", hf->cn4l, (size_t)kp},    {"cn4s", hf->cn4s, (size_t)kp},
+                        {"z2", hf->z2, (size_t)kp + 2},    {"wind_profile", hf->wind_profile, (size_t)jp * kp}};
+    for (const Arr &a : tabs) {
+        if (!a.p) continue;
+        const long long t = first_non_finite(a.p, a.n);
+        if (t >= 0) return fail(LES_ERR_NAN, "les_ctx_upload: %s[%lld] is not finite", a.name, t);
+    }
+    static const char *names[LES_NFIELDS] = {"u",    "v",    "w",    "p",      "usum",   "vsum",   "wsum",
+                                             "f",    "g",    "h",    "fold",   "gold",   "hold",   "rhs",
+                                             "sm",   "amask1", "bmask1", "cmask1", "dmask1"};
+    const float *src[LES_NFIELDS] = {hf->u,    hf->v,    hf->w,    hf->p,   hf->usum,   hf->vsum,   hf->wsum,
+                                     hf->f,    hf->g,    hf->h,    hf->fold, hf->gold,  hf->hold,   hf->rhs,
+                                     hf->sm,   hf->amask1, hf->bmask1, hf->cmask1, hf->dmask1};
+    for (int f = 0; f < LES_NFIELDS; ++f) {
+        if (!src[f]) continue;
+        const FBounds b = field_bounds(f, ip, jp, kp);
+        const long long t = first_non_finite(src[f], b.n());
+        if (t >= 0) {
+            const int i = b.li + (int)(t % b.ni()), r = (int)(t / b.ni());
+            const int j = b.lj + r % b.nj(), k = b.lk + r / b.nj();
+            return fail(LES_ERR_NAN, "les_ctx_upload: %s(%d,%d,%d) is not finite", names[f], i, j, k);
+        }
+    }
+    return LES_OK;
+}
+
 les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
     if (!c || !hf) return fail(LES_ERR_BAD_ARG, "NULL argument");
     if (!hf->dx1 || !hf->dy1 || !hf->dzn || !hf->dzs || !hf->dxs || !hf->dys || !hf->cn2l || !hf->cn2s ||
         !hf->cn3l || !hf->cn3s || !hf->cn4l || !hf->cn4s)
         return fail(LES_ERR_BAD_ARG, "metric tables and Poisson coefficients are required");
-    les_status s = build_tables(c, hf, true);
+    les_status s = scan_inputs(c, hf);
+    if (s != LES_OK) return s;
+    s = build_tables(c, hf, true);
     if (s != LES_OK) return s;
     const float *src[LES_NFIELDS] = {hf->u,    hf->v,    hf->w,    hf->p,   hf->usum,   hf->vsum,   hf->wsum,
                                      hf->f,    hf->g,    hf->h,    hf->fold, hf->gold,  hf->hold,   hf->rhs,
@@ -1067,9 +1142,28 @@ les_status les_ctx_set_sor_path(les_ctx *c, int exact) {
     return ok();
 }
 
+les_status les_ctx_set_reduction_mode(les_ctx *c, int mode) {
+    if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    if (mode < 0 || mode > LES_RED_FAITHFUL) return fail(LES_ERR_BAD_ARG, "bad reduction mode %d", mode);
+    if (mode != LES_RED_CANONICAL && c->ref_outer > 0)
+        return fail(LES_ERR_STATE, "reference-order sums and the FP64-refined press exclude each other");
+    if ((mode & LES_RED_F_SOR) && !c->d_r2) {
+        if (cudaMalloc(&c->d_r2, sizeof(float) * c->box_elems) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LES_ERR_NOMEM, "reltmp^2 buffer");
+        }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->red_mode = mode;
+    drop_step_graphs(c);  // the captured steps hold the previous mode's kernels
+    return ok();
+}
+
 les_status les_set_wind_profile(les_ctx *c, const float *wp) {
     if (!c || !wp) return fail(LES_ERR_BAD_ARG, "NULL argument");
     if (c->prm.inflow_mode != LES_INFLOW_EXTERNAL) return fail(LES_ERR_STATE, "context uses the power-law inflow");
+    const long long bad = first_non_finite(wp, (size_t)c->prm.jp * c->prm.kp);
+    if (bad >= 0) return fail(LES_ERR_NAN, "les_set_wind_profile: wind_profile[%lld] is not finite", bad);
     CK(cudaMemcpyAsync(c->d_tables + c->tl.wind, wp, sizeof(float) * (size_t)c->prm.jp * c->prm.kp,
                        cudaMemcpyHostToDevice, c->stream));
     return ok();
@@ -1278,6 +1372,9 @@ static les_status ctx_halo(les_ctx *c, int which, float *buf, int write) {
     if (!ctx_halo_view(c, which, cv, d)) return fail(LES_ERR_BAD_ARG, "bad halo id %d", which);
     const size_t n = d.vsz * d.vdim;
     if (n > c->stage_elems) return fail(LES_ERR_DIMS, "halo larger than the staging buffer");
+    // p2 = (p, p): both components read p; on write the second is ignored,
+    // so one value lands on each p point
+    if (write && which == LES_H_P) cv.comp[1] = nullptr;
     if (write) CK(cudaMemcpyAsync(c->d_stage, buf, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
     LAUNCH(c, k_ctx_halo, dim3(cdiv((long long)n, 256)), dim3(256), c->geo, cv, c->d_stage, d, write);
     if (!write) CK(cudaMemcpyAsync(buf, c->d_stage, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));

@@ -20,7 +20,10 @@
 //                     of dx1*dy1*dzn); written before they are read, so
 //                     their contents between calls do not matter.
 // One scratch serves all calls on a device: calls that overlap in time on
-// the same device (two streams, two host threads) race on it.
+// the same device (two streams, two host threads) race on it.  The looked-up
+// address is kept per device for the life of the process, which assumes one
+// primary context per device: a cudaDeviceReset unloads the module and
+// leaves the kept address stale (documented at the declaration).
 #include <cuda_runtime.h>
 
 #include <cstdio>

@@ -145,10 +145,12 @@ __global__ void __launch_bounds__(1024) k_final_rhsav(const FixPart *part, int n
 // other colour and ghost cells, so the in-place parallel sweep equals the
 // reference's sequential one.  cn1 is rebuilt from its separable parts, or
 // read from the caller's array (CN1MEM, the per-routine press entry).
+// r2 (may be NULL): each swept cell's reltmp^2 stored at its box index, for
+// the reference-order residual sum (k_seq_sum).
 template <bool CN1MEM>
 __global__ void __launch_bounds__(kRedNT) k_sor_colour(Geo g, float *__restrict__ p, const float *__restrict__ rhs,
                                                         const float *__restrict__ cn1b, int nrd, int kchunk,
-                                                        FixPart *part, const Scal *s) {
+                                                        FixPart *part, const Scal *s, float *__restrict__ r2) {
     if (s->converged) return;
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
@@ -172,6 +174,7 @@ __global__ void __launch_bounds__(kRedNT) k_sor_colour(Geo g, float *__restrict_
                            pc);
             p[c] = pc + reltmp;
             acc += fix_term(reltmp * reltmp, bad);
+            if (r2) r2[c] = reltmp * reltmp;
         }
     }
     block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
@@ -294,6 +297,108 @@ __global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *p, const fl
         };
         put(k);
         if (ke != -9) put(ke);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Reference-order sums (reduction mode bits LES_RED_F_*): the sequential FP32
+// loops of press.f95 restated exactly, for parity runs against the
+// reference's own summation order.
+//   kind 0: rhsav = sum(dx1*dy1*dzn*rhs) / sum(dx1*dy1*dzn), press.f95:66-75
+//   kind 1: sor = sum(reltmp^2) over colour 0 then colour 1, each in
+//           (k, j, i) order, press.f95:87-99, and the stop test of :114
+//   kind 2: pav = sum(p*dx1*dy1*dzn) / sum(dx1*dy1*dzn), press.f95:123-133
+// A serial FP32 sum has one order, so one block does it: the threads walk
+// the interior in Fortran order in chunks of kSeqChunk cells, each thread
+// loads kSeqPer cells of the chunk, the terms that take part are packed in
+// order into shared memory (warp ballots plus a prefix over the warps), and
+// thread 0 adds them one after another.  A test mode: about 4 cycles per
+// term, so milliseconds per sum at 2 M cells.
+constexpr int kSeqNT = 512, kSeqPer = 8, kSeqChunk = kSeqNT * kSeqPer;
+
+template <int KIND>
+__global__ void __launch_bounds__(kSeqNT, 1) k_seq_sum(Geo g, const float *__restrict__ a0,
+                                                        const float *__restrict__ a1, float pjuge, Scal *s) {
+    __shared__ float ta[kSeqChunk];
+    __shared__ float tb[KIND == 1 ? 1 : kSeqChunk];
+    __shared__ int wcount[kSeqNT / 32];
+    if (KIND == 1 && s->converged) return;
+    const float *__restrict__ src = (KIND == 2 && s->pbuf) ? a1 : a0;
+    const int N = g.im * g.jm * g.km;  // < 2^31: the padded box is (les_ctx_create)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float acc = 0.0f, acc2 = 0.0f;  // thread 0's running sums
+    for (int colour = 0; colour < (KIND == 1 ? 2 : 1); ++colour) {
+        for (int base = 0; base < N; base += kSeqChunk) {
+            float x[kSeqPer], y[kSeqPer];
+            bool take[kSeqPer];
+#pragma unroll
+            for (int q = 0; q < kSeqPer; ++q) {
+                const int t = base + q * kSeqNT + (int)threadIdx.x;
+                take[q] = false;
+                x[q] = 0.0f;
+                y[q] = 0.0f;
+                if (t < N) {
+                    const int r = t / g.im, i = 1 + (t - r * g.im);
+                    const int k = 1 + r / g.jm, j = 1 + (r - (k - 1) * g.jm);
+                    const int c = IX(g, i, j, k);
+                    if (KIND == 1) {
+                        // colour nrd: i = 1 + mod(k+j+nrd, 2), step 2, i.e. i+j+k+nrd odd
+                        take[q] = ((i + j + k + colour) & 1) != 0;
+                        if (take[q]) x[q] = src[c];
+                    } else if (KIND == 0) {
+                        const float w = g.dx1[i] * g.dy1[j] * g.dzn[k];
+                        x[q] = w * src[c];
+                        y[q] = w;
+                        take[q] = true;
+                    } else {
+                        x[q] = src[c] * g.dx1[i] * g.dy1[j] * g.dzn[k];
+                        y[q] = g.dx1[i] * g.dy1[j] * g.dzn[k];
+                        take[q] = true;
+                    }
+                }
+            }
+            int packed = 0;  // terms of this chunk packed so far
+#pragma unroll
+            for (int q = 0; q < kSeqPer; ++q) {
+                const unsigned m = __ballot_sync(0xffffffffu, take[q]);
+                if (lane == 0) wcount[wid] = __popc(m);
+                __syncthreads();
+                int off = packed, total = packed;
+                for (int w = 0; w < kSeqNT / 32; ++w) {
+                    const int cw = wcount[w];
+                    if (w < wid) off += cw;
+                    total += cw;
+                }
+                if (take[q]) {
+                    const int pos = off + __popc(m & ((1u << lane) - 1u));
+                    ta[pos] = x[q];
+                    if (KIND != 1) tb[pos] = y[q];
+                }
+                packed = total;
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                if (KIND == 1) {
+                    for (int t = 0; t < packed; ++t) acc = acc + ta[t];
+                } else {
+                    for (int t = 0; t < packed; ++t) {
+                        acc = acc + ta[t];
+                        acc2 = acc2 + tb[t];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x != 0) return;
+    if (KIND == 0) {
+        s->rhsav = acc / acc2;
+    } else if (KIND == 1) {
+        s->sor = acc;
+        s->sor_iters += 1;
+        if (acc < pjuge) s->converged = 1;
+    } else {
+        s->pav = acc / acc2;
     }
 }
 

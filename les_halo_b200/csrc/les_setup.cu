@@ -13,6 +13,7 @@
 #include "les_abi.h"
 #include "les_halo.cuh"
 #include "les_synth.h"
+#include "les_synth_gen.h"
 
 using namespace les;
 
@@ -126,18 +127,6 @@ les_status halo_common(const float *in, float *out, unsigned im, unsigned jm, un
     return les_internal_ok();
 }
 
-// SplitMix64 (Steele, Lea, Flood 2014).
-struct SplitMix64 {
-    uint64_t s;
-    uint64_t next() {
-        uint64_t z = (s += 0x9e3779b97f4a7c15ull);
-        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-        return z ^ (z >> 31);
-    }
-    double uniform() { return ((next() >> 11) + 0.5) * (1.0 / 9007199254740992.0); }  // (0,1)
-    int irange(int lo, int hi) { return lo + (int)(next() % (uint64_t)(hi - lo + 1)); }
-};
 
 }  // namespace setup_impl
 
@@ -282,80 +271,23 @@ les_status les_halo_unpack_inner(float *a, const float *b, unsigned im, unsigned
 }
 
 // ---------------------------------------------------------------- synthetic
+// (les_synth_gen.h, shared with the CPU oracle)
 void les_synth_default(les_synth_cfg *c, int ip, int jp, int kp, uint64_t seed) {
-    std::memset(c, 0, sizeof *c);
-    c->ip = ip;
-    c->jp = jp;
-    c->kp = kp;
-    c->dx = 4.0f;
-    c->dy = 4.0f;
-    c->dz0 = 2.0f;
-    c->dz_growth = 1.05f;
-    c->plan_area = 0.30f;
-    c->foot_min = 2;
-    c->foot_max = 6;
-    c->h_mean = 20.0f;
-    c->h_sigma_ln = 0.5f;
-    c->h_min = 4.0f;
-    c->h_max = 80.0f;
-    c->ustar = 0.3f;
-    c->z0 = 0.1f;
-    c->kappa = 0.4f;
-    c->noise = 0.02f;
-    c->seed = seed;
+    les_synth_gen::defaults(c, ip, jp, kp, seed);
 }
 
 les_status les_synth_grid(const les_synth_cfg *c, float *dx1, float *dxl, float *dy1, float *dyl, float *z2,
                           float *dzn, float *dzs, float *dxs, float *dys) {
     if (!c || !dx1 || !dy1 || !dzn) return les_internal_fail(LES_ERR_BAD_ARG, "NULL argument");
-    for (int i = -1; i <= c->ip + 1; ++i) dx1[i + 1] = c->dx;
-    for (int j = 0; j <= c->jp + 1; ++j) dy1[j] = c->dy;
-    dzn[1 + 1] = c->dz0;
-    for (int k = 2; k <= c->kp + 1; ++k) dzn[k + 1] = dzn[k] * c->dz_growth;
+    les_synth_gen::base_grid(c, dx1, dy1, dzn);
     return les_grid_metrics(c->ip, c->jp, c->kp, dx1, dxl, dy1, dyl, z2, dzn, dzs, dxs, dys);
 }
 
-float les_synth_terrain(const les_synth_cfg *c, float *zbm) {
-    const int ip = c->ip, jp = c->jp;
-    const size_t ni = ip + 3;
-    std::memset(zbm, 0, sizeof(float) * ni * (jp + 3));
-    auto Z = [&](int i, int j) -> float & { return zbm[(size_t)(i + 1) + ni * (size_t)(j + 1)]; };
-    SplitMix64 rng{c->seed ^ 0x5445525241494eull};
-    const int margin = std::max(2, ip / 16);
-    const long long target = (long long)std::ceil((double)c->plan_area * ip * jp);
-    long long built = 0;
-    const double sig = c->h_sigma_ln, mu = std::log((double)c->h_mean) - 0.5 * sig * sig;
-    const int ilo = 1 + margin, ihi = ip - margin;
-    for (int tries = 0; built < target && tries < 1000000; ++tries) {
-        const int wx = rng.irange(c->foot_min, c->foot_max), wy = rng.irange(c->foot_min, c->foot_max);
-        if (ihi - ilo + 1 < wx) break;
-        const int i0 = rng.irange(ilo, ihi - wx + 1), j0 = rng.irange(1, jp);
-        const double u1 = rng.uniform(), u2 = rng.uniform();
-        const double nrm = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
-        double hgt = std::exp(mu + sig * nrm);
-        hgt = std::min<double>(std::max<double>(hgt, c->h_min), c->h_max);
-        for (int j = j0; j < j0 + wy; ++j)
-            for (int i = i0; i < i0 + wx; ++i) {
-                const int jj = 1 + (j - 1) % jp;  // periodic in j
-                float &z = Z(i, jj);
-                if (z == 0.0f) ++built;
-                z = std::max(z, (float)hgt);
-            }
-    }
-    return (float)((double)built / ((double)ip * jp));
-}
+float les_synth_terrain(const les_synth_cfg *c, float *zbm) { return les_synth_gen::terrain(c, zbm); }
 
 les_status les_synth_inflow(const les_synth_cfg *c, const float *z2, const float *dzn, float *wp) {
     if (!c || !z2 || !dzn || !wp) return les_internal_fail(LES_ERR_BAD_ARG, "NULL argument");
-    SplitMix64 rng{c->seed ^ 0x494e464c4f57ull};
-    for (int k = 1; k <= c->kp; ++k) {
-        const float zc = z2[k - 1] + 0.5f * dzn[k + 1];
-        const double base = ((double)c->ustar / c->kappa) * std::log((double)zc / c->z0);
-        for (int j = 1; j <= c->jp; ++j) {
-            const double xi = (2.0 * rng.uniform() - 1.0) * c->noise;
-            wp[(size_t)(j - 1) + (size_t)c->jp * (k - 1)] = (float)(base * (1.0 + xi));
-        }
-    }
+    les_synth_gen::inflow(c, z2, dzn, wp);
     return les_internal_ok();
 }
 

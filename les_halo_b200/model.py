@@ -184,6 +184,11 @@ class GpuLes:
                                              None if fghold is None else FL.ptr(fghold)))
         return n.value, t.value
 
+    def set_reduction_mode(self, mode: int):
+        """Order of the step's global sums: abi.LES_RED_CANONICAL (exact) or
+        LES_RED_F_* bits for the reference's serial FP32 loops (parity runs)."""
+        abi.check(abi.lib().les_ctx_set_reduction_mode(self.ctx, mode))
+
     def press_refine_fp64(self, outer, inner, rel_tol=0.0):
         abi.check(abi.lib().les_press_refine_fp64(self.ctx, outer, inner, rel_tol))
 

@@ -23,7 +23,9 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liblesoracle.so"
 REF_DIR = HERE / "_ref"
 
-RED_CANONICAL, RED_FAITHFUL = 0, 1
+# Reduction modes (les_oracle.h): a bit mask of the sums taken in the
+# reference's sequential FP32 order; 0 = the exact canonical sums.
+RED_CANONICAL, RED_F_RHSAV, RED_F_SOR, RED_F_PAV, RED_FAITHFUL = 0, 1, 2, 4, 7
 
 _lib = None
 _P = C.c_void_p
@@ -78,6 +80,14 @@ def lib():
         L.oracle_set_press_refine.argtypes = [C.c_int, C.c_int, C.c_double]
         L.oracle_last_refine.argtypes = [C.POINTER(C.c_double)]
         L.oracle_last_refine.restype = C.c_int
+        L.oracle_synth_default.restype = None
+        L.oracle_synth_default.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_uint64]
+        L.oracle_synth_grid.restype = None
+        L.oracle_synth_grid.argtypes = [_P] * 10
+        L.oracle_synth_terrain.restype = C.c_float
+        L.oracle_synth_terrain.argtypes = [_P, _P]
+        L.oracle_synth_inflow.restype = None
+        L.oracle_synth_inflow.argtypes = [_P] * 4
         _lib = L
     return _lib
 
@@ -179,3 +189,49 @@ def last_refine():
     out = (C.c_double * 4)()
     n = lib().oracle_last_refine(out)
     return {"rhsav": out[0], "pav": out[1], "rel_initial": out[2], "rel_final": out[3], "outer": n}
+
+
+def constants():
+    """set.f95:78-82 as the Fortran computes them: ro, vn, alpha, beta."""
+    v = [C.c_float() for _ in range(4)]
+    lib().oracle_constants(*[C.addressof(x) for x in v])
+    return tuple(x.value for x in v)
+
+
+def synthetic_case(ip, jp, kp, seed=1, dt=0.05, inflow="external", nmaxp=50, **cfg_over):
+    """The seeded synthetic case of les_synth.h built on the CPU alone: the
+    same generator source (les_halo_b200/csrc/les_synth_gen.h, compiled
+    into this library), the oracle's grid metrics (grid.f95:55-82), masks
+    and Poisson coefficients (init.f95:82-107, feedbfm.f95:21-63).  Gives
+    the arrays of les_halo_b200.synthetic_case bit for bit, without loading
+    liblesb200.so; state zeroed as init.f95:46-69 leaves it."""
+    from les_halo_b200 import abi as A, fields as FL
+    from les_halo_b200.model import LesCase
+    L = lib()
+    cfg = A.LesSynthCfg()
+    L.oracle_synth_default(C.addressof(cfg), ip, jp, kp, seed)
+    for k, v in cfg_over.items():
+        setattr(cfg, k, v)
+    p = A.LesParams()
+    p.ip, p.jp, p.kp = ip, jp, kp
+    p.dt = dt
+    p.ro, p.vn, p.alpha, p.beta = constants()
+    p.cs0, p.nmaxp, p.pjuge, p.omega = 0.1, nmaxp, 0.0001, 1.0
+    p.inflow_mode = A.LES_INFLOW_EXTERNAL if inflow == "external" else A.LES_INFLOW_POWER_LAW
+    p.ical = 0
+    case = LesCase(ip, jp, kp, p)
+    arr = case.arrays
+    for n in FL.METRICS:
+        arr[n] = FL.alloc(n, ip, jp, kp)
+    L.oracle_synth_grid(C.addressof(cfg), *[ptr(arr[n]) for n in
+                                            ("dx1", "dxl", "dy1", "dyl", "z2", "dzn", "dzs", "dxs", "dys")])
+    zbm = FL.alloc("zbm", ip, jp, kp)
+    case.built_fraction = float(L.oracle_synth_terrain(C.addressof(cfg), ptr(zbm)))
+    arr["zbm"] = zbm
+    if inflow == "external":
+        arr["wind_profile"] = FL.alloc("wind_profile", ip, jp, kp)
+        L.oracle_synth_inflow(C.addressof(cfg), ptr(arr["z2"]), ptr(arr["dzn"]), ptr(arr["wind_profile"]))
+    for n in FL.STATE + FL.MASKS + FL.POISSON + ["delx1"]:
+        arr[n] = FL.alloc(n, ip, jp, kp)
+    masks_and_poisson(case, zbm)
+    return case

@@ -1330,7 +1330,9 @@ int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const 
     A1 dx1 = mk1(dx1_, -1), dy1 = mk1(dy1_, 0), dzn = mk1(dzn_, -1);
     A1 cn2l = mk1(cn2l_, 1), cn2s = mk1(cn2s_, 1), cn3l = mk1(cn3l_, 1), cn3s = mk1(cn3s_, 1),
        cn4l = mk1(cn4l_, 1), cn4s = mk1(cn4s_, 1);
-    const bool canon = (g_red_mode == ORACLE_RED_CANONICAL);
+    const bool canon = !(g_red_mode & ORACLE_RED_F_RHSAV);      // rhsav and area
+    const bool canon_sor = !(g_red_mode & ORACLE_RED_F_SOR);    // SOR residual
+    const bool canon_pav = !(g_red_mode & ORACLE_RED_F_PAV);    // pav and pco
 
     oracle_bondfg(km, jm, f_, im, g_, h_);
 #pragma omp parallel for schedule(static)
@@ -1406,13 +1408,13 @@ int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const 
             for (int k = 1; k <= km; ++k)
                 for (int j = 1; j <= jm; ++j)
                     for (int i = 1 + (k + j + nrd) % 2; i <= im; i += 2) {
-                        if (canon) sfix.add(rr(i, j, k));
+                        if (canon_sor) sfix.add(rr(i, j, k));
                         else sor32 = sor32 + rr(i, j, k);
                     }
             oracle_boundp1(km, jm, p_, im);
         }
         oracle_boundp2(jm, im, p_, km);
-        sor = canon ? (float)sfix.value() : sor32;
+        sor = canon_sor ? (float)sfix.value() : sor32;
         if (sor < pjuge) break;
     }
 
@@ -1425,7 +1427,7 @@ int oracle_press_ex(int km, int jm, int im, float *rhs_, const float *u_, const 
         return l_exec;
     }
     float pav;
-    if (canon) {
+    if (canon_pav) {
         const double num = canonical_sum3(
             im, jm, km, [&](int i, int j, int k) { return p(i, j, k) * dx1(i) * dy1(j) * dzn(k); });
         const double den =

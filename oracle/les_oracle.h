@@ -18,7 +18,12 @@
  *       are summed exactly in 128 bits, then finished in FP64.  The sum does
  *       not depend on order, and the CUDA path uses the same definition, so
  *       parity is bit-exact whatever reduction tree the kernels use.
- *   ORACLE_RED_FAITHFUL: the reference's sequential FP32 sums.
+ *   ORACLE_RED_FAITHFUL: the reference's sequential FP32 sums, in the
+ *       Fortran loop order (press.f95:66-75 rhsav and area, 91-99 the SOR
+ *       residual colour by colour, 127-133 pav and pco).
+ * The mode is a bit mask: ORACLE_RED_F_RHSAV, ORACLE_RED_F_SOR and
+ * ORACLE_RED_F_PAV make one sum faithful each (FAITHFUL = all three), so
+ * the effect of each sum on the fields can be measured on its own.
  * Parity status: halo pack/unpack is pinned against the reference's own C
  * programs (src/OpenCL/test_halo_*.c); the physics fields are "parity
  * unpinned" because the reference ships no stored field values and no Fortran
@@ -30,7 +35,13 @@
 extern "C" {
 #endif
 
-enum { ORACLE_RED_CANONICAL = 0, ORACLE_RED_FAITHFUL = 1 };
+enum {
+    ORACLE_RED_CANONICAL = 0,
+    ORACLE_RED_F_RHSAV = 1,
+    ORACLE_RED_F_SOR = 2,
+    ORACLE_RED_F_PAV = 4,
+    ORACLE_RED_FAITHFUL = 7
+};
 
 void oracle_set_reduction_mode(int mode);
 int oracle_get_reduction_mode(void);

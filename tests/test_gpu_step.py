@@ -81,6 +81,30 @@ def test_benchmark_case_200_steps(require_gpu):
     gpu.close()
 
 
+@pytest.mark.slow
+def test_benchmarked_configuration_bitexact(require_gpu):
+    # the configuration the throughput is measured on: 600 x 600 x 120, 35%
+    # plan area, heights to 120 m (bench.py's workload), warm-up and three
+    # steps, the first with the n == 1 inflow broadcast.  Exercises the SOR
+    # pass shape the autotuner picks at this size on real tile counts and
+    # the interior/edge mix of the 1425 momentum tiles.
+    ip, jp, kp = 600, 600, 120
+    ref, dev = _pair(ip, jp, kp, seed=1, plan_area=0.35, h_max=120.0)
+    gpu = GpuLes(dev)
+    oracle.ifdata(ref, 1)
+    gpu.warmup(1)
+    _compare(gpu, ref, FL.STATE)
+    for n in range(1, 4):
+        iters = oracle.run_steps(ref, n, 1)
+        gpu.step(n, 1)
+        assert gpu.metrics()["sor_iters"] == iters[0] == 50
+        T, ty, tx, nch = _sor_shape(gpu)
+        print(f"step {n}: SOR pass shape T={T} rows={ty} cols={tx} k-chunks={nch}")
+        assert T >= 1
+        _compare(gpu, ref, FL.STATE)
+    gpu.close()
+
+
 def test_power_law_inflow(require_gpu):
     ip, jp, kp = 12, 10, 80
     ref, dev = _pair(ip, jp, kp, seed=3, inflow="power")

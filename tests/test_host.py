@@ -105,3 +105,21 @@ def test_field_bounds_table():
     assert FL.bounds("w", 10, 8, 6) == [(0, 11), (-1, 9), (-1, 7)]
     assert FL.bounds("diu1", 10, 8, 6) == [(-1, 12), (0, 10), (0, 8)]
     assert FL.alloc("sm", 10, 8, 6).shape == (13, 11, 8)
+
+
+@pytest.mark.parametrize("dims,over", [((48, 40, 30), {}), ((60, 44, 20), {"plan_area": 0.35, "h_max": 120.0}),
+                                       ((32, 24, 80), {"dx": 3.0, "dy": 5.0})])
+def test_oracle_builds_the_library_case(dims, over):
+    # CPU-only runs (bench.py's reference arm and CPU baseline) build their
+    # cases with the oracle alone; they must be the library's cases bit for
+    # bit, parameters included
+    from les_halo_b200 import synthetic_case
+    ip, jp, kp = dims
+    a = oracle.synthetic_case(ip, jp, kp, seed=3, **over)
+    b = synthetic_case(ip, jp, kp, seed=3, masks_and_poisson=oracle.masks_and_poisson, **over)
+    assert sorted(a.arrays) == sorted(b.arrays)
+    for n in a.arrays:
+        assert np.array_equal(a.arrays[n].view(np.uint32), b.arrays[n].view(np.uint32)), n
+    for f, _ in abi.LesParams._fields_:
+        assert np.float32(getattr(a.params, f)) == np.float32(getattr(b.params, f)), f
+    assert a.built_fraction == b.built_fraction
