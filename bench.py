@@ -334,6 +334,69 @@ def ensemble_bench(steps, warmup, ws=1, rank=0, dist=None):
     return out
 
 
+ADJOINT = dict(ip=150, jp=150, kp=90, steps=100, ckpt=10, box=((66, 85), (66, 85), (1, 5)), seed=1)
+
+
+def adjoint_bench():
+    """The adjoint configuration: the 150 x 150 x 90 benchmark terrain from
+    its warm-up, 100 steps (all 50 SOR iterations each) with the time-mean
+    resolved TKE of a 20 x 20 x 5-cell pedestrian box as the objective, and
+    its gradient with respect to the inflow profile, the per-column drag
+    scale and the initial state by the device step adjoint with a checkpoint
+    every 10 steps (each segment recomputed).  Cost ratio = wall time of the
+    gradient (forward with checkpoints, recomputation and adjoint) over the
+    forward alone (the same 100 steps with the objective evaluated)."""
+    import les_halo_b200 as lh
+    A = ADJOINT
+    case = lh.synthetic_case(A["ip"], A["jp"], A["kp"], seed=A["seed"], dt=0.05, nmaxp=50)
+    case.params.pjuge = -1.0
+    gpu = lh.GpuLes(case)
+    gpu.warmup(1)
+    lh.set_drag(gpu, np.ones((A["ip"], A["jp"]), np.float32))
+    nt, ckpt, box = A["steps"], A["ckpt"], A["box"]
+    adj = lh.GpuAdjoint(gpu, -(-nt // ckpt) + ckpt + 1, 50)
+    try:
+        init = adj.nslots - 1
+        adj.save(init)
+        gpu.step(1, 2)  # capture the step graphs, autotune
+        gpu.sync()
+
+        def forward():
+            adj.load(init)
+            J = 0.0
+            for t in range(nt):
+                gpu.step(1 + t, 1)
+                J += adj.tke(-1, box) / nt
+            gpu.sync()
+            return J
+
+        forward()
+        t0 = time.perf_counter()
+        J = forward()
+        fwd_s = time.perf_counter() - t0
+        adj.load(init)
+        lh.tke_gradient(gpu, adj, 1, nt, box, ckpt)  # warm
+        adj.load(init)
+        gpu.sync()
+        t0 = time.perf_counter()
+        Jg, g = lh.tke_gradient(gpu, adj, 1, nt, box, ckpt)
+        gpu.sync()
+        grad_s = time.perf_counter() - t0
+        return {"config": f"{A['ip']}x{A['jp']}x{A['kp']}, {nt} steps (SOR 50 each), checkpoint every {ckpt}, "
+                          f"J = time-mean resolved TKE of box i{box[0]} j{box[1]} k{box[2]}; gradients: inflow "
+                          "profile (jp x kp), drag scale (ip x jp), initial state",
+                "J": J, "J_in_gradient_run": Jg, "forward_s": round(fwd_s, 4), "gradient_s": round(grad_s, 4),
+                "cost_ratio": round(grad_s / fwd_s, 3),
+                "adjoint_over_forward": round((grad_s - fwd_s) / fwd_s, 3),
+                "grad_wp_norm": float(np.linalg.norm(g["wp"])), "grad_drag_norm": float(np.linalg.norm(g["drag"])),
+                "precision": "FP32 fields and adjoint, FP64 objective and parameter-gradient sums"}
+    except Exception as exc:
+        return {"error": f"{type(exc).__name__}: {exc}"[:300]}
+    finally:
+        adj.close()
+        gpu.close()
+
+
 def run_ours(args):
     import torch
     ws, rank, local = _dist()
@@ -526,6 +589,8 @@ def run_ours(args):
         }
         if ens_line is not None:
             line["ensemble"] = ens_line
+        if not args.profile and not args.no_adjoint and ws == 1:
+            line["adjoint"] = adjoint_bench()
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
@@ -546,6 +611,8 @@ def main():
                     help="skip the FP64-refined press measurement")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 64-domain ensemble measurement")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint (config-3) cost measurement")
     ap.add_argument("--profile", action="store_true",
                     help="no in-graph timing events (for runs under ncu)")
     ap.add_argument("--grid", default=None,

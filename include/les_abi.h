@@ -558,6 +558,53 @@ void *les_ensemble_stream(les_ensemble *ens);
 uint64_t les_ensemble_launch_count(les_ensemble *ens);
 les_status les_ensemble_destroy(les_ensemble *ens);
 
+/* ---- Adjoint of whole time steps (no counterpart in the reference) --------
+ * The discrete adjoint of the step run by les_step (velnw, bondv1 with the
+ * external inflow profile, velfg, feedbf, les, adam, press with a fixed SOR
+ * iteration count), in FP32 with FP64 parameter gradients, on the device
+ * state of a context created with LES_INFLOW_EXTERNAL.  The caller drives
+ * checkpointing and recomputation: state slots hold copies of the
+ * context's state (u v w p usum vsum wsum f g h fold gold hold rhs sm), and
+ * les_adj_step_b applies the adjoint of step n whose input state is in a
+ * slot to the adjoint state the handle holds, recomputing the forward
+ * values it needs (the velocities after velnw and after bondv1, vel2's diu,
+ * les's sm, feedbf's force) from that slot.  Parameter gradients
+ * accumulate: the inflow profile wind_profile(1:jp,1:kp) (held fixed over
+ * the steps) and, with les_ctx_set_drag, the per-column force scale.
+ *
+ * les_ctx_set_drag: f += s(i,j) * fx in feedbf (and g, h alike) for the
+ *   following steps (drag(1:ip,1:jp), host; NULL: s = 1, the reference).
+ * les_adj_create: nslots state slots; niter is the SOR iteration count
+ *   every differentiated step executes (run the forward with nmaxp = niter
+ *   and a pjuge it never reaches, e.g. -1).  Call after les_ctx_upload;
+ *   the grid tables must not change afterwards.
+ * les_adj_save / les_adj_load: context state to / from a slot.
+ * les_adj_zero: adjoint state and parameter gradients to zero.
+ * les_adj_tke: J = mean over the cells of box {i0,i1,j0,j1,k0,k1}
+ *   (inclusive, interior indices) of 0.5 (uc^2 + vc^2 + wc^2) with the
+ *   cell-centred velocities of anime.f95:45-47, of a slot (-1: the
+ *   context's state), in FP64.
+ * les_adj_seed_tke: adjoint of u, v, w += scale * dJ/d(u, v, w) at a slot
+ *   (-1: the context's state).
+ * les_adj_step_b: the adjoint of step n (input state in slot); afterwards
+ *   the adjoint state is that of the step's input.
+ * les_adj_read: parameter gradients (FP64: wind_profile jp*kp, drag ip*jp)
+ *   and the adjoint state (Fortran layouts); NULL pointers are skipped.
+ * les_adj_write: set the adjoint state from host arrays (Fortran layouts;
+ *   NULL: that array's adjoint is zero). */
+typedef struct les_adj les_adj;
+les_status les_ctx_set_drag(les_ctx *ctx, const float *drag);
+les_status les_adj_create(les_ctx *ctx, int nslots, int niter, les_adj **out);
+les_status les_adj_destroy(les_adj *adj);
+les_status les_adj_save(les_adj *adj, int slot);
+les_status les_adj_load(les_adj *adj, int slot);
+les_status les_adj_zero(les_adj *adj);
+les_status les_adj_tke(les_adj *adj, int slot, const int *box, double *J);
+les_status les_adj_seed_tke(les_adj *adj, int slot, const int *box, double scale);
+les_status les_adj_step_b(les_adj *adj, int n, int slot);
+les_status les_adj_read(les_adj *adj, double *wind_profile_b, double *drag_b, les_host_fields *state_b);
+les_status les_adj_write(les_adj *adj, const les_host_fields *state_b);
+
 #ifdef __cplusplus
 }
 #endif

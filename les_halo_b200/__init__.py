@@ -6,6 +6,8 @@ reference's driver: Fortran-layout arrays, the synthetic benchmark inputs,
 and ``GpuLes`` (initialise_LES_kernel / run_LES_kernel).
 """
 from . import abi, fields
-from .model import Ensemble, GpuLes, LesCase, default_params, synth_cfg, synthetic_case
+from .model import (Ensemble, GpuAdjoint, GpuLes, LesCase, default_params, set_drag, synth_cfg,
+                    synthetic_case, tke_forward, tke_gradient, tke_reverse)
 
-__all__ = ["abi", "fields", "Ensemble", "GpuLes", "LesCase", "default_params", "synth_cfg", "synthetic_case"]
+__all__ = ["abi", "fields", "Ensemble", "GpuAdjoint", "GpuLes", "LesCase", "default_params", "set_drag", "synth_cfg",
+           "synthetic_case", "tke_forward", "tke_gradient", "tke_reverse"]

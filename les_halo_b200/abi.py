@@ -139,6 +139,17 @@ _SIGS = {
     "les_netcdf_write_host": (C.c_int, [_P, C.c_int] + [_P] * 7),
     "les_netcdf_close": (C.c_int, [_P]),
     "les_last_refine_metrics": (C.c_int, [_P, C.POINTER(LesRefineMetrics)]),
+    "les_ctx_set_drag": (C.c_int, [_P, _P]),
+    "les_adj_create": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "les_adj_destroy": (C.c_int, [_P]),
+    "les_adj_save": (C.c_int, [_P, C.c_int]),
+    "les_adj_load": (C.c_int, [_P, C.c_int]),
+    "les_adj_zero": (C.c_int, [_P]),
+    "les_adj_tke": (C.c_int, [_P, C.c_int, _P, C.POINTER(C.c_double)]),
+    "les_adj_seed_tke": (C.c_int, [_P, C.c_int, _P, C.c_double]),
+    "les_adj_step_b": (C.c_int, [_P, C.c_int, C.c_int]),
+    "les_adj_read": (C.c_int, [_P, _P, _P, C.POINTER(LesHostFields)]),
+    "les_adj_write": (C.c_int, [_P, C.POINTER(LesHostFields)]),
 }
 
 # Per-routine entries: every argument is a pointer (Fortran by-reference).

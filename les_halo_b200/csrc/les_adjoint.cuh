@@ -260,15 +260,18 @@ __global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_velnw(Geo g, const float
 // feedbf.f95:38-67 transposed, per interior cell and component:
 //   usum' = (usum + u) m;  fx = (alpha usum') dt + (beta u) m;  f' = f + fx.
 // f keeps its adjoint; fx's is spent (fx is overwritten); usum and u gather.
+// With a force scale s (drag, f' = f + s fx) fx's adjoint is s times f's.
 __global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_feedbf(Geo g, Fields F, float *fxb, float *fyb, float *fzb,
-                                                               float alpha, float dt, float beta) {
+                                                               float alpha, float dt, float beta,
+                                                               const float *drag = nullptr) {
     const int i = 1 + blockIdx.x * kAdjBX + threadIdx.x, j = 1 + blockIdx.y * kAdjBY + threadIdx.y;
     const int k = 1 + blockIdx.z;
     if (i > g.im || j > g.jm) return;
     const int c = IX(g, i, j, k);
+    const float s = drag ? drag[(i - 1) + g.im * (j - 1)] : 1.0f;
     auto comp = [&](float *sumb, float *vb, const float *mask, float *xb, const float *fb) {
         const float m = mask[c];
-        const float t = xb[c] + fb[c];
+        const float t = xb[c] + (drag ? s * fb[c] : fb[c]);
         const float sb = sumb[c] + (alpha * dt) * t;
         vb[c] += (beta * m) * t + m * sb;
         sumb[c] = m * sb;

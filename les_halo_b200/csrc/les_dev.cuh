@@ -34,6 +34,9 @@ struct Geo {
     // 0 where kdiv must divide
     const float *rdzn, *rdzs, *rdzn2;
     float dt, ro, vn, alpha, beta, omega;
+    // per-column scale s(i,j) of the IBM force, f += s*fx in feedbf
+    // (drag[(i-1) + im*(j-1)]); NULL is the reference's s = 1
+    const float *drag;
 };
 
 // a/d with d's exact reciprocal r when d is a power of two (r != 0).

@@ -18,11 +18,13 @@
 
 #include "les_abi.h"
 #include "les_adjoint.cuh"
+#include "les_adjstep.cuh"
 #include "les_halo.cuh"
 #include "les_mom.cuh"
 #include "les_press.cuh"
 #include "les_routines.cuh"
 #include "les_sor_tb.cuh"
+#include "les_sor1.cuh"
 #include "les_stats.cuh"
 #include "les_refine.cuh"
 #include "les_spectral.cuh"
@@ -213,6 +215,7 @@ struct les_ctx {
     // rhsav, the SOR residual or pav in the reference's sequential FP32 order
     int red_mode = LES_RED_CANONICAL;
     float *d_r2 = nullptr;                // reltmp^2 per cell (box), LES_RED_F_SOR only
+    float *d_drag = nullptr;              // per-column IBM force scale (les_ctx_set_drag)
 };
 
 // Buffers of an SOR pass other than the context's p / second p / rhs / scalars.
@@ -616,8 +619,8 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     const Geo &g = c->geo;
 #define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a, c->kq)
     switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
-        case 2: TBL(1, false); break;
-        case 3: TBL(1, true); break;
+        case 2: LAUNCH_SMEM(c, k_sor1<false>, grid, block, s1_smem(sh.ty), g, a, c->kq); break;
+        case 3: LAUNCH_SMEM(c, k_sor1<true>, grid, block, s1_smem(sh.ty), g, a, c->kq); break;
         case 4: TBL(2, false); break;
         case 5: TBL(2, true); break;
         case 6: TBL(3, false); break;
@@ -644,8 +647,18 @@ les_status set_tb_smem_attrs() {
         CK(cudaFuncSetAttribute(k_sor_tb<TT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
         lim = std::min(lim, mx);                                                                   \
     }
-    TBA(1, false) TBA(1, true) TBA(2, false) TBA(2, true) TBA(3, false) TBA(3, true)
+    TBA(2, false) TBA(2, true) TBA(3, false) TBA(3, true)
 #undef TBA
+#define S1A(KT)                                                                                \
+    {                                                                                          \
+        cudaFuncAttributes fa;                                                                 \
+        CK(cudaFuncGetAttributes(&fa, k_sor1<KT>));                                            \
+        const int mx = optin - (int)fa.sharedSizeBytes;                                        \
+        CK(cudaFuncSetAttribute(k_sor1<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+        lim = std::min(lim, mx);                                                               \
+    }
+    S1A(false) S1A(true)
+#undef S1A
     g_tb_dyn_max = lim;
     return LES_OK;
 }
@@ -664,7 +677,7 @@ std::mutex g_tune_mu;
 // memory and the partial-sum array.
 bool tb_shape_ok(const les_ctx *c, const TbShape &sh) {
     if (!tb_fits(sh.T, sh.ty) || sh.nch < 1 || sh.nch > kTbMaxChunks) return false;
-    if (tb_smem(sh.T, sh.ty) > (size_t)g_tb_dyn_max) return false;
+    if ((sh.T == 1 ? s1_smem(sh.ty) : tb_smem(sh.T, sh.ty)) > (size_t)g_tb_dyn_max) return false;
     const int kc = cdiv(c->prm.kp, sh.nch);
     const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(sh.T)) * cdiv(c->prm.jp, sh.ty) * cdiv(c->prm.kp, kc);
     return nblk * kTbTMax <= c->npart;
@@ -940,6 +953,7 @@ les_status les_ctx_destroy(les_ctx *c) {
     cudaFree(c->d_dpart);
     cudaFree(c->d_refw);
     cudaFree(c->d_r2);
+    cudaFree(c->d_drag);
     spec_release(c->spec);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1393,3 +1407,4 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 #include "les_ensemble.inc"
 #include "les_refine.inc"
 #include "les_adjoint.inc"
+#include "les_adjstep.inc"

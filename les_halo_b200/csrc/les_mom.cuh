@@ -602,9 +602,16 @@ __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
         F.wsum[c] = ws;
         float f1x = g.alpha * us * g.dt, f1y = g.alpha * vs * g.dt, f1z = g.alpha * ws * g.dt;
         float f2x = g.beta * u0 * bm0, f2y = g.beta * v0 * cm0, f2z = g.beta * w0 * dm0;
-        F.f[c] = fv + (f1x + f2x);
-        F.g[c] = gv + (f1y + f2y);
-        F.h[c] = hv + (f1z + f2z);
+        if (g.drag) {  // the adjoint's per-column force scale (s = 1: the reference)
+            const float s = g.drag[(i - 1) + g.im * (j - 1)];
+            F.f[c] = fv + s * (f1x + f2x);
+            F.g[c] = gv + s * (f1y + f2y);
+            F.h[c] = hv + s * (f1z + f2z);
+        } else {
+            F.f[c] = fv + (f1x + f2x);
+            F.g[c] = gv + (f1y + f2y);
+            F.h[c] = hv + (f1z + f2z);
+        }
         F.sm[c] = sgs_sm(g, t, i, j, k);
     };
     if (tile_interior(g))

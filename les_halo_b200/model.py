@@ -212,6 +212,126 @@ class GpuLes:
         return d.value, ox.value, si.value, sj.value, sk.value
 
 
+class GpuAdjoint:
+    """Adjoint of whole time steps of a GpuLes (les_adj_* of les_abi.h):
+    state slots for checkpoints and recomputation, the step adjoint, the
+    resolved-TKE objective and its seed, and the accumulated gradients."""
+
+    def __init__(self, gpu: GpuLes, nslots: int, niter: int):
+        self.gpu = gpu
+        self.h = C.c_void_p()
+        abi.check(abi.lib().les_adj_create(gpu.ctx, nslots, niter, C.byref(self.h)))
+        self.nslots = nslots
+
+    def close(self):
+        if self.h:
+            abi.lib().les_adj_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def save(self, slot):
+        abi.check(abi.lib().les_adj_save(self.h, slot))
+
+    def load(self, slot):
+        abi.check(abi.lib().les_adj_load(self.h, slot))
+
+    def zero(self):
+        abi.check(abi.lib().les_adj_zero(self.h))
+
+    @staticmethod
+    def _box(box):
+        (i0, i1), (j0, j1), (k0, k1) = box
+        return (C.c_int * 6)(i0, i1, j0, j1, k0, k1)
+
+    def tke(self, slot, box) -> float:
+        J = C.c_double()
+        abi.check(abi.lib().les_adj_tke(self.h, slot, self._box(box), C.byref(J)))
+        return J.value
+
+    def seed_tke(self, slot, box, scale):
+        abi.check(abi.lib().les_adj_seed_tke(self.h, slot, self._box(box), scale))
+
+    def step_b(self, n, slot):
+        abi.check(abi.lib().les_adj_step_b(self.h, n, slot))
+
+    def read(self, state=False):
+        c = self.gpu.case
+        wp = np.zeros((c.jp, c.kp), np.float64, order="F")
+        drag = np.zeros((c.ip, c.jp), np.float64, order="F")
+        out = {}
+        hf = None
+        if state:
+            out = {n: FL.alloc(n, c.ip, c.jp, c.kp) for n in FL.STATE}
+            hf = abi.LesHostFields()
+            for n in FL.STATE:
+                setattr(hf, n, FL.ptr(out[n]))
+        abi.check(abi.lib().les_adj_read(self.h, wp.ctypes.data, drag.ctypes.data,
+                                         C.byref(hf) if hf is not None else None))
+        return {"wp": wp, "drag": drag, "state": out}
+
+    def write(self, state_b: dict):
+        hf = abi.LesHostFields()
+        keep = {n: np.asfortranarray(state_b[n], dtype=np.float32) for n in FL.STATE if n in state_b}
+        for n, a in keep.items():
+            setattr(hf, n, FL.ptr(a))
+        abi.check(abi.lib().les_adj_write(self.h, C.byref(hf)))
+
+
+def set_drag(gpu: GpuLes, drag):
+    """Per-column scale s(i, j) of feedbf's force (f += s fx) for the next
+    steps; None restores the reference's s = 1."""
+    d = None if drag is None else np.asfortranarray(drag, dtype=np.float32)
+    abi.check(abi.lib().les_ctx_set_drag(gpu.ctx, FL.ptr(d) if d is not None else None))
+
+
+def tke_forward(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int) -> float:
+    """J = (1/nt) sum over steps n0 .. n0+nt-1 of the resolved TKE of box
+    after the step, from the context's current state, keeping a checkpoint
+    every ckpt steps in slots 0, 1, .. (slot 0: the initial state)."""
+    adj.save(0)
+    J = 0.0
+    for t in range(nt):
+        gpu.step(n0 + t, 1)
+        J += adj.tke(-1, box) / nt
+        if (t + 1) % ckpt == 0 and t + 1 < nt:
+            adj.save((t + 1) // ckpt)
+    return J
+
+
+def tke_reverse(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int) -> dict:
+    """The gradient of tke_forward's J (same arguments, run just before):
+    the step adjoint backwards over the checkpoints, each segment's step
+    inputs recomputed from its checkpoint into slots ceil(nt/ckpt) ...  The
+    context is left at the end of the first segment.  Returns the FP64
+    gradients of the inflow profile ("wp", jp x kp) and the drag scale
+    ("drag", ip x jp; zero unless set) and the adjoint of the initial state."""
+    nck = -(-nt // ckpt)
+    assert adj.nslots >= nck + ckpt, "too few slots"
+    adj.zero()
+    for seg in reversed(range(nck)):
+        t0, t1 = seg * ckpt, min(seg * ckpt + ckpt, nt)
+        adj.load(seg)
+        for t in range(t0, t1):
+            adj.save(nck + t - t0)
+            gpu.step(n0 + t, 1)
+        for t in reversed(range(t0, t1)):
+            adj.seed_tke(-1 if t == t1 - 1 else nck + t + 1 - t0, box, 1.0 / nt)
+            adj.step_b(n0 + t, nck + t - t0)
+    return adj.read(state=True)
+
+
+def tke_gradient(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int):
+    """tke_forward then tke_reverse: (J, gradients).  Needs ceil(nt/ckpt) +
+    ckpt slots."""
+    J = tke_forward(gpu, adj, n0, nt, box, ckpt)
+    return J, tke_reverse(gpu, adj, n0, nt, box, ckpt)
+
+
 class Ensemble:
     """Independent domains (GpuLes members) advanced by one graph launch per step."""
 

@@ -48,3 +48,30 @@ def tke_torch(ip, jp, kp, state, box):
     vc = 0.5 * (view("v", I, sh(J), K) + view("v", I, J, K))
     wc = 0.5 * (view("w", I, J, sh(K)) + view("w", I, J, K))
     return torch.mean(0.5 * (uc * uc + vc * vc + wc * wc))
+
+
+class TkeObjective(torch.autograd.Function):
+    """The config-3 objective on the GPU through the C ABI: J(wp, drag) =
+    time-mean resolved TKE of a box over nt steps from the state in slot
+    `init` of a GpuAdjoint.  forward runs the CUDA steps keeping a checkpoint
+    every ckpt steps (les_halo_b200.tke_forward); backward runs the device
+    step adjoint over the checkpoints with recomputation
+    (les_halo_b200.tke_reverse) and returns the gradients of the inflow
+    profile wp(jp, kp) and the drag scale s(ip, jp)."""
+
+    @staticmethod
+    def forward(ctx, wp, drag, gpu, adj, init, n0, nt, box, ckpt):
+        import les_halo_b200 as lh
+        adj.load(init)
+        gpu.set_wind_profile(np.asfortranarray(wp.detach().numpy(), dtype=np.float32))
+        lh.set_drag(gpu, drag.detach().numpy())
+        J = lh.tke_forward(gpu, adj, n0, nt, box, ckpt)
+        ctx.args = (gpu, adj, n0, nt, box, ckpt)
+        return torch.tensor(J, dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx, gJ):
+        import les_halo_b200 as lh
+        g = lh.tke_reverse(*ctx.args)
+        return (gJ * torch.from_numpy(g["wp"]), gJ * torch.from_numpy(g["drag"]),
+                None, None, None, None, None, None, None)
