@@ -166,7 +166,9 @@ def test_config3_gradient_against_central_differences(require_gpu):
     # profile and the drag scale moved by a relative h) in 16 seeded
     # directions.  Here the differences are the less exact side: the FP32
     # forward's rounding, carried through 100 steps of the flow, is a part in
-    # 1e6 to 1e7 of J, against a change of J of about a part in 1e3.
+    # 1e6 to 1e7 of J, against a change of J of about a part in 1e3, so a
+    # direction whose derivative is small can show a relative error of a few
+    # 1e-4 while the typical one agrees to about 1e-5.
     ip, jp, kp, nt, ckpt = 150, 150, 90, 100, 10
     box = ((66, 85), (66, 85), (1, 5))
     case = synthetic_case(ip, jp, kp, seed=1, masks_and_poisson=oracle.masks_and_poisson)
@@ -206,7 +208,8 @@ def test_config3_gradient_against_central_differences(require_gpu):
         errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
     print("config-3 adjoint vs central differences of the FP32 forward, relative errors:",
           " ".join(f"{e:.1e}" for e in errs))
-    assert float(np.median(errs)) <= 1e-2, errs
+    assert max(errs) <= 1e-3, errs
+    assert float(np.median(errs)) <= 1e-4, errs
     adj.close()
     gpu.close()
 
