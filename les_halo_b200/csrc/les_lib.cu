@@ -520,7 +520,7 @@ les_status enqueue_press(les_ctx *c, bool exact) {
         // exact sums (at most once per step): one more pass, which returns
         // at once when all nmaxp iterations are done or the SOR stopped
         if (nmaxp >= 2 && tb_fast_ok(c, c->tb)) {
-            les_status st = launch_sor_tb(c, c->tb, 1, 0, c->prm.pjuge, nmaxp);
+            les_status st = launch_sor_tb(c, c->tb, c->tb.T, 0, c->prm.pjuge, nmaxp);
             if (st != LES_OK) return st;
         }
     }
@@ -579,7 +579,7 @@ les_status check_params(const les_params *p) {
 // strided pass over the block partials), a threshold below 2^40, and
 // LES_SOR_SUMS not set to "exact".
 bool tb_fast_ok(const les_ctx *c, const TbShape &sh) {
-    if (sh.T != 1 || !c->sor_fp32_test || !(c->prm.pjuge < 0x1p40f)) return false;
+    if (sh.T > 2 || !c->sor_fp32_test || !(c->prm.pjuge < 0x1p40f)) return false;
     const int kc = cdiv(c->prm.kp, sh.nch), nt = 32 * tb_warps(sh.T, sh.ty);
     const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(sh.T)) * cdiv(c->prm.jp, sh.ty) * cdiv(c->prm.kp, kc);
     const long long depth = 4LL * kc + 2 * (5 + nt / 32) + (nblk + nt - 1) / nt;
@@ -621,8 +621,8 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
         case 2: LAUNCH_SMEM(c, k_sor1<false>, grid, block, s1_smem(sh.ty), g, a, c->kq); break;
         case 3: LAUNCH_SMEM(c, k_sor1<true>, grid, block, s1_smem(sh.ty), g, a, c->kq); break;
-        case 4: TBL(2, false); break;
-        case 5: TBL(2, true); break;
+        case 4: LAUNCH_SMEM(c, k_sor2<false>, grid, block, s2_smem(sh.ty), g, a, c->kq); break;
+        case 5: LAUNCH_SMEM(c, k_sor2<true>, grid, block, s2_smem(sh.ty), g, a, c->kq); break;
         case 6: TBL(3, false); break;
         case 7: TBL(3, true); break;
         default: return fail(LES_ERR_BAD_ARG, "SOR pass shape %d,%d", sh.T, sh.ty);
@@ -647,7 +647,7 @@ les_status set_tb_smem_attrs() {
         CK(cudaFuncSetAttribute(k_sor_tb<TT, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
         lim = std::min(lim, mx);                                                                   \
     }
-    TBA(2, false) TBA(2, true) TBA(3, false) TBA(3, true)
+    TBA(3, false) TBA(3, true)
 #undef TBA
 #define S1A(KT)                                                                                \
     {                                                                                          \
@@ -659,6 +659,16 @@ les_status set_tb_smem_attrs() {
     }
     S1A(false) S1A(true)
 #undef S1A
+#define S2A(KT)                                                                                \
+    {                                                                                          \
+        cudaFuncAttributes fa;                                                                 \
+        CK(cudaFuncGetAttributes(&fa, k_sor2<KT>));                                            \
+        const int mx = optin - (int)fa.sharedSizeBytes;                                        \
+        CK(cudaFuncSetAttribute(k_sor2<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+        lim = std::min(lim, mx);                                                               \
+    }
+    S2A(false) S2A(true)
+#undef S2A
     g_tb_dyn_max = lim;
     return LES_OK;
 }
@@ -677,7 +687,8 @@ std::mutex g_tune_mu;
 // memory and the partial-sum array.
 bool tb_shape_ok(const les_ctx *c, const TbShape &sh) {
     if (!tb_fits(sh.T, sh.ty) || sh.nch < 1 || sh.nch > kTbMaxChunks) return false;
-    if ((sh.T == 1 ? s1_smem(sh.ty) : tb_smem(sh.T, sh.ty)) > (size_t)g_tb_dyn_max) return false;
+    const size_t smem = sh.T == 1 ? s1_smem(sh.ty) : (sh.T == 2 ? s2_smem(sh.ty) : tb_smem(sh.T, sh.ty));
+    if (smem > (size_t)g_tb_dyn_max) return false;
     const int kc = cdiv(c->prm.kp, sh.nch);
     const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(sh.T)) * cdiv(c->prm.jp, sh.ty) * cdiv(c->prm.kp, kc);
     return nblk * kTbTMax <= c->npart;

@@ -276,3 +276,320 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
 
 }  // namespace
 }  // namespace les
+
+namespace les {
+namespace {
+
+// ---- two iterations per pass (T = 2) ----------------------------------------
+// The layout of k_sor1 with a four-row, four-plane ring (the region shrinks
+// by one per half-sweep): at step tau half-sweep s works on plane tau-s, the
+// colours of iteration 1 (s = 0, 1) and then of iteration 2 (s = 2, 3), all
+// four on the same x parity; each half-sweep publishes its row, and plane
+// tau-3 is final after s = 3.  The window holds planes tau+1 .. tau-4 (six),
+// so the loop is unrolled by six.  One plane of p and rhs is requested one
+// step ahead: seven plane slots, 168 KB at 24 rows.  Iteration 2's k ghosts
+// take the cell's own value by select (its ghost is the value after
+// iteration 1); iteration 1's come from the window as in k_sor1.  A pass
+// that is not the step's last takes FP32 residual sums with the bound of
+// tb_finish_fast for each of its iterations.  nit = 1 (an odd last pass,
+// the redo of a pass that converged after its first iteration, or the spare
+// pass) runs the first two half-sweeps only.  At most 24 rows (768 threads,
+// 80 registers: the six-plane window does not fit in 64).
+constexpr int kS2Depth = 1, kS2NS = 6 + kS2Depth;
+__host__ __device__ inline size_t s2_smem(int ty) {
+    return sizeof(float) * 2 * (size_t)kTbRW * tb_rh(2, ty) * kS2NS;
+}
+
+// Stop test of a fast (FP32-summed) pass of nit iterations: all counted if
+// every iteration's lower bound rules the stop out, else none and exact
+// sums for the rest of the step (the next pass repeats from the unchanged
+// input buffer).  See tb_finish_fast for the bound.
+__device__ void s2_finish_fast(const FixPart *part, int nblocks, int nit, float pjuge, Scal *s) {
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) s_ok = 1;
+    __syncthreads();
+    for (int t = 0; t < nit; ++t) {
+        float v = 0.0f;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+            v += __uint_as_float((unsigned)__ldcg(&part[(size_t)b * kTbTMax + t].lo));
+        v = block_float_sum0(v);
+        if (threadIdx.x == 0) {
+            const float lb = __fsub_rd(__fmul_rd(v, 0.99609375f), 0x1p-33f);
+            if (!(lb >= pjuge && lb < 0x1p40f)) s_ok = 0;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (s_ok) {
+            s->sor_iters += nit;
+            s->pbuf ^= 1;
+        } else {
+            s->exact_sums = 1;
+        }
+    }
+}
+
+template <bool CN1K>
+__global__ void __launch_bounds__(768, 1) k_sor2(Geo g, TbArgs a, const __grid_constant__ TbKCoef kq) {
+    extern __shared__ float4 smem4[];
+    Scal *sc = a.sc;
+    const bool redo = (a.mode == 1);
+    if (!redo && (sc->converged || sc->sor_iters >= a.itmax)) return;
+    const int nit = redo ? sc->redo : min(a.niter, a.itmax - sc->sor_iters);
+    if (nit <= 0) return;
+    const bool fast = a.fast && !redo && !sc->exact_sums && sc->sor_iters + nit < a.itmax;
+    constexpr int RX = tb_ringx(2), TX = tb_tx(2), NS = kS2NS, D = kS2Depth, RW4 = kTbRW / 4;
+    const int ty = a.ty, RH = ty + 8, RA4 = RW4 * RH;
+    float4 *P = smem4;
+    float4 *Bs = P + NS * RA4;
+    const float *pin = sc->pbuf ? a.pb1 : a.pb0;
+    float *pout = sc->pbuf ? a.pb0 : a.pb1;
+    const float rhsav = sc->rhsav, omega = g.omega;
+    const int im = g.im, jm = g.jm, km = g.km;
+    const int lane = threadIdx.x & 31, y = threadIdx.x >> 5;
+    const int ir0 = 1 + blockIdx.x * TX - RX, jr0 = 1 + blockIdx.y * ty - 4;
+    const int k0 = 1 + blockIdx.z * a.kc, k1 = min(km, k0 + a.kc - 1);
+    const int kb = max(1, k0 - 4), ke = min(km, k1 + 4);
+    const long long pstride = (long long)g.si * g.sj;
+    const int jw = ((jr0 + y - 1) % jm + jm) % jm + 1;
+    const long long coff = IX(g, ir0, jw, 0) + kTbCW * lane;
+    const float c3l = g.cn3l[jw], c3s = g.cn3s[jw], cB = CN1K ? 0.0f : g.cnB[jw];
+    const bool ytile = (y >= 4 && y < 4 + ty && jr0 + y <= jm);
+    float c2l[kTbCW], c2s[kTbCW], cA[kTbCW];
+    int fl[kTbCW];
+#pragma unroll
+    for (int c = 0; c < kTbCW; ++c) {
+        const int i = ir0 + kTbCW * lane + c;
+        const bool ok = (i >= 1 && i <= im);
+        c2l[c] = ok ? g.cn2l[i] : 0.0f;
+        c2s[c] = ok ? g.cn2s[i] : 0.0f;
+        cA[c] = (!CN1K && ok) ? g.cnA[i] : 0.0f;
+        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0);
+    }
+    const int x0 = kTbCW * lane;
+    const bool lane_tile = (x0 >= RX && x0 < RX + TX);
+    const bool acc_cells = !redo && ytile && lane_tile;
+    const int par0 = (jr0 + y + 1 - ir0 + kb) & 1;
+
+    const int d0 = y * RW4 + lane;
+    const float *gsrc = pin + coff, *bsrc = a.rhs + coff;
+    auto request = [&](int k, int slot) {
+        if (k <= ke) {
+            tb_cp_async16(reinterpret_cast<float *>(P + slot * RA4 + d0), gsrc + pstride * k);
+            tb_cp_async16(reinterpret_cast<float *>(Bs + slot * RA4 + d0), bsrc + pstride * k);
+        }
+        tb_cp_commit();
+    };
+#pragma unroll
+    for (int q = 0; q <= D; ++q) request(kb + q, q);
+    tb_cp_wait<D>();
+    __syncthreads();
+    // window: w[x][c], plane kb + x' at phase x' mod 6
+    float w[6][kTbCW];
+    {
+        const float4 v = P[d0];
+        w[0][0] = v.x, w[0][1] = v.y, w[0][2] = v.z, w[0][3] = v.w;
+#pragma unroll
+        for (int c = 0; c < kTbCW; ++c) {
+            w[1][c] = 0.0f;
+            w[2][c] = w[0][c];  // planes kb-4 .. kb-1: the bottom ghost (kb = 1) or ring planes
+            w[3][c] = w[0][c];
+            w[4][c] = w[0][c];
+            w[5][c] = w[0][c];
+        }
+    }
+    float fs0 = 0.0f, fs1 = 0.0f;  // FP32 residual sums of iterations 1 and 2
+    unsigned long long h0 = 0, l0 = 0, h1 = 0, l1 = 0;
+    int bad = 0;
+    const int tau_end = k1 + (nit == 2 ? 3 : 1);
+    const bool edge = ir0 <= 1 || ir0 + kTbRW - 1 >= im;
+
+    auto run = [&](auto PARc, auto FASTc, auto EDGEc, auto NITc) {
+        constexpr int PAR = decltype(PARc)::value, NIT = decltype(NITc)::value;
+        constexpr bool FAST = decltype(FASTc)::value, EDGE = decltype(EDGEc)::value;
+        int slot1 = 1;  // slot of plane tau+1
+        for (int tau0 = kb; tau0 <= tau_end; tau0 += 6) {
+            auto step = [&](auto Mc) {
+                constexpr int m = decltype(Mc)::value;
+                constexpr int C0 = (PAR + m) & 1;
+                // window phases of planes tau+1, tau, tau-1, .., tau-4
+                constexpr int XP1 = (m + 1) % 6, X0 = m % 6, X1 = (m + 5) % 6, X2 = (m + 4) % 6,
+                              X3 = (m + 3) % 6, X4 = (m + 2) % 6;
+                const int tau = tau0 + m;
+                if (tau > tau_end) return;
+                int sq[4];  // slots of planes tau, tau-1, tau-2, tau-3
+                sq[0] = slot1 == 0 ? NS - 1 : slot1 - 1;
+#pragma unroll
+                for (int s = 1; s < 4; ++s) sq[s] = sq[s - 1] == 0 ? NS - 1 : sq[s - 1] - 1;
+                int sreq = slot1 + D;
+                if (sreq >= NS) sreq -= NS;
+                request(tau + 1 + D, sreq);
+                tb_cp_wait<D>();
+                __syncthreads();
+                if (tau + 1 <= ke) {
+                    const float4 v = P[slot1 * RA4 + d0];
+                    w[XP1][0] = v.x, w[XP1][1] = v.y, w[XP1][2] = v.z, w[XP1][3] = v.w;
+                } else {
+#pragma unroll
+                    for (int c = 0; c < kTbCW; ++c) w[XP1][c] = w[X0][c];
+                }
+                // half-sweep s on plane q = tau - s: the cell's window row XQ, its
+                // neighbours above (XU) and below (XD)
+                auto half = [&](auto Sc, auto XQc, auto XUc, auto XDc) {
+                    constexpr int S = decltype(Sc)::value, XQ = decltype(XQc)::value, XU = decltype(XUc)::value,
+                                  XD = decltype(XDc)::value;
+                    const int q = tau - S;
+                    if (!(q >= kb && q <= ke && y >= S + 1 && y < RH - S - 1)) return;
+                    const float4 *Pq = P + sq[S] * RA4 + d0;
+                    const float4 nn = Pq[RW4], ss = Pq[-RW4], bb = Bs[sq[S] * RA4 + d0];
+                    const float c4l = kq.c4l[q], c4s = kq.c4s[q];
+                    const float cnq = CN1K ? kq.cnk[q] : 0.0f, cC = CN1K ? 0.0f : g.cnC[q];
+                    const bool acc = acc_cells && q >= k0 && q <= k1;
+                    const bool top = S >= 2 && q == km, bot = S >= 2 && q == 1;
+                    auto upd = [&](auto Cc, float west, float east, float pn, float ps, float b) {
+                        constexpr int C = decltype(Cc)::value;
+                        const float pc = w[XQ][C];
+                        const float pe = (EDGE && (fl[C] & 4)) ? pc : east;
+                        const float pw = (EDGE && (fl[C] & 2)) ? pc : west;
+                        const float pu = top ? pc : w[XU][C];
+                        const float pd = bot ? pc : w[XD][C];
+                        const float cn1 = CN1K ? cnq : 1.0f / (cA[C] + cB + cC);
+                        const float reltmp = omega * (cn1 * (c2l[C] * pe + c2s[C] * pw + c3l * pn + c3s * ps +
+                                                             c4l * pu + c4s * pd - (b - rhsav)) -
+                                                      pc);
+                        w[XQ][C] = pc + reltmp;
+                        if (acc && (!EDGE || (fl[C] & 1))) {
+                            const float t2 = reltmp * reltmp;
+                            if constexpr (FAST) {
+                                if (S < 2)
+                                    fs0 += t2;
+                                else
+                                    fs1 += t2;
+                            } else {
+                                if (S < 2)
+                                    fix_add_nonneg(t2, h0, l0, bad);
+                                else
+                                    fix_add_nonneg(t2, h1, l1, bad);
+                            }
+                        }
+                    };
+                    if constexpr (C0 == 0) {
+                        const float nb = __shfl_sync(0xffffffffu, w[XQ][3], lane - 1);
+                        upd(IC<0>(), nb, w[XQ][1], nn.x, ss.x, bb.x);
+                        upd(IC<2>(), w[XQ][1], w[XQ][3], nn.z, ss.z, bb.z);
+                    } else {
+                        const float nb = __shfl_sync(0xffffffffu, w[XQ][0], lane + 1);
+                        upd(IC<1>(), w[XQ][0], w[XQ][2], nn.y, ss.y, bb.y);
+                        upd(IC<3>(), w[XQ][2], nb, nn.w, ss.w, bb.w);
+                    }
+                    if (S < 2 * NIT - 1)  // later half-sweeps of the pass read this row
+                        P[sq[S] * RA4 + d0] = make_float4(w[XQ][0], w[XQ][1], w[XQ][2], w[XQ][3]);
+                };
+                half(IC<0>(), IC<X0>(), IC<XP1>(), IC<X1>());
+                half(IC<1>(), IC<X1>(), IC<X0>(), IC<X2>());
+                if constexpr (NIT == 2) {
+                    half(IC<2>(), IC<X2>(), IC<X1>(), IC<X3>());
+                    half(IC<3>(), IC<X3>(), IC<X2>(), IC<X4>());
+                }
+                // the pass's last half-sweep finished plane qs: store its tile part
+                constexpr int XS = NIT == 2 ? X3 : X1;
+                const int qs = tau - (2 * NIT - 1);
+                if (acc_cells || (redo && ytile && lane_tile)) {
+                    if (qs >= k0 && qs <= k1) {
+                        float *dst = pout + (coff + pstride * qs);
+                        if (!EDGE || (fl[3] & fl[0] & 1))
+                            *reinterpret_cast<float4 *>(dst) = make_float4(w[XS][0], w[XS][1], w[XS][2], w[XS][3]);
+                        else {
+#pragma unroll
+                            for (int c = 0; c < kTbCW; ++c)
+                                if (fl[c] & 1) dst[c] = w[XS][c];
+                        }
+                    }
+                }
+                slot1 = slot1 + 1 == NS ? 0 : slot1 + 1;
+            };
+            step(IC<0>());
+            step(IC<1>());
+            step(IC<2>());
+            step(IC<3>());
+            step(IC<4>());
+            step(IC<5>());
+        }
+    };
+    using True = std::true_type;
+    using False = std::false_type;
+#define S2_RUN(F, E, N)                         \
+    do {                                        \
+        if (par0)                               \
+            run(IC<1>(), F(), E(), IC<N>());    \
+        else                                    \
+            run(IC<0>(), F(), E(), IC<N>());    \
+    } while (0)
+    if (nit == 2) {
+        if (fast) {
+            if (edge) S2_RUN(True, True, 2);
+            else S2_RUN(True, False, 2);
+        } else {
+            if (edge) S2_RUN(False, True, 2);
+            else S2_RUN(False, False, 2);
+        }
+    } else {
+        if (fast) {
+            if (edge) S2_RUN(True, True, 1);
+            else S2_RUN(True, False, 1);
+        } else {
+            if (edge) S2_RUN(False, True, 1);
+            else S2_RUN(False, False, 1);
+        }
+    }
+#undef S2_RUN
+    tb_cp_wait<0>();
+
+    const int nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    __syncthreads();
+    if (!redo) {
+        if (fast) {
+            const float v0 = block_float_sum0(fs0);
+            __syncthreads();
+            const float v1 = block_float_sum0(fs1);
+            if (threadIdx.x == 0) {
+                FixPart f0{}, f1{};
+                f0.lo = __float_as_uint(v0);
+                f1.lo = __float_as_uint(v1);
+                a.part[b * kTbTMax] = f0;
+                a.part[b * kTbTMax + 1] = f1;
+            }
+        } else {
+            block_fix_sum_any((i128)(((unsigned __int128)h0 << 64) | (unsigned __int128)l0), bad,
+                              &a.part[b * kTbTMax]);
+            __syncthreads();
+            block_fix_sum_any((i128)(((unsigned __int128)h1 << 64) | (unsigned __int128)l1), bad,
+                              &a.part[b * kTbTMax + 1]);
+        }
+    }
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&sc->ticket, 1u) == (unsigned)nblocks - 1u);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) sc->ticket = 0u;
+    if (redo) {
+        if (threadIdx.x == 0) {
+            sc->redo = 0;
+            sc->pbuf ^= 1;
+        }
+        return;
+    }
+    if (fast)
+        s2_finish_fast(a.part, nblocks, nit, a.pjuge, sc);
+    else
+        tb_finish_pass(a.part, nblocks, nit, a.pjuge, sc);
+}
+
+}  // namespace
+}  // namespace les

@@ -191,12 +191,12 @@ def _residual_after(ip, jp, kp, seed, iters, monkeypatch):
     return r
 
 
-@pytest.mark.parametrize("shape", ["1,8,1", "1,12,2"])
+@pytest.mark.parametrize("shape", ["1,8,1", "1,12,2", "2,8,1", "2,12,2"])
 @pytest.mark.parametrize("at,scale", [(6, 1.0), (6, 1.0009765625), (1, 1.0), (1, 1.0009765625),
-                                      (24, 1.0), (24, 1.0009765625)])
+                                      (24, 1.0), (24, 1.0009765625), (23, 1.0), (23, 1.0009765625)])
 def test_undecided_fp32_stop_test_repeats_the_iteration_exactly(require_gpu, monkeypatch, shape, at, scale):
-    # One-iteration passes before the last iteration take an FP32 stop test
-    # that only rules out convergence.  A threshold at iteration `at`'s exact
+    # Passes (of one or two iterations) that do not hold the step's last
+    # iteration take an FP32 stop test that only rules out convergence.  A threshold at iteration `at`'s exact
     # residual (scale 1: the exact test does not stop there) or just above
     # it (it stops there) leaves that test undecided: the iteration runs
     # again with exact sums, also on the first iteration and on the one
