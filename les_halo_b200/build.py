@@ -25,7 +25,6 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
     "-Xptxas", "-v",
     "-shared",
-    "-lcufft",
 ]
 
 

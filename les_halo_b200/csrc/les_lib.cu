@@ -1,7 +1,6 @@
 // les_lib.cu -- host side of liblesb200.so: contexts, the host boundary,
 // the graph-captured time step and the setup routines (les_abi.h).
 #include <cuda_runtime.h>
-#include <cufft.h>
 
 #include <algorithm>
 #include <climits>
@@ -28,6 +27,7 @@
 #include "les_stats.cuh"
 #include "les_refine.cuh"
 #include "les_spectral.cuh"
+#include "les_fft.cuh"
 #include "les_step.cuh"
 
 using namespace les;
@@ -235,12 +235,6 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
 // sequence with materialised ghosts) instead of the temporal-blocked passes:
 // on request, for odd jp (same-colour periodic partners), for a just-uploaded
 // p whose ghosts are not boundary-consistent, and for km >= kTbKMax.
-// The refined press with the spectral inner solve (inner = 0) runs after
-// the captured step graph, issued directly on the stream: its cuFFT
-// executions captured into the step graph faulted (misaligned address) on a
-// B200 where the same sequence issued directly ran correctly.
-bool spec_eager(const les_ctx *c) { return c->ref_outer > 0 && c->ref_inner == 0; }
-
 bool sor_per_colour(const les_ctx *c) {
     return c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok || c->prm.kp >= kTbKMax ||
            (c->red_mode & LES_RED_F_SOR);
@@ -518,14 +512,16 @@ les_status enqueue_press(les_ctx *c, bool exact) {
         }
         // an iteration whose FP32 stop test was undecided runs again with
         // exact sums (at most once per step): one more pass, which returns
-        // at once when all nmaxp iterations are done or the SOR stopped
+        // at once when all nmaxp iterations are done or the SOR stopped, and
+        // for multi-iteration passes its redo (the repeated iterations may
+        // be the ones where the SOR stops)
         if (nmaxp >= 2 && tb_fast_ok(c, c->tb)) {
             les_status st = launch_sor_tb(c, c->tb, c->tb.T, 0, c->prm.pjuge, nmaxp);
             if (st != LES_OK) return st;
+            if (c->tb.T > 1 && (st = launch_sor_tb(c, c->tb, c->tb.T, 1, c->prm.pjuge, nmaxp)) != LES_OK) return st;
         }
     }
     MARK(c, EV_SOR_END);
-    if (c->ref_outer > 0 && spec_eager(c)) return LES_OK;  // the tail runs after the graph (les_step)
     if (c->ref_outer > 0) {
         les_status st = enqueue_refine(c);
         MARK(c, EV_PAV);
@@ -551,7 +547,6 @@ les_status enqueue_step(les_ctx *c, int n, bool exact_sor) {
     MARK(c, EV_BONDV1);
     if ((s = enqueue_velfg_les(c, true)) != LES_OK) return s;
     if ((s = enqueue_press(c, exact_sor)) != LES_OK) return s;
-    if (c->ref_outer > 0 && spec_eager(c)) return LES_OK;  // probe after the eager tail
     LAUNCH(c, k_probe, dim3(1), dim3(1), c->geo, c->F, c->d_scal);
     return LES_OK;
 }
@@ -1260,11 +1255,6 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
         LAUNCH(c, k_step_begin, dim3(1), dim3(1), c->d_scal, n);
         CK(cudaGraphLaunch(c->graph[gi], c->stream));
         c->launches += c->graph_kernels[gi];
-        if (c->ref_outer > 0 && spec_eager(c)) {  // the refined press's tail, issued directly
-            les_status st = enqueue_refine(c);
-            if (st != LES_OK) return st;
-            LAUNCH(c, k_probe, dim3(1), dim3(1), c->geo, c->F, c->d_scal);
-        }
         c->last_n = n;
         c->rhs_raw = true;
         c->p_ghosts_ok = true;  // press ends with boundp1/boundp2

@@ -621,8 +621,10 @@ __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
 }
 
 // les.f95:170-274 viscous terms (+ adam.f95:32-46) for a 32 x 8 tile, all k.
+// Three CTAs per SM (at most 62 registers, no spills): 1.91 -> 1.72 ms at
+// 600 x 600 x 120 (k_mom1 at three was slower, 2.16 -> 2.25 ms).
 template <bool ADAM, bool BAND, bool P2>
-__global__ void __launch_bounds__(kMNT) k_mom2(Geo g, Fields F) {
+__global__ void __launch_bounds__(kMNT, 3) k_mom2(Geo g, Fields F) {
     const int i = 1 + blockIdx.x * kMX + threadIdx.x % kMX, j = 1 + blockIdx.y * kMY + threadIdx.x / kMX;
     const bool mine = threadIdx.x < kMX * kMY && i <= g.im && j <= g.jm;
     // the cell's f, g, h (and fold, gold, hold) of plane k, loaded ahead by

@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(768, 1) k_sor2(Geo g, TbArgs a, const __grid_c
                 constexpr int C0 = (PAR + m) & 1;
                 // window phases of planes tau+1, tau, tau-1, .., tau-4
                 constexpr int XP1 = (m + 1) % 6, X0 = m % 6, X1 = (m + 5) % 6, X2 = (m + 4) % 6,
-                              X3 = (m + 3) % 6, X4 = (m + 2) % 6;
+                              X3 = (m + 3) % 6;
                 const int tau = tau0 + m;
                 if (tau > tau_end) return;
                 int sq[4];  // slots of planes tau, tau-1, tau-2, tau-3
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(768, 1) k_sor2(Geo g, TbArgs a, const __grid_c
                 half(IC<1>(), IC<X1>(), IC<X0>(), IC<X2>());
                 if constexpr (NIT == 2) {
                     half(IC<2>(), IC<X2>(), IC<X1>(), IC<X3>());
-                    half(IC<3>(), IC<X3>(), IC<X2>(), IC<X4>());
+                    half(IC<3>(), IC<X3>(), IC<X2>(), IC<(m + 2) % 6>());  // below: plane tau-4
                 }
                 // the pass's last half-sweep finished plane qs: store its tile part
                 constexpr int XS = NIT == 2 ? X3 : X1;

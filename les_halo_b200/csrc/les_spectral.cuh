@@ -10,8 +10,10 @@
 // transforms.  The DCT-II of an even-length line is one real FFT of the
 // line's values taken in even-then-reversed-odd order, twiddled by
 // exp(-i pi m / 2N) (J. Makhoul, IEEE Trans. ASSP 28(1), 1980), and its
-// inverse the reverse.  FFTs are cuFFT's (double precision); the twiddles,
-// transposes, tridiagonal solves and the correction are these kernels.
+// inverse the reverse.  The FFTs are les_fft.cuh's (FP64, mixed radix); the
+// twiddles, transposes, tridiagonal solves and the correction are these
+// kernels.  The whole tail is captured in the step graph: corrections after
+// the tolerance is met return at once on the device (Ref64::stop).
 //
 // Layouts (dense, FP64): r and v lines [k][j][pos] (makhoul_pos order);
 // V = FFT of a line [k][j][0..im/2]; X [k][m][j] (j contiguous, for the
