@@ -146,6 +146,13 @@ les_status les_ctx_set_timing(les_ctx *ctx, int nslots);
  * give identical results; odd jp and a just-uploaded p whose ghosts are not
  * boundary-consistent always use the per-colour sweeps. */
 les_status les_ctx_set_sor_path(les_ctx *ctx, int exact);
+/* Bounds-checked build (liblesb200_checked.so, compiled with LES_CHECKED):
+ * every box index of the time step's kernels is checked against its
+ * allocation; an index outside it is counted, the first one's (i, j, k)
+ * kept, and the access redirected (no fault, no trap).  Returns the count
+ * and that index after synchronising the device; in the regular build it
+ * returns LES_ERR_STATE. */
+les_status les_bounds_violations(unsigned long long *count, int *first_ijk);
 /* Order of the step's global sums.  LES_RED_CANONICAL (default): rhsav, the
  * SOR residual and pav are exact sums (each FP32 term converted exactly to
  * fixed point, summed without rounding, finished in FP64), the same whatever

@@ -6,9 +6,13 @@ Python or CPU fallback for any compute entry point.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "liblesb200.so"
+CHECKED_LIB_PATH = Path(__file__).resolve().parent / "liblesb200_checked.so"
+if os.environ.get("LES_B200_CHECKED") == "1":  # the bounds-checked build (tests)
+    LIB_PATH = CHECKED_LIB_PATH
 
 LES_OK, LES_ERR_BAD_ARG, LES_ERR_DIMS, LES_ERR_CUDA, LES_ERR_TIMEOUT, LES_ERR_NAN, \
     LES_ERR_NOMEM, LES_ERR_STATE, LES_ERR_IO = range(9)
@@ -99,6 +103,7 @@ _SIGS = {
     "les_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "les_ctx_set_sor_path": (C.c_int, [_P, C.c_int]),
     "les_ctx_set_reduction_mode": (C.c_int, [_P, C.c_int]),
+    "les_bounds_violations": (C.c_int, [C.POINTER(C.c_ulonglong), _I]),
     "les_ctx_sor_iters_per_launch": (C.c_float, [_P]),
     "les_ctx_sor_tile": (C.c_int, [_P, _I, _I]),
     "les_ctx_sor_shape": (C.c_int, [_P, _I, _I, _I, _I]),

@@ -115,8 +115,37 @@ struct Scal {
     int exact_sums;  // 1: the rest of this step's SOR passes sum the residual exactly
 };
 
+#ifdef LES_CHECKED
+// LES_CHECKED builds (liblesb200_checked.so): every box index is checked
+// against the allocation; a miss is counted, the first one's (i, j, k) is
+// kept, and the access goes to element 0 instead -- no fault and no trap.
+// One record per translation unit; les_bounds_violations reads the time
+// step's (les_lib.cu).
+struct LesOob {
+    unsigned long long count;
+    int claimed;
+    int first[3];
+};
+static __device__ LesOob g_les_oob;
+static __device__ __noinline__ void les_oob_record(int i, int j, int k) {
+    atomicAdd(&g_les_oob.count, 1ull);
+    if (atomicCAS(&g_les_oob.claimed, 0, 1) == 0) {
+        g_les_oob.first[0] = i;
+        g_les_oob.first[1] = j;
+        g_les_oob.first[2] = k;
+    }
+}
+#endif
+
 __device__ __forceinline__ int IX(const Geo &g, int i, int j, int k) {
-    return (i + g.ox) + g.si * ((j + 1) + g.sj * (k + 1));
+    const int off = (i + g.ox) + g.si * ((j + 1) + g.sj * (k + 1));
+#ifdef LES_CHECKED
+    if (off < 0 || off >= g.si * g.sj * g.sk) {
+        les_oob_record(i, j, k);
+        return 0;
+    }
+#endif
+    return off;
 }
 
 // ---------------------------------------------------------------------------

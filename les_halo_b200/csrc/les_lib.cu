@@ -1162,6 +1162,22 @@ les_status les_ctx_set_sor_path(les_ctx *c, int exact) {
     return ok();
 }
 
+les_status les_bounds_violations(unsigned long long *count, int *first_ijk) {
+#ifdef LES_CHECKED
+    LesOob h{};
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpyFromSymbol(&h, g_les_oob, sizeof h));
+    if (count) *count = h.count;
+    if (first_ijk)
+        for (int q = 0; q < 3; ++q) first_ijk[q] = h.claimed ? h.first[q] : 0;
+    return ok();
+#else
+    (void)count;
+    (void)first_ijk;
+    return fail(LES_ERR_STATE, "not a LES_CHECKED build (liblesb200_checked.so)");
+#endif
+}
+
 les_status les_ctx_set_reduction_mode(les_ctx *c, int mode) {
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     if (mode < 0 || mode > LES_RED_FAITHFUL) return fail(LES_ERR_BAD_ARG, "bad reduction mode %d", mode);

@@ -22,14 +22,26 @@ def _declared():
     return names
 
 
-def test_every_declared_symbol_is_exported():
-    out = subprocess.run(["nm", "-D", "--defined-only", str(abi.LIB_PATH)], capture_output=True,
+@pytest.mark.parametrize("path", [abi.LIB_PATH, abi.CHECKED_LIB_PATH], ids=["plain", "checked"])
+def test_every_declared_symbol_is_exported(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(path)], capture_output=True,
                          text=True, check=True).stdout
     exported = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
     missing = sorted(_declared() - exported)
     assert not missing, f"declared in include/*.h but not exported: {missing}"
+
+
+def test_library_loads_and_binds():
     lib = abi.lib()  # loads and binds every prototype
     assert lib.les_version().startswith(b"lesb200")
+
+
+def test_bounds_violations_needs_the_checked_build():
+    """The plain library answers les_bounds_violations with LES_ERR_STATE
+    (no GPU call is made)."""
+    if abi.LIB_PATH != abi.CHECKED_LIB_PATH:
+        n = C.c_ulonglong(7)
+        assert abi.lib().les_bounds_violations(C.byref(n), None) == abi.LES_ERR_STATE
 
 
 def test_grid_metrics_match_oracle():
