@@ -4,7 +4,8 @@ against its allocation.  The same workload (tests/checked_workload.py: time
 steps over ragged shapes in both sum modes, the context's halo entries, both
 FP64 refinements, the step adjoint with a drag scale, an ensemble) runs on
 both libraries in child processes; the checked one must see no index out of
-range, and its results must be bit-identical to the plain library's.
+range, and its results must be bit-identical to the plain library's (the
+step adjoint, whose atomic sums are order-dependent, to 1e-5 relative).
 """
 import json
 import os
@@ -37,4 +38,7 @@ def test_checked_build_sees_no_out_of_range_index(require_gpu):
     plain = _run(False)
     assert plain["lib"] == "liblesb200.so"
     assert plain["status"] != 0  # the plain build has no bounds record
-    assert chk["digest"] == plain["digest"]
+    for part in ("steps", "refine", "ensemble"):
+        assert chk[part] == plain[part], part
+    for k, v in plain["adjoint"].items():
+        assert abs(chk["adjoint"][k] - v) <= 1e-5 * abs(v), (k, chk["adjoint"][k], v)

@@ -65,3 +65,26 @@ def test_ensemble_member_against_oracle(require_gpu):
     ens.close()
     for g in members:
         g.close()
+
+
+def test_ensemble_with_refined_members(require_gpu):
+    # members on the FP64-refined press (spectral and SOR inner solves; the
+    # refine tail is part of each member's captured step) give what they give
+    # alone
+    doms = [((24, 20, 12), 3, 0.3), ((40, 26, 16), 4, 0.45)]
+    cases = [_case(*d) for d in doms]
+    solo = [GpuLes(c.copy()) for c in cases]
+    members = [GpuLes(c.copy()) for c in cases]
+    for g, (outer, inner) in zip(solo + members, [(2, 0), (1, 6)] * 2):
+        g.warmup(1)
+        g.press_refine_fp64(outer, inner, 1e-9)
+    ens = Ensemble(members)
+    ens.step(1, 3)
+    for g in solo:
+        g.step(1, 3)
+    for (dims, _, _), a, b in zip(doms, members, solo):
+        assert_bitexact(a.download(ALL), b.download(ALL), *dims, ALL)
+        assert a.refine_metrics() == b.refine_metrics()
+    ens.close()
+    for g in solo + members:
+        g.close()

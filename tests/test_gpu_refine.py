@@ -86,7 +86,7 @@ def test_refine_rejects_odd_jp(require_gpu):
 
 @pytest.mark.parametrize("outer", [1, 2])
 def test_spectral_refined_press_matches_oracle(require_gpu, outer):
-    # inner = 0: the FP64 spectral solve (cuFFT on the GPU, direct sums in
+    # inner = 0: the FP64 spectral solve (FFT kernels on the GPU, direct sums in
     # the oracle) solves the FP64 system in one correction; both agree to
     # FP64 rounding, so p after its FP32 rounding differs by at most an ulp
     ref, gpu, got, want_m, m = _run(outer, 0, 0.0)
