@@ -233,11 +233,13 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
 
 // The SOR of the next step runs one colour sweep at a time (press.f95's own
 // sequence with materialised ghosts) instead of the temporal-blocked passes:
-// on request, for odd jp (same-colour periodic partners), for a just-uploaded
-// p whose ghosts are not boundary-consistent, and for km >= kTbKMax.
+// on request, for odd jp below the shortest one-iteration pass region
+// (odd jp takes one-iteration passes only, whose region must not hold a row
+// twice), for a just-uploaded p whose ghosts are not boundary-consistent,
+// for km >= kTbKMax, and for reference-order residual sums.
 bool sor_per_colour(const les_ctx *c) {
-    return c->force_exact_sor || (c->prm.jp % 2) != 0 || !c->p_ghosts_ok || c->prm.kp >= kTbKMax ||
-           (c->red_mode & LES_RED_F_SOR);
+    return c->force_exact_sor || ((c->prm.jp % 2) != 0 && c->prm.jp < tb_rh(1, 4)) || !c->p_ghosts_ok ||
+           c->prm.kp >= kTbKMax || (c->red_mode & LES_RED_F_SOR);
 }
 
 void drop_step_graphs(les_ctx *c) {
@@ -614,8 +616,18 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     const Geo &g = c->geo;
 #define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a, c->kq)
     switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
-        case 2: LAUNCH_SMEM(c, k_sor1<false>, grid, block, s1_smem(sh.ty), g, a, c->kq); break;
-        case 3: LAUNCH_SMEM(c, k_sor1<true>, grid, block, s1_smem(sh.ty), g, a, c->kq); break;
+        case 2:
+            if (c->prm.jp % 2)
+                LAUNCH_SMEM(c, (k_sor1<false, true>), grid, block, s1_smem(sh.ty), g, a, c->kq);
+            else
+                LAUNCH_SMEM(c, (k_sor1<false, false>), grid, block, s1_smem(sh.ty), g, a, c->kq);
+            break;
+        case 3:
+            if (c->prm.jp % 2)
+                LAUNCH_SMEM(c, (k_sor1<true, true>), grid, block, s1_smem(sh.ty), g, a, c->kq);
+            else
+                LAUNCH_SMEM(c, (k_sor1<true, false>), grid, block, s1_smem(sh.ty), g, a, c->kq);
+            break;
         case 4: LAUNCH_SMEM(c, k_sor2<false>, grid, block, s2_smem(sh.ty), g, a, c->kq); break;
         case 5: LAUNCH_SMEM(c, k_sor2<true>, grid, block, s2_smem(sh.ty), g, a, c->kq); break;
         case 6: TBL(3, false); break;
@@ -644,15 +656,15 @@ les_status set_tb_smem_attrs() {
     }
     TBA(3, false) TBA(3, true)
 #undef TBA
-#define S1A(KT)                                                                                \
-    {                                                                                          \
-        cudaFuncAttributes fa;                                                                 \
-        CK(cudaFuncGetAttributes(&fa, k_sor1<KT>));                                            \
-        const int mx = optin - (int)fa.sharedSizeBytes;                                        \
-        CK(cudaFuncSetAttribute(k_sor1<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
-        lim = std::min(lim, mx);                                                               \
+#define S1A(KT, JO)                                                                                \
+    {                                                                                              \
+        cudaFuncAttributes fa;                                                                     \
+        CK(cudaFuncGetAttributes(&fa, k_sor1<KT, JO>));                                            \
+        const int mx = optin - (int)fa.sharedSizeBytes;                                            \
+        CK(cudaFuncSetAttribute(k_sor1<KT, JO>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+        lim = std::min(lim, mx);                                                                   \
     }
-    S1A(false) S1A(true)
+    S1A(false, false) S1A(true, false) S1A(false, true) S1A(true, true)
 #undef S1A
 #define S2A(KT)                                                                                \
     {                                                                                          \
@@ -682,6 +694,8 @@ std::mutex g_tune_mu;
 // memory and the partial-sum array.
 bool tb_shape_ok(const les_ctx *c, const TbShape &sh) {
     if (!tb_fits(sh.T, sh.ty) || sh.nch < 1 || sh.nch > kTbMaxChunks) return false;
+    // odd jp: one iteration per pass (k_sor1), each real row once in a region
+    if ((c->prm.jp % 2) != 0 && (sh.T != 1 || tb_rh(1, sh.ty) > c->prm.jp)) return false;
     const size_t smem = sh.T == 1 ? s1_smem(sh.ty) : (sh.T == 2 ? s2_smem(sh.ty) : tb_smem(sh.T, sh.ty));
     if (smem > (size_t)g_tb_dyn_max) return false;
     const int kc = cdiv(c->prm.kp, sh.nch);
@@ -701,9 +715,11 @@ les_status autotune_sor(les_ctx *c) {
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const TuneKey key{c->prm.ip, c->prm.jp, c->prm.kp, nsm};
     TbShape best;
-    if (const char *ov = std::getenv("LES_SOR_TILE")) {
+    if (const char *ov = std::getenv("LES_SOR_TILE")) {  // taken where this grid can run it
         std::sscanf(ov, "%d,%d,%d", &best.T, &best.ty, &best.nch);
-    } else {
+        if (!tb_shape_ok(c, best)) best = TbShape{};
+    }
+    if (!best.T) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(key);
         if (it != g_tune.end()) best = it->second;

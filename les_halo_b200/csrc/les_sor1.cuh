@@ -33,16 +33,25 @@ namespace {
 
 constexpr int kS1Depth = 2;                       // planes requested ahead of the incoming one
 constexpr int kS1NS = 4 + kS1Depth;               // plane slots (p and rhs each)
+// p and rhs slots, then per slot the input copies of the two rows that meet
+// across the periodic j boundary (odd jm)
 __host__ __device__ inline size_t s1_smem(int ty) {
-    return sizeof(float) * 2 * (size_t)kTbRW * tb_rh(1, ty) * kS1NS;
+    return sizeof(float) * 2 * (size_t)kTbRW * tb_rh(1, ty) * kS1NS + sizeof(float) * 2 * (size_t)kTbRW * kS1NS;
 }
 
 template <int V>
 using IC = std::integral_constant<int, V>;
 
 // One pass of one SOR iteration.  blockDim.x = 32 * (ty + 4): warp y owns
-// region row y.
-template <bool CN1K>
+// region row y, the real row jw (periodic), whose colour parity is that of
+// jw.  JODD (odd jm): rows jm and 1 are j-neighbours of the same colour, and in
+// press.f95 each reads the other through the ghost rows 0 and jm+1, which
+// boundp1 refreshed before the half-sweep -- the other's value before its own
+// update, i.e. its input value in a one-iteration pass.  The warps of those
+// two rows also copy their input rows into a side pair of rows per plane
+// slot, and read each other there (the region holds each real row once:
+// ty + 4 <= jm).
+template <bool CN1K, bool JODD>
 __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_constant__ TbKCoef kq) {
     extern __shared__ float4 smem4[];
     Scal *sc = a.sc;
@@ -52,6 +61,7 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
     const int ty = a.ty, RH = ty + 4, RA4 = RW4 * RH;
     float4 *P = smem4;          // NS plane slots of p
     float4 *Bs = P + NS * RA4;  // NS plane slots of rhs
+    float4 *Sd = Bs + NS * RA4;  // NS slots of the input rows jm (row 0) and 1 (row 1), odd jm
     const float *pin = sc->pbuf ? a.pb1 : a.pb0;
     float *pout = sc->pbuf ? a.pb0 : a.pb1;
     const float rhsav = sc->rhsav, omega = g.omega;
@@ -61,7 +71,8 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
     const int k0 = 1 + blockIdx.z * a.kc, k1 = min(km, k0 + a.kc - 1);
     const int kb = max(1, k0 - 2), ke = min(km, k1 + 2);
     const long long pstride = (long long)g.si * g.sj;
-    const int jw = ((jr0 + y - 1) % jm + jm) % jm + 1;  // periodic j (jm even)
+    const int jw = ((jr0 + y - 1) % jm + jm) % jm + 1;  // periodic j
+    const bool wrapn = JODD && jw == jm, wraps = JODD && jw == 1;  // j+1 resp. j-1 across the boundary
     const long long coff = IX(g, ir0, jw, 0) + kTbCW * lane;
     const float c3l = g.cn3l[jw], c3s = g.cn3s[jw], cB = CN1K ? 0.0f : g.cnB[jw];
     const bool ytile = (y >= 2 && y < 2 + ty && jr0 + y <= jm);
@@ -81,7 +92,7 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
     const bool lane_tile = (x0 >= RX && x0 < RX + TX);
     const bool acc_cells = ytile && lane_tile;
     // x parity of the colour-0 columns at the first step (tau = kb)
-    const int par0 = (jr0 + y + 1 - ir0 + kb) & 1;
+    const int par0 = (jw + 1 - ir0 + kb) & 1;
 
     const int d0 = y * RW4 + lane;
     const float *gsrc = pin + coff, *bsrc = a.rhs + coff;
@@ -89,6 +100,9 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
         if (k <= ke) {
             tb_cp_async16(reinterpret_cast<float *>(P + slot * RA4 + d0), gsrc + pstride * k);
             tb_cp_async16(reinterpret_cast<float *>(Bs + slot * RA4 + d0), bsrc + pstride * k);
+            if (wrapn || wraps)  // row jm -> side row 0, row 1 -> side row 1
+                tb_cp_async16(reinterpret_cast<float *>(Sd + (2 * slot + (wraps ? 1 : 0)) * RW4 + lane),
+                              gsrc + pstride * k);
         }
         tb_cp_commit();
     };
@@ -164,7 +178,9 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
                 // colour 0 on plane tau
                 if (row0 && tau <= ke) {
                     const float4 *Pq = P + sq0 * RA4 + d0;
-                    const float4 nn = Pq[RW4], ss = Pq[-RW4], bb = Bs[sq0 * RA4 + d0];
+                    const float4 nn = wrapn ? Sd[(2 * sq0 + 1) * RW4 + lane] : Pq[RW4];
+                    const float4 ss = wraps ? Sd[2 * sq0 * RW4 + lane] : Pq[-RW4];
+                    const float4 bb = Bs[sq0 * RA4 + d0];
                     const float c4l = kq.c4l[tau], c4s = kq.c4s[tau];
                     const float cnq = CN1K ? kq.cnk[tau] : 0.0f, cC = CN1K ? 0.0f : g.cnC[tau];
                     const bool acc = acc_cells && tau >= k0 && tau <= k1;
@@ -186,7 +202,9 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
                 const int q = tau - 1;
                 if (row1 && q >= kb) {
                     const float4 *Pq = P + sqm * RA4 + d0;
-                    const float4 nn = Pq[RW4], ss = Pq[-RW4], bb = Bs[sqm * RA4 + d0];
+                    const float4 nn = wrapn ? Sd[(2 * sqm + 1) * RW4 + lane] : Pq[RW4];
+                    const float4 ss = wraps ? Sd[2 * sqm * RW4 + lane] : Pq[-RW4];
+                    const float4 bb = Bs[sqm * RA4 + d0];
                     const float c4l = kq.c4l[q], c4s = kq.c4s[q];
                     const float cnq = CN1K ? kq.cnk[q] : 0.0f, cC = CN1K ? 0.0f : g.cnC[q];
                     const bool acc = acc_cells && q >= k0 && q <= k1;

@@ -293,6 +293,51 @@ def test_each_sor_pass_shape_equals_per_colour_sweeps(require_gpu, monkeypatch, 
     g2.close()
 
 
+@pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "1,20,1"])
+def test_odd_jp_sor_pass_shapes_equal_per_colour_sweeps(require_gpu, monkeypatch, shape):
+    # odd jp: rows jp and 1 are j-neighbours of the same colour, which read
+    # each other's value from before the half-sweep (press.f95's ghost rows);
+    # the one-iteration passes against the per-colour sweeps on a grid with
+    # several tiles in i, j and k, the wrap inside a tile's rows
+    from les_halo_b200 import abi
+    ip, jp, kp = 130, 97, 40
+    _, a = _pair(ip, jp, kp, seed=5)
+    b = a.copy()
+    monkeypatch.setenv("LES_SOR_TILE", shape)
+    g1, g2 = GpuLes(a), GpuLes(b)
+    abi.check(abi.lib().les_ctx_set_sor_path(g2.ctx, 1))
+    for g in (g1, g2):
+        g.warmup(1)
+        g.step(1, 3)
+    T, ty, _, nch = _sor_shape(g1)
+    assert (T, ty, nch) == tuple(int(x) for x in shape.split(","))
+    assert_bitexact(g1.download(ALL), g2.download(ALL), ip, jp, kp, ALL)
+    assert g1.metrics()["sor_iters"] == g2.metrics()["sor_iters"]
+    g1.close()
+    g2.close()
+
+
+@pytest.mark.parametrize("dims", [(70, 33, 10), (40, 9, 12), (36, 7, 8)])
+def test_odd_jp_against_oracle(require_gpu, dims):
+    # jp = 33 and 9 take one-iteration passes (9: the 8-row region of the
+    # shortest shape holds 8 of the 9 rows); jp = 7 is below every region
+    # and keeps the per-colour sweeps
+    from les_halo_b200 import abi
+    ip, jp, kp = dims
+    ref, dev = _pair(ip, jp, kp, seed=ip + jp)
+    gpu = GpuLes(dev)
+    oracle.ifdata(ref, 1)
+    gpu.warmup(1)
+    for n in range(1, 4):
+        iters = oracle.run_steps(ref, n, 1)
+        gpu.step(n, 1)
+        assert gpu.metrics()["sor_iters"] == iters[0]
+        _compare(gpu, ref)
+    per_launch = abi.lib().les_ctx_sor_iters_per_launch(gpu.ctx)
+    assert per_launch == (0.5 if jp < 8 else 1.0)
+    gpu.close()
+
+
 def _sor_shape(gpu):
     import ctypes as C
     from les_halo_b200 import abi
