@@ -278,7 +278,7 @@ def ensemble_bench(steps, warmup, ws=1, rank=0, dist=None):
     E = ENSEMBLE
     doms = ensemble_members()
     mine = shard_members([ip * jp * E["kp"] for ip, jp, _, _ in doms], ws)[rank]
-    err, ens_ms, cells, launches, seq_ms = None, float("nan"), 0, 0, None
+    err, ens_ms, cells, launches, seq_ms, tune = None, float("nan"), 0, 0, None, None
     members, ens = [], None
     try:
         for m in mine:
@@ -300,16 +300,29 @@ def ensemble_bench(steps, warmup, ws=1, rank=0, dist=None):
         torch.cuda.synchronize()
         ens_ms = e0.elapsed_time(e1)
         launches = ens.launches() - l0
+        tune = ens.tune_info()
         if ws == 1:
-            n, seq_ms = 1 + warmup + steps, 0.0
-            for g in members:  # one run after another
-                ms = torch.cuda.ExternalStream(g.stream())
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(ms)
-                g.step(n, steps)
-                b.record(ms)
-                torch.cuda.synchronize()
-                seq_ms += a.elapsed_time(b)
+            # 64 sequential plain runs: each member in a fresh context with
+            # its own autotuned SOR shape and its step graph captured by an
+            # untimed step first, one member after another
+            seq_ms = 0.0
+            for m in mine:
+                ip, jp, ustar, seed = doms[m]
+                case = lh.synthetic_case(ip, jp, E["kp"], seed=seed, dt=0.05, nmaxp=50, ustar=ustar)
+                g = lh.GpuLes(case)
+                try:
+                    g.warmup(1)
+                    g.step(1, 1)
+                    g.sync()
+                    ms = torch.cuda.ExternalStream(g.stream())
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(ms)
+                    g.step(2, steps)
+                    b.record(ms)
+                    torch.cuda.synchronize()
+                    seq_ms += a.elapsed_time(b)
+                finally:
+                    g.close()
     except Exception as exc:  # reported, never fatal to the headline line
         err = f"{type(exc).__name__}: {exc}"[:300]
     finally:
@@ -326,6 +339,7 @@ def ensemble_bench(steps, warmup, ws=1, rank=0, dist=None):
            "ensemble_mpts": round(cells_all * steps / (ens_ms / 1e3) / 1e6, 1),
            "ensemble_ms_per_step": round(ens_ms / steps, 3), "graph_launches_per_step": 1,
            "kernels_per_step_rank0": int(launches // max(steps, 1)),
+           "sor_shape_autotuner": tune,
            "config": f"ip,jp ~ U{{{E['size_lo']}..{E['size_hi']}}}, kp={E['kp']}, u* ~ "
                      f"U[{E['ustar_lo']},{E['ustar_hi']}], seed {E['seed']}"}
     if seq_ms is not None:

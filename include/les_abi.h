@@ -561,6 +561,13 @@ les_status les_ensemble_create(int nmembers, les_ctx *const *members, les_ensemb
 les_status les_ensemble_step(les_ensemble *ens, int n0, int nsteps);
 les_status les_ensemble_sync(les_ensemble *ens);
 void *les_ensemble_stream(les_ensemble *ens);
+/* The ensemble autotuner's record (after the first les_ensemble_step): the
+ * candidates' times in ms per four tuning passes of every member (cap
+ * entries at most; -1 where not run), their count and the index chosen.
+ * Candidate 0: each member's own shape; 1..5: one-iteration passes of
+ * (28, 1), (28, 2), (24, 1), (20, 1), (12, 1) tile rows and k chunks where a
+ * member can run them.  LES_ENSEMBLE_TUNE=own skips the tuner. */
+les_status les_ensemble_tune_info(les_ensemble *ens, float *ms, int cap, int *ncand, int *chosen);
 /* kernels launched by the ensemble so far (all members) */
 uint64_t les_ensemble_launch_count(les_ensemble *ens);
 les_status les_ensemble_destroy(les_ensemble *ens);

@@ -136,6 +136,8 @@ _SIGS = {
     "les_ensemble_step": (C.c_int, [_P, C.c_int, C.c_int]),
     "les_ensemble_sync": (C.c_int, [_P]),
     "les_ensemble_stream": (C.c_void_p, [_P]),
+    "les_ensemble_tune_info": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int)]),
     "les_ensemble_launch_count": (C.c_uint64, [_P]),
     "les_ensemble_destroy": (C.c_int, [_P]),
     "les_press_refine_fp64": (C.c_int, [_P, C.c_int, C.c_int, C.c_double]),

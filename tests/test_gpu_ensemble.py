@@ -30,6 +30,9 @@ def test_ensemble_equals_member_steps(require_gpu):
         g.step(1, 4)
     l1 = ens.launches()
     assert l1 > 0
+    ti = ens.tune_info()  # the ensemble autotuner ran once, at the first step
+    assert len(ti["candidates"]) == 6 and ti["chosen"] in ti["candidates"]
+    assert all(v > 0 for v in ti["candidates"].values())
     for (dims, _, _), a, b in zip(DOMAINS, members, solo):
         assert_bitexact(a.download(ALL), b.download(ALL), *dims, ALL)
         ma, mb = a.metrics(), b.metrics()
