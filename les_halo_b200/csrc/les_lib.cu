@@ -739,28 +739,37 @@ les_status autotune_sor(les_ctx *c) {
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         double best_t = 0.0;
-        const int rhs_[] = {8, 12, 16, 20, 24, 28, 32};
+        // candidates: region heights 8, 12, .., 32 rows, and per (T, k chunks)
+        // and wave count w = 1..4 the smallest tile height whose grid still
+        // fits in w waves of one CTA per SM (no partly filled last wave)
+        std::vector<TbShape> cand;
         for (int T = 1; T <= kTbTMax; ++T)
-            for (int ri = 0; ri < 7; ++ri)
-                for (int nch = 1; nch <= 4; nch *= 2) {
-                        TbShape sh;
-                        sh.T = T;
-                        sh.ty = rhs_[ri] - 2 * tb_ring(T);
-                        sh.nch = nch;
-                        if (sh.ty < 4 || (nch > 1 && cdiv(c->prm.kp, nch) < 8) || !tb_shape_ok(c, sh)) continue;
-                        CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
-                        les_status st = launch_sor_tb(c, sh, T, 0, -1.0f, INT_MAX, true);
-                        if (st != LES_OK) return st;
-                        CK(cudaEventRecord(e0, c->stream));
-                        for (int r = 0; r < 2; ++r)
-                            if ((st = launch_sor_tb(c, sh, T, 0, -1.0f, INT_MAX, true)) != LES_OK) return st;
-                        CK(cudaEventRecord(e1, c->stream));
-                        CK(cudaEventSynchronize(e1));
-                        float ms = 0.0f;
-                        CK(cudaEventElapsedTime(&ms, e0, e1));
-                        const double per_iter = ms / (2.0 * T);
-                        if (!best.T || per_iter < best_t) best_t = per_iter, best = sh;
-                    }
+            for (int nch = 1; nch <= 4; nch *= 2) {
+                for (int rh = 8; rh <= 32; rh += 4) cand.push_back(TbShape{T, rh - 2 * tb_ring(T), nch});
+                const long long gx = cdiv(c->prm.ip, tb_tx(T));
+                for (int w = 1; w <= 4; ++w)
+                    for (int ty = 4; ty + 2 * tb_ring(T) <= kTbMaxRH; ++ty)
+                        if (gx * cdiv(c->prm.jp, ty) * nch <= (long long)w * nsm) {
+                            if ((ty + 2 * tb_ring(T)) % 4) cand.push_back(TbShape{T, ty, nch});
+                            break;
+                        }
+            }
+        for (const TbShape &sh : cand) {
+            const int T = sh.T, nch = sh.nch;
+            if (sh.ty < 4 || (nch > 1 && cdiv(c->prm.kp, nch) < 8) || !tb_shape_ok(c, sh)) continue;
+            CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));
+            les_status st = launch_sor_tb(c, sh, T, 0, -1.0f, INT_MAX, true);
+            if (st != LES_OK) return st;
+            CK(cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < 2; ++r)
+                if ((st = launch_sor_tb(c, sh, T, 0, -1.0f, INT_MAX, true)) != LES_OK) return st;
+            CK(cudaEventRecord(e1, c->stream));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            const double per_iter = ms / (2.0 * T);
+            if (!best.T || per_iter < best_t) best_t = per_iter, best = sh;
+        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         CK(cudaMemsetAsync(c->d_scal, 0, sizeof(Scal), c->stream));

@@ -270,8 +270,8 @@ def test_upload_with_inconsistent_p_ghosts(require_gpu):
     gpu.close()
 
 
-@pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "2,16,1", "2,8,3", "3,8,2",
-                                   "3,4,1"])
+@pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "1,21,1", "2,16,1", "2,8,3", "2,13,2",
+                                   "3,8,2", "3,4,1"])
 def test_each_sor_pass_shape_equals_per_colour_sweeps(require_gpu, monkeypatch, shape):
     # shapes (iterations per pass, tile rows, k chunks) the
     # autotuner may pick, on a grid with several tiles in i, j and k
@@ -293,7 +293,7 @@ def test_each_sor_pass_shape_equals_per_colour_sweeps(require_gpu, monkeypatch, 
     g2.close()
 
 
-@pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "1,20,1"])
+@pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "1,20,1", "1,23,1"])
 def test_odd_jp_sor_pass_shapes_equal_per_colour_sweeps(require_gpu, monkeypatch, shape):
     # odd jp: rows jp and 1 are j-neighbours of the same colour, which read
     # each other's value from before the half-sweep (press.f95's ghost rows);
