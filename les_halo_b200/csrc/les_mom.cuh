@@ -438,9 +438,34 @@ __device__ __forceinline__ void visc_tile(const Geo &g, const TV &d, const ViscV
 // the face-value ring plane by plane, call `cell` for every tile cell.
 // `pre(k)` runs at the top of plane k's iteration: the cell's global inputs
 // loaded there arrive while the plane's face values are being filled.
+// The x and y tables a tile reads (dx1, rdx1, rsx at i = ib-1 .. ib+kMEX,
+// dy1, rdy1, rsy at j = jb-1 .. jb+kMEY), copied into shared memory at the
+// start of an interior tile's march; the Geo the march hands on points its
+// x/y tables there (same values, read from shared instead of global memory).
+constexpr int kTabX = kMEX + 2, kTabY = kMEY + 2;
+__device__ __forceinline__ void tile_tables(const Geo &g0, Geo &g, float *tab, int ib, int jb) {
+    const float *srcx[3] = {g0.dx1, g0.rdx1, g0.rsx}, *srcy[3] = {g0.dy1, g0.rdy1, g0.rsy};
+    for (int t = threadIdx.x; t < 3 * kTabX + 3 * kTabY; t += blockDim.x) {
+        if (t < 3 * kTabX)
+            tab[t] = srcx[t / kTabX][ib - 1 + t % kTabX];
+        else {
+            const int u = t - 3 * kTabX;
+            tab[t] = srcy[u / kTabY][jb - 1 + u % kTabY];
+        }
+    }
+    g = g0;
+    g.dx1 = tab - (ib - 1);
+    g.rdx1 = tab + kTabX - (ib - 1);
+    g.rsx = tab + 2 * kTabX - (ib - 1);
+    g.dy1 = tab + 3 * kTabX - (jb - 1);
+    g.rdy1 = tab + 3 * kTabX + kTabY - (jb - 1);
+    g.rsy = tab + 3 * kTabX + 2 * kTabY - (jb - 1);
+}
+
 template <bool DIU_ONLY, bool BAND, bool INTERIOR, bool P2, class PreFn, class CellFn>
-__device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn pre, CellFn cell) {
+__device__ __forceinline__ void mom_march(const Geo &g0, const Fields &F, PreFn pre, CellFn cell) {
     extern __shared__ float sh[];
+    __shared__ float tabs[3 * kTabX + 3 * kTabY];
     constexpr int NVU = DIU_ONLY ? 9 : NV;
     float *const s0 = sh, *const s1 = sh + NVU * kMPOS;  // the two face-value plane slots
     auto slot = [&](int x) { return x ? s1 : s0; };
@@ -448,6 +473,12 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
     float *band = prv8 + kMPOS;
     const int i0 = 1 + blockIdx.x * kMX, j0 = 1 + blockIdx.y * kMY;
     const int ib = i0 - 1, jb = j0 - 1;
+    Geo gl;
+    if (BAND && INTERIOR)
+        tile_tables(g0, gl, tabs, ib, jb);  // read after the first barrier below
+    else
+        gl = g0;
+    const Geo &g = gl;
     const UVW qg{{}, F.u, F.v, F.w};
     const UVWBand qb{{}, band, i0 - 2, j0 - 2};
     auto fill = [&](float *dst, int k, bool save) {
@@ -551,7 +582,7 @@ __device__ __forceinline__ void mom_march(const Geo &g, const Fields &F, PreFn p
             __syncthreads();
             vv = ViscView{sm_slot(k), S1, vXY, vFXY, vXZ + ((k + 1) & 1) * kMPOS, XZ, vYZ};
         }
-        cell(t, k, vv);
+        cell(g, t, k, vv);
         if (BAND || DIU_ONLY) cp_async_wait<0>();
         __syncthreads();
     }
@@ -588,7 +619,7 @@ __global__ void __launch_bounds__(kMNT) k_mom1(Geo g, Fields F) {
         cm0 = __ldg(&F.cmask[c]);
         dm0 = __ldg(&F.dmask[c]);
     };
-    auto cell = [&](const TileView<P2> &t, int k, const ViscView &) {
+    auto cell = [&](const Geo &g, const TileView<P2> &t, int k, const ViscView &) {
         if (!mine) return;
         const int c = IX(g, i, j, k);
         float fv, gv, hv = h0;
@@ -642,7 +673,7 @@ __global__ void __launch_bounds__(kMNT, 3) k_mom2(Geo g, Fields F) {
             ho0 = F.hold[c];
         }
     };
-    auto cell = [&](const TileView<P2> &t, int k, const ViscView &vv) {
+    auto cell = [&](const Geo &g, const TileView<P2> &t, int k, const ViscView &vv) {
         if (!mine) return;
         float vfu, vfv, vfw;
         visc_tile(g, t, vv, i, j, k, vfu, vfv, vfw);
