@@ -280,8 +280,16 @@ __global__ void __launch_bounds__(kRedNT) k_pav_adjust(Geo g, float *p, const fl
     if (i > g.im || j > g.jm) return;
     const float *src = s->pbuf ? p1 : p;
     const float pav = s->pav;
-    for (int k = k0; k <= k1; ++k) {
-        const float val = src[IX(g, i, j, k)] - pav;
+    // the chunk's loads first (kchunk <= kRedKMax): the stores below write
+    // this thread's own cells and ghosts only, which no thread reads here
+    float pv[kRedKMax];
+#pragma unroll
+    for (int q = 0; q < kRedKMax; ++q) pv[q] = (k0 + q <= k1) ? src[IX(g, i, j, k0 + q)] : 0.0f;
+#pragma unroll
+    for (int q = 0; q < kRedKMax; ++q) {
+        const int k = k0 + q;
+        if (k > k1) break;
+        const float val = pv[q] - pav;
         // the cell and its boundp1/boundp2 copies: at most one extra i, j and k
         // (im, jm >= 2, km >= 3)
         const int ie = (i == 1) ? 0 : (i == g.im ? g.im + 1 : -9);
