@@ -660,7 +660,7 @@ def run_ours(args):
             line["ensemble"] = ens_line
         if not args.profile and not args.no_adjoint and ws == 1:
             line["adjoint"] = adjoint_bench()
-        if not args.profile and args.refine and ws == 1:
+        if not args.profile and args.refine and not args.no_config2 and ws == 1:
             line["config2_refined_press"] = config2_bench()
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
@@ -684,6 +684,8 @@ def main():
                     help="skip the 64-domain ensemble measurement")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (config-3) cost measurement")
+    ap.add_argument("--no-config2", action="store_true",
+                    help="skip the 1000x1000x150 refined-press measurement")
     ap.add_argument("--profile", action="store_true",
                     help="no in-graph timing events (for runs under ncu)")
     ap.add_argument("--grid", default=None,

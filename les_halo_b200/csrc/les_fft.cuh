@@ -32,6 +32,7 @@ namespace les {
 namespace {
 
 constexpr int kFftMaxStages = 24, kFftMaxRadix = 13, kFftThreads = 256, kFftPoints = 2048;
+constexpr int kLoadBatch = 8;  // global loads of a thread issued together
 
 struct FftPlan {
     int n, nstage;
@@ -103,6 +104,84 @@ __device__ __forceinline__ void small_dft(double2 (&v)[R]) {
     }
 }
 
+// Roots w_R^e = exp(-2 pi i e / R) of the composite radices 6, 8, 10 as
+// exact constants (cos and sin of multiples of 60, 45 and 36 degrees).
+constexpr double kS2 = 0.70710678118654752440;  // sqrt(2) / 2
+template <int R, int E>
+__device__ __forceinline__ constexpr double2 root_c() {
+    constexpr int e = E % R;
+    if constexpr (R == 6) {
+        constexpr double re[6] = {1.0, 0.5, -0.5, -1.0, -0.5, 0.5};
+        constexpr double im[6] = {0.0, -kS3, -kS3, 0.0, kS3, kS3};
+        return make_double2(re[e], im[e]);
+    } else if constexpr (R == 8) {
+        constexpr double re[8] = {1.0, kS2, 0.0, -kS2, -1.0, -kS2, 0.0, kS2};
+        constexpr double im[8] = {0.0, -kS2, -1.0, -kS2, 0.0, kS2, 1.0, kS2};
+        return make_double2(re[e], im[e]);
+    } else {  // 10: cos 36 = -c52, sin 36 = s52, cos 72 = c51, sin 72 = s51
+        constexpr double re[10] = {1.0, -kC52, kC51, -kC51, kC52, -1.0, kC52, -kC51, kC51, -kC52};
+        constexpr double im[10] = {0.0, -kS52, -kS51, -kS51, -kS52, 0.0, kS52, kS51, kS51, kS52};
+        return make_double2(re[e], im[e]);
+    }
+}
+
+// x * w_R^E, the trivial roots (1, -1, -i, i) without arithmetic.
+template <int R, int E>
+__device__ __forceinline__ double2 mul_root(double2 x) {
+    constexpr int e = E % R;
+    if constexpr (e == 0) {
+        return x;
+    } else if constexpr (2 * e == R) {
+        return make_double2(-x.x, -x.y);
+    } else if constexpr (4 * e == R) {  // -i
+        return make_double2(x.y, -x.x);
+    } else if constexpr (4 * e == 3 * R) {  // i
+        return make_double2(-x.y, x.x);
+    } else {
+        return cmul(x, root_c<R, E>());
+    }
+}
+
+// Length R1 R2 DFT of v in place (Cooley-Tukey): Y[r2][k1] = DFT_R1 over r1
+// of v[R2 r1 + r2], times w_R^(r2 k1); then X[k1 + R1 k2] = DFT_R2 over r2
+// of Y[r2][k1].  All indices compile-time: the values stay in registers.
+template <int R1, int R2>
+__device__ __forceinline__ void dft_comp(double2 (&v)[R1 * R2]) {
+    constexpr int R = R1 * R2;
+    double2 y[R];
+#pragma unroll
+    for (int r2 = 0; r2 < R2; ++r2) {
+        double2 t[R1];
+#pragma unroll
+        for (int r1 = 0; r1 < R1; ++r1) t[r1] = v[R2 * r1 + r2];
+        small_dft<R1>(t);
+        y[r2 * R1] = t[0];
+#pragma unroll
+        for (int k1 = 1; k1 < R1; ++k1) {
+            double2 z = t[k1];
+            // exponent r2 k1 (compile-time after unrolling)
+            switch (r2 * k1) {
+#define LES_ROOT_CASE(E) \
+    case E: z = mul_root<R, E>(z); break;
+                LES_ROOT_CASE(0) LES_ROOT_CASE(1) LES_ROOT_CASE(2) LES_ROOT_CASE(3) LES_ROOT_CASE(4)
+                LES_ROOT_CASE(5) LES_ROOT_CASE(6) LES_ROOT_CASE(7) LES_ROOT_CASE(8) LES_ROOT_CASE(9)
+#undef LES_ROOT_CASE
+                default: break;
+            }
+            y[r2 * R1 + k1] = z;
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        double2 t[R2];
+#pragma unroll
+        for (int r2 = 0; r2 < R2; ++r2) t[r2] = y[r2 * R1 + k1];
+        small_dft<R2>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+    }
+}
+
 // One Stockham stage of radix R over npts points (whole lines), a -> b.
 // The twiddles of butterfly k of the stage are tws[(r - 1) Ns + k],
 // r = 1..R-1: consecutive k, consecutive addresses.
@@ -123,6 +202,10 @@ __device__ __forceinline__ void fft_stage(const FftPlan &P, const double2 *a, do
         double2 *dst = b + line * n + (j - k) * R + k;
         if constexpr (R <= 5) {
             small_dft<R>(v);
+#pragma unroll
+            for (int r = 0; r < R; ++r) dst[r * Ns] = v[r];
+        } else if constexpr (R == 6 || R == 8 || R == 10) {
+            dft_comp<(R == 8 ? 4 : 2), (R == 8 ? 2 : R / 2)>(v);
 #pragma unroll
             for (int r = 0; r < R; ++r) dst[r * Ns] = v[r];
         } else {  // V_q = sum_r v_r root^(r q), root = w^(n/R), each stored as it is summed
@@ -163,6 +246,9 @@ __device__ __forceinline__ double2 *fft_stages(const FftPlan &P, double2 *a, dou
             case 3: fft_stage<3>(P, a, b, npts, Ns, tws); break;
             case 4: fft_stage<4>(P, a, b, npts, Ns, tws); break;
             case 5: fft_stage<5>(P, a, b, npts, Ns, tws); break;
+            case 6: fft_stage<6>(P, a, b, npts, Ns, tws); break;
+            case 8: fft_stage<8>(P, a, b, npts, Ns, tws); break;
+            case 10: fft_stage<10>(P, a, b, npts, Ns, tws); break;
             case 7: fft_stage_call<7>(P, a, b, npts, Ns, tws); break;
             case 11: fft_stage_call<11>(P, a, b, npts, Ns, tws); break;
             default: fft_stage_call<13>(P, a, b, npts, Ns, tws); break;
@@ -189,13 +275,26 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_fft_r2c(const __grid_constan
     constexpr int nwarp = kFftThreads / 32;
     double2 *za = fsm, *zb = fsm + P.lpb * n;
     double *zr = reinterpret_cast<double *>(za);
+    const float rn = 1.0f / (float)n;
     for (int p0 = blockIdx.x * P.lpb; p0 < npair; p0 += gridDim.x * P.lpb) {
-        const int pairs = min(P.lpb, npair - p0);
-        for (int l = warp; l < 2 * pairs; l += nwarp) {
-            const double *src = in + (size_t)(2 * p0 + l) * n;
-            double *dz = zr + (l >> 1) * 2 * n + (l & 1);
-#pragma unroll 4
-            for (int i = lane; i < n; i += 32) dz[2 * i] = src[i];
+        const int pairs = min(P.lpb, npair - p0), tot = 2 * pairs * n;
+        const double *src = in + (size_t)2 * p0 * n;
+        // the group's lines, kLoadBatch loads of each thread in flight at a time
+        for (int t0 = threadIdx.x; t0 < tot; t0 += kLoadBatch * kFftThreads) {
+            double x[kLoadBatch];
+#pragma unroll
+            for (int q = 0; q < kLoadBatch; ++q) {
+                const int t = t0 + q * kFftThreads;
+                x[q] = t < tot ? src[t] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < kLoadBatch; ++q) {
+                const int t = t0 + q * kFftThreads;
+                if (t < tot) {
+                    const int line = fdiv_small(t, n, rn), i = t - line * n;
+                    zr[2 * ((line >> 1) * n + i) + (line & 1)] = x[q];
+                }
+            }
         }
         __syncthreads();
         const double2 *res = fft_stages(P, za, zb, pairs * n);
@@ -224,20 +323,36 @@ __global__ void __launch_bounds__(kFftThreads, 3) k_fft_c2r(const __grid_constan
     const int n = P.n, nh = n / 2 + 1, npair = nlines / 2, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarp = kFftThreads / 32;
     double2 *za = fsm, *zb = fsm + P.lpb * n;
+    const float rnh = 1.0f / (float)nh;
     for (int p0 = blockIdx.x * P.lpb; p0 < npair; p0 += gridDim.x * P.lpb) {
-        const int pairs = min(P.lpb, npair - p0);
-        // conj Z_m, Z_m = A_m + i B_m; for m > n/2, A_m = conj A_{n-m}, B_m = conj B_{n-m}
-        for (int p = warp; p < pairs; p += nwarp) {
-            const double2 *A = in + (size_t)2 * (p0 + p) * nh, *B = A + nh;
-            double2 *z = za + p * n;
-#pragma unroll 2
-            for (int m = lane; m < nh; m += 32) {
-                const double2 x = A[m], y = B[m];
-                if (m == 0 || 2 * m == n) {
-                    z[m] = make_double2(x.x, -y.x);
-                } else {
-                    z[m] = make_double2(x.x - y.y, -(x.y + y.x));
-                    z[n - m] = make_double2(x.x + y.y, x.y - y.x);
+        const int pairs = min(P.lpb, npair - p0), tot = pairs * nh;
+        // conj Z_m, Z_m = A_m + i B_m; for m > n/2, A_m = conj A_{n-m}, B_m = conj B_{n-m};
+        // kLoadBatch / 2 (A, B) pairs of loads of each thread in flight at a time
+        for (int t0 = threadIdx.x; t0 < tot; t0 += (kLoadBatch / 2) * kFftThreads) {
+            double2 xa[kLoadBatch / 2], xb[kLoadBatch / 2];
+#pragma unroll
+            for (int q = 0; q < kLoadBatch / 2; ++q) {
+                const int t = t0 + q * kFftThreads;
+                if (t < tot) {
+                    const int p = fdiv_small(t, nh, rnh), m = t - p * nh;
+                    const double2 *A = in + (size_t)2 * (p0 + p) * nh;
+                    xa[q] = A[m];
+                    xb[q] = A[nh + m];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kLoadBatch / 2; ++q) {
+                const int t = t0 + q * kFftThreads;
+                if (t < tot) {
+                    const int p = fdiv_small(t, nh, rnh), m = t - p * nh;
+                    const double2 x = xa[q], y = xb[q];
+                    double2 *z = za + p * n;
+                    if (m == 0 || 2 * m == n) {
+                        z[m] = make_double2(x.x, -y.x);
+                    } else {
+                        z[m] = make_double2(x.x - y.y, -(x.y + y.x));
+                        z[n - m] = make_double2(x.x + y.y, x.y - y.x);
+                    }
                 }
             }
         }
@@ -266,7 +381,7 @@ inline int fft_plan(int n, int nsm, FftPlan &P) {
     if (n < 2 || n % 2 || n > kFftPoints) return -1;
     P.n = n;
     int m = n, ofs = 0, Ns = 1;
-    for (int r : {4, 5, 3, 2, 7, 11, 13})
+    for (int r : {10, 8, 6, 4, 5, 3, 2, 7, 11, 13})
         while (m % r == 0 && m > 1) {
             if (P.nstage == kFftMaxStages) return -1;
             P.tofs[P.nstage] = ofs;

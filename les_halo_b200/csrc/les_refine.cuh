@@ -118,22 +118,28 @@ __global__ void __launch_bounds__(kRedNT) k_ref_defect(Geo g, const float *rhs, 
     const int k1 = min(g.km, k0 + kchunk - 1);
     double2 acc = make_double2(0.0, 0.0);
     if (i <= g.im && j <= g.jm && !(R->stop && !FIRST)) {
-        const float *p32 = sc->pbuf ? p1 : p0;
+        // the defect's outputs (rline or r32, and p64 below) are no location
+        // the loop reads
+        const float *__restrict__ p32 = sc->pbuf ? p1 : p0;
+        const double *__restrict__ p64r = p64;
+        double *__restrict__ rl = rline;
+        float *__restrict__ r32o = r32;
         const int jn = (j == g.jm) ? 1 : j + 1, js = (j == 1) ? g.jm : j - 1;
         const double c2l = g.cn2l[i], c2s = g.cn2s[i], c3l = g.cn3l[j], c3s = g.cn3s[j];
         const double bsh = R->bshift;
+        auto P = [&](int ii, int jj, int kk) -> double {
+            const int c = IX(g, ii, jj, kk);
+            return FIRST ? (double)p32[c] : p64r[c];
+        };
+        // the k neighbours move through registers from one plane to the next
+        double pc = P(i, j, k0);
+        double pd = (k0 == 1) ? pc : P(i, j, k0 - 1);
         for (int k = k0; k <= k1; ++k) {
-            auto P = [&](int ii, int jj, int kk) -> double {
-                const int c = IX(g, ii, jj, kk);
-                return FIRST ? (double)p32[c] : p64[c];
-            };
             const int c = IX(g, i, j, k);
-            const double pc = P(i, j, k);
             const double pe = (i == g.im) ? pc : P(i + 1, j, k);
             const double pw = (i == 1) ? pc : P(i - 1, j, k);
             const double pn = P(i, jn, k), ps = P(i, js, k);
             const double pu = (k == g.km) ? pc : P(i, j, k + 1);
-            const double pd = (k == 1) ? pc : P(i, j, k - 1);
             const double c4l = g.cn4l[k], c4s = g.cn4s[k];
             const double diag = ((((c2l + c2s) + c3l) + c3s) + c4l) + c4s;
             double s = c2l * pe;
@@ -146,11 +152,13 @@ __global__ void __launch_bounds__(kRedNT) k_ref_defect(Geo g, const float *rhs, 
             const double b = (double)rhs[c] - bsh;
             const double r = b - ap;
             if (SPEC)
-                rline[((size_t)(k - 1) * g.jm + (j - 1)) * g.im + makhoul_pos(i, g.im)] = r;
+                rl[((size_t)(k - 1) * g.jm + (j - 1)) * g.im + makhoul_pos(i, g.im)] = r;
             else
-                r32[c] = (float)r;
+                r32o[c] = (float)r;
             acc.x += r * r;
             if (FIRST) acc.y += b * b;
+            pd = pc;
+            pc = pu;
         }
     }
     // FIRST stores p64 only after every read of this block is done: other

@@ -153,7 +153,8 @@ __global__ void __launch_bounds__(128) k_spec_tridiag(double2 *__restrict__ Y, d
 }
 
 // p64 += scale * e on the interior, e from the inverse transforms' lines.
-__global__ void __launch_bounds__(kRedNT) k_spec_correct(Geo g, double *p64, const double *v, double scale, Ref64 *R) {
+__global__ void __launch_bounds__(kRedNT) k_spec_correct(Geo g, double *__restrict__ p64, const double *__restrict__ v,
+                                                          double scale, Ref64 *R) {
     if (R->stop) return;
     const int i = 1 + blockIdx.x * kRedBX + threadIdx.x;
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
