@@ -45,32 +45,31 @@ __global__ void k_adj_boundp2(Geo g, float *pb) {
     a0 = 0.0f;
 }
 
-// boundp1 transposed, second loop (boundp.f95:36-42): p(i,0,k) = p(i,jm,k),
-// then p(i,jm+1,k) = p(i,1,k), for i = 0..im+1, k = 0..km+1.
-__global__ void k_adj_boundp1_j(Geo g, float *pb) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x, ni = g.im + 2;
-    if (t >= ni * (g.km + 2)) return;
-    const int i = t % ni, k = t / ni;
-    float &a0 = pb[IX(g, i, 0, k)], &a1 = pb[IX(g, i, 1, k)];
-    float &am = pb[IX(g, i, g.jm, k)], &am1 = pb[IX(g, i, g.jm + 1, k)];
-    a1 += am1;
-    am1 = 0.0f;
-    am += a0;
-    a0 = 0.0f;
-}
-
-// boundp1 transposed, first loop (boundp.f95:28-34): p(0,j,k) = p(1,j,k),
-// then p(im+1,j,k) = p(im,j,k), for j = 0..jm+1, k = 0..km+1.
-__global__ void k_adj_boundp1_i(Geo g, float *pb) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x, nj = g.jm + 2;
-    if (t >= nj * (g.km + 2)) return;
-    const int j = t % nj, k = t / nj;
-    float &a0 = pb[IX(g, 0, j, k)], &a1 = pb[IX(g, 1, j, k)];
-    float &am = pb[IX(g, g.im, j, k)], &am1 = pb[IX(g, g.im + 1, j, k)];
-    am += am1;
-    am1 = 0.0f;
-    a1 += a0;
-    a0 = 0.0f;
+// boundp1 transposed (boundp.f95:23-44), one block per plane k = 0..km+1:
+// the second loop's copies first (p(i,0,k) = p(i,jm,k), then
+// p(i,jm+1,k) = p(i,1,k), i = 0..im+1: in reverse, row jm+1 into row 1, row 0
+// into row jm), then, after the block's barrier, the first loop's
+// (p(0,j,k) = p(1,j,k), then p(im+1,j,k) = p(im,j,k), j = 0..jm+1: column
+// im+1 into column im, column 0 into column 1).
+__global__ void __launch_bounds__(256) k_adj_boundp1(Geo g, float *pb) {
+    const int k = blockIdx.x;
+    for (int i = threadIdx.x; i <= g.im + 1; i += blockDim.x) {
+        float &a0 = pb[IX(g, i, 0, k)], &a1 = pb[IX(g, i, 1, k)];
+        float &am = pb[IX(g, i, g.jm, k)], &am1 = pb[IX(g, i, g.jm + 1, k)];
+        a1 += am1;
+        am1 = 0.0f;
+        am += a0;
+        a0 = 0.0f;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j <= g.jm + 1; j += blockDim.x) {
+        float &a0 = pb[IX(g, 0, j, k)], &a1 = pb[IX(g, 1, j, k)];
+        float &am = pb[IX(g, g.im, j, k)], &am1 = pb[IX(g, g.im + 1, j, k)];
+        am += am1;
+        am1 = 0.0f;
+        a1 += a0;
+        a0 = 0.0f;
+    }
 }
 
 // One SOR half-sweep of colour nrd transposed: in -> out over p's range;
