@@ -451,7 +451,8 @@ def adjoint_bench():
         Jg, g = lh.tke_gradient(gpu, adj, 1, nt, box, ckpt)
         gpu.sync()
         grad_s = time.perf_counter() - t0
-        return {"config": f"{A['ip']}x{A['jp']}x{A['kp']}, {nt} steps (SOR 50 each), checkpoint every {ckpt}, "
+        return {"config": f"{A['ip']}x{A['jp']}x{A['kp']}, {nt} steps (SOR 50 each), checkpoint every {ckpt} "
+                          "(the last segment's step inputs kept from the forward run, the others recomputed), "
                           f"J = time-mean resolved TKE of box i{box[0]} j{box[1]} k{box[2]}; gradients: inflow "
                           "profile (jp x kp), drag scale (ip x jp), initial state",
                 "J": J, "J_in_gradient_run": Jg, "forward_s": round(fwd_s, 4), "gradient_s": round(grad_s, 4),

@@ -289,13 +289,20 @@ def set_drag(gpu: GpuLes, drag):
     abi.check(abi.lib().les_ctx_set_drag(gpu.ctx, FL.ptr(d) if d is not None else None))
 
 
-def tke_forward(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int) -> float:
+def tke_forward(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int, keep_last: bool = False) -> float:
     """J = (1/nt) sum over steps n0 .. n0+nt-1 of the resolved TKE of box
     after the step, from the context's current state, keeping a checkpoint
-    every ckpt steps in slots 0, 1, .. (slot 0: the initial state)."""
+    every ckpt steps in slots 0, 1, .. (slot 0: the initial state).  With
+    keep_last, the inputs of the last segment's steps also go to the slots
+    tke_reverse recomputes them into (ceil(nt/ckpt) ...), so that it need not
+    recompute that segment."""
+    nck = -(-nt // ckpt)
+    tl = (nck - 1) * ckpt  # first step of the last segment
     adj.save(0)
     J = 0.0
     for t in range(nt):
+        if keep_last and t >= tl:
+            adj.save(nck + t - tl)
         gpu.step(n0 + t, 1)
         J += adj.tke(-1, box) / nt
         if (t + 1) % ckpt == 0 and t + 1 < nt:
@@ -303,22 +310,25 @@ def tke_forward(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int) 
     return J
 
 
-def tke_reverse(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int) -> dict:
+def tke_reverse(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int, last_kept: bool = False) -> dict:
     """The gradient of tke_forward's J (same arguments, run just before):
     the step adjoint backwards over the checkpoints, each segment's step
-    inputs recomputed from its checkpoint into slots ceil(nt/ckpt) ...  The
-    context is left at the end of the first segment.  Returns the FP64
-    gradients of the inflow profile ("wp", jp x kp) and the drag scale
-    ("drag", ip x jp; zero unless set) and the adjoint of the initial state."""
+    inputs recomputed from its checkpoint into slots ceil(nt/ckpt) ... (the
+    last segment's taken as tke_forward left them when it ran with
+    keep_last and last_kept is set).  The context is left at the end of the
+    first segment.  Returns the FP64 gradients of the inflow profile ("wp",
+    jp x kp) and the drag scale ("drag", ip x jp; zero unless set) and the
+    adjoint of the initial state."""
     nck = -(-nt // ckpt)
     assert adj.nslots >= nck + ckpt, "too few slots"
     adj.zero()
     for seg in reversed(range(nck)):
         t0, t1 = seg * ckpt, min(seg * ckpt + ckpt, nt)
-        adj.load(seg)
-        for t in range(t0, t1):
-            adj.save(nck + t - t0)
-            gpu.step(n0 + t, 1)
+        if not (last_kept and seg == nck - 1):  # else the context still holds the state after step t1-1
+            adj.load(seg)
+            for t in range(t0, t1):
+                adj.save(nck + t - t0)
+                gpu.step(n0 + t, 1)
         for t in reversed(range(t0, t1)):
             adj.seed_tke(-1 if t == t1 - 1 else nck + t + 1 - t0, box, 1.0 / nt)
             adj.step_b(n0 + t, nck + t - t0)
@@ -326,10 +336,11 @@ def tke_reverse(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int) 
 
 
 def tke_gradient(gpu: GpuLes, adj: GpuAdjoint, n0: int, nt: int, box, ckpt: int):
-    """tke_forward then tke_reverse: (J, gradients).  Needs ceil(nt/ckpt) +
-    ckpt slots."""
-    J = tke_forward(gpu, adj, n0, nt, box, ckpt)
-    return J, tke_reverse(gpu, adj, n0, nt, box, ckpt)
+    """tke_forward then tke_reverse: (J, gradients), the last segment's step
+    inputs kept from the forward run instead of recomputed.  Needs
+    ceil(nt/ckpt) + ckpt slots."""
+    J = tke_forward(gpu, adj, n0, nt, box, ckpt, keep_last=True)
+    return J, tke_reverse(gpu, adj, n0, nt, box, ckpt, last_kept=True)
 
 
 class Ensemble:
