@@ -607,6 +607,8 @@ def run_ours(args):
     sh = [C.c_int() for _ in range(4)]
     abi.check(L.les_ctx_sor_shape(gpu.ctx, *[C.byref(x) for x in sh]))
     tT, tY, tX, tK = (x.value for x in sh)
+    rw = C.c_int()
+    abi.check(L.les_ctx_sor_rows(gpu.ctx, C.byref(rw)))
     achieved = SOR_BYTES_PER_CELL_PER_ITER * ipl * cells / (sor_launch_ms / 1e3) / 1e9
     step_gbs = STEP_BYTES_PER_CELL * cells / (ms_step / 1e3) / 1e9
     traffic = None
@@ -629,7 +631,8 @@ def run_ours(args):
             "config": {"workload": workload_desc(case.ip, case.jp, case.kp),
                        "grid": [case.ip, case.jp, case.kp], "sor_iters": int(m["sor_iters"]),
                        "parallelism": f"replicas x{ws}",
-                       "sor_tile": {"iters_per_pass": tT, "rows": tY, "cols": tX, "k_chunks": tK},
+                       "sor_tile": {"iters_per_pass": tT, "rows": tY, "cols": tX, "k_chunks": tK,
+                                    "rows_per_warp": rw.value},
                        "l2": "inputs larger than L2 (19 state fields, 3.5 GB)"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "k_sor_tb" if ipl >= 1 else "k_sor_colour",

@@ -175,6 +175,10 @@ les_status les_ctx_sor_tile(les_ctx *ctx, int *iters_per_pass, int *tile_rows);
 /* The full pass shape: tile columns and k chunks too. */
 les_status les_ctx_sor_shape(les_ctx *ctx, int *iters_per_pass, int *tile_rows, int *tile_cols,
                              int *k_chunks);
+/* Region rows per warp of the chosen pass (1, or 2 for one-iteration passes
+ * with two rows per warp; 0 before the first step that uses a pass).
+ * LES_SOR_TILE=T,rows,chunks[,rows per warp] forces a shape. */
+les_status les_ctx_sor_rows(les_ctx *ctx, int *rows_per_warp);
 les_status les_ctx_phase_times(les_ctx *ctx, int slot, float *ms, int n);
 
 /* Device state access for callers that keep fields on the GPU.  The field

@@ -107,6 +107,7 @@ _SIGS = {
     "les_ctx_sor_iters_per_launch": (C.c_float, [_P]),
     "les_ctx_sor_tile": (C.c_int, [_P, _I, _I]),
     "les_ctx_sor_shape": (C.c_int, [_P, _I, _I, _I, _I]),
+    "les_ctx_sor_rows": (C.c_int, [_P, _I]),
     "les_ctx_phase_times": (C.c_int, [_P, C.c_int, _F, C.c_int]),
     "les_ctx_field": (C.c_int, [_P, C.c_int, C.POINTER(C.c_void_p), _I, _I, _I, _I]),
     "les_ctx_halo_floats": (C.c_size_t, [_P, C.c_int]),

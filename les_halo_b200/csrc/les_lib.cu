@@ -24,6 +24,7 @@
 #include "les_routines.cuh"
 #include "les_sor_tb.cuh"
 #include "les_sor1.cuh"
+#include "les_sor1p.cuh"
 #include "les_stats.cuh"
 #include "les_refine.cuh"
 #include "les_spectral.cuh"
@@ -151,6 +152,7 @@ TableLayout table_layout(int ip, int jp, int kp) {
 // k chunks.
 struct TbShape {
     int T = 0, ty = 0, nch = 1;
+    int rows = 1;  // region rows per warp: 2 takes k_sor1p (T = 1, ty + 4 even)
 };
 
 struct SpecState;  // spectral solve of the refined press (les_refine.inc)
@@ -577,9 +579,9 @@ les_status check_params(const les_params *p) {
 // LES_SOR_SUMS not set to "exact".
 bool tb_fast_ok(const les_ctx *c, const TbShape &sh) {
     if (sh.T > 2 || !c->sor_fp32_test || !(c->prm.pjuge < 0x1p40f)) return false;
-    const int kc = cdiv(c->prm.kp, sh.nch), nt = 32 * tb_warps(sh.T, sh.ty);
+    const int kc = cdiv(c->prm.kp, sh.nch), nt = 32 * tb_warps(sh.T, sh.ty) / sh.rows;
     const long long nblk = (long long)cdiv(c->prm.ip, tb_tx(sh.T)) * cdiv(c->prm.jp, sh.ty) * cdiv(c->prm.kp, kc);
-    const long long depth = 4LL * kc + 2 * (5 + nt / 32) + (nblk + nt - 1) / nt;
+    const long long depth = 4LL * sh.rows * kc + 2 * (5 + nt / 32) + (nblk + nt - 1) / nt;
     return depth <= (1LL << 16);
 }
 
@@ -591,7 +593,7 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
                          const SorBufs *bufs) {
     const int kc = cdiv(c->prm.kp, sh.nch);
     const dim3 grid(cdiv(c->prm.ip, tb_tx(sh.T)), cdiv(c->prm.jp, sh.ty), cdiv(c->prm.kp, kc));
-    const dim3 block(32 * tb_warps(sh.T, sh.ty));
+    const dim3 block(32 * tb_warps(sh.T, sh.ty) / sh.rows);
     const size_t sm = tb_smem(sh.T, sh.ty);
     TbArgs a;
     a.pb0 = tuning ? c->d_p2 : c->F.p;
@@ -615,6 +617,21 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     }
     const Geo &g = c->geo;
 #define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a, c->kq)
+    if (sh.rows == 2) {  // T = 1 (tb_shape_ok)
+        const size_t smp = s1_smem(sh.ty);
+        if (c->prm.jp % 2) {
+            if (c->cn1_by_k)
+                LAUNCH_SMEM(c, (k_sor1p<true, true>), grid, block, smp, g, a, c->kq);
+            else
+                LAUNCH_SMEM(c, (k_sor1p<false, true>), grid, block, smp, g, a, c->kq);
+        } else {
+            if (c->cn1_by_k)
+                LAUNCH_SMEM(c, (k_sor1p<true, false>), grid, block, smp, g, a, c->kq);
+            else
+                LAUNCH_SMEM(c, (k_sor1p<false, false>), grid, block, smp, g, a, c->kq);
+        }
+        return LES_OK;
+    }
     switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
         case 2:
             if (c->prm.jp % 2)
@@ -666,6 +683,16 @@ les_status set_tb_smem_attrs() {
     }
     S1A(false, false) S1A(true, false) S1A(false, true) S1A(true, true)
 #undef S1A
+#define S1PA(KT, JO)                                                                                \
+    {                                                                                               \
+        cudaFuncAttributes fa;                                                                      \
+        CK(cudaFuncGetAttributes(&fa, k_sor1p<KT, JO>));                                            \
+        const int mx = optin - (int)fa.sharedSizeBytes;                                             \
+        CK(cudaFuncSetAttribute(k_sor1p<KT, JO>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+        lim = std::min(lim, mx);                                                                    \
+    }
+    S1PA(false, false) S1PA(true, false) S1PA(false, true) S1PA(true, true)
+#undef S1PA
 #define S2A(KT)                                                                                \
     {                                                                                          \
         cudaFuncAttributes fa;                                                                 \
@@ -694,6 +721,7 @@ std::mutex g_tune_mu;
 // memory and the partial-sum array.
 bool tb_shape_ok(const les_ctx *c, const TbShape &sh) {
     if (!tb_fits(sh.T, sh.ty) || sh.nch < 1 || sh.nch > kTbMaxChunks) return false;
+    if (sh.rows != 1 && (sh.rows != 2 || sh.T != 1 || tb_rh(1, sh.ty) % 2)) return false;
     // odd jp: one iteration per pass (k_sor1), each real row once in a region
     if ((c->prm.jp % 2) != 0 && (sh.T != 1 || tb_rh(1, sh.ty) > c->prm.jp)) return false;
     const size_t smem = sh.T == 1 ? s1_smem(sh.ty) : (sh.T == 2 ? s2_smem(sh.ty) : tb_smem(sh.T, sh.ty));
@@ -716,7 +744,7 @@ les_status autotune_sor(les_ctx *c) {
     const TuneKey key{c->prm.ip, c->prm.jp, c->prm.kp, nsm};
     TbShape best;
     if (const char *ov = std::getenv("LES_SOR_TILE")) {  // taken where this grid can run it
-        std::sscanf(ov, "%d,%d,%d", &best.T, &best.ty, &best.nch);
+        std::sscanf(ov, "%d,%d,%d,%d", &best.T, &best.ty, &best.nch, &best.rows);
         if (!tb_shape_ok(c, best)) best = TbShape{};
     }
     if (!best.T) {
@@ -729,7 +757,7 @@ les_status autotune_sor(les_ctx *c) {
         if (FILE *fp = std::fopen(cache, "r")) {
             int a, b, cc, d;
             TbShape sh;
-            while (std::fscanf(fp, "%d %d %d %d %d %d %d", &a, &b, &cc, &d, &sh.T, &sh.ty, &sh.nch) == 7)
+            while (std::fscanf(fp, "%d %d %d %d %d %d %d %d", &a, &b, &cc, &d, &sh.T, &sh.ty, &sh.nch, &sh.rows) == 8)
                 if (a == key.ip && b == key.jp && cc == key.kp && d == key.nsm) best = sh;
             std::fclose(fp);
         }
@@ -754,6 +782,23 @@ les_status autotune_sor(les_ctx *c) {
                             break;
                         }
             }
+        // and every one-iteration shape with two rows per warp where it has an
+        // even region height, with its own wave-fitted heights (even regions)
+        for (size_t q = 0, n0 = cand.size(); q < n0; ++q)
+            if (cand[q].T == 1 && tb_rh(1, cand[q].ty) % 2 == 0) {
+                TbShape s2 = cand[q];
+                s2.rows = 2;
+                cand.push_back(s2);
+            }
+        for (int nch = 1; nch <= 4; nch *= 2) {
+            const long long gx = cdiv(c->prm.ip, tb_tx(1));
+            for (int w = 1; w <= 4; ++w)
+                for (int ty = 4; tb_rh(1, ty) <= kTbMaxRH; ty += 2)
+                    if (gx * cdiv(c->prm.jp, ty) * nch <= (long long)w * nsm) {
+                        if (tb_rh(1, ty) % 4) cand.push_back(TbShape{1, ty, nch, 2});
+                        break;
+                    }
+        }
         for (const TbShape &sh : cand) {
             const int T = sh.T, nch = sh.nch;
             if (sh.ty < 4 || (nch > 1 && cdiv(c->prm.kp, nch) < 8) || !tb_shape_ok(c, sh)) continue;
@@ -777,8 +822,8 @@ les_status autotune_sor(les_ctx *c) {
         if (!best.T) return fail(LES_ERR_DIMS, "no SOR pass shape fits");
         if (cache)
             if (FILE *fp = std::fopen(cache, "a")) {
-                std::fprintf(fp, "%d %d %d %d %d %d %d\n", key.ip, key.jp, key.kp, key.nsm, best.T, best.ty,
-                             best.nch);
+                std::fprintf(fp, "%d %d %d %d %d %d %d %d\n", key.ip, key.jp, key.kp, key.nsm, best.T, best.ty,
+                             best.nch, best.rows);
                 std::fclose(fp);
             }
     }
@@ -1172,6 +1217,12 @@ les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *nch) {
     if (ty) *ty = c->tb.ty;
     if (tx) *tx = c->tb.T ? tb_tx(c->tb.T) : 0;
     if (nch) *nch = c->tb.nch;
+    return ok();
+}
+
+les_status les_ctx_sor_rows(les_ctx *c, int *rows) {
+    if (!c || !rows) return fail(LES_ERR_BAD_ARG, "NULL argument");
+    *rows = c->tb.T ? c->tb.rows : 0;
     return ok();
 }
 

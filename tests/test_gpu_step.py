@@ -271,7 +271,7 @@ def test_upload_with_inconsistent_p_ghosts(require_gpu):
 
 
 @pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "1,21,1", "2,16,1", "2,8,3", "2,13,2",
-                                   "3,8,2", "3,4,1"])
+                                   "3,8,2", "3,4,1", "1,28,4,2", "1,12,1,2", "1,20,2,2"])
 def test_each_sor_pass_shape_equals_per_colour_sweeps(require_gpu, monkeypatch, shape):
     # shapes (iterations per pass, tile rows, k chunks) the
     # autotuner may pick, on a grid with several tiles in i, j and k
@@ -286,14 +286,16 @@ def test_each_sor_pass_shape_equals_per_colour_sweeps(require_gpu, monkeypatch, 
         g.warmup(1)
         g.step(1, 3)
     T, ty, _, nch = _sor_shape(g1)
-    assert (T, ty, nch) == tuple(int(x) for x in shape.split(","))
+    want = [int(x) for x in shape.split(",")]
+    assert (T, ty, nch, _sor_rows(g1)) == tuple(want + [1] * (4 - len(want)))
     assert_bitexact(g1.download(ALL), g2.download(ALL), ip, jp, kp, ALL)
     assert g1.metrics()["sor_iters"] == g2.metrics()["sor_iters"]
     g1.close()
     g2.close()
 
 
-@pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "1,20,1", "1,23,1"])
+@pytest.mark.parametrize("shape", ["1,4,1", "1,28,2", "1,12,4", "1,20,1", "1,23,1", "1,28,2,2", "1,12,4,2",
+                                   "1,4,1,2"])
 def test_odd_jp_sor_pass_shapes_equal_per_colour_sweeps(require_gpu, monkeypatch, shape):
     # odd jp: rows jp and 1 are j-neighbours of the same colour, which read
     # each other's value from before the half-sweep (press.f95's ghost rows);
@@ -310,7 +312,8 @@ def test_odd_jp_sor_pass_shapes_equal_per_colour_sweeps(require_gpu, monkeypatch
         g.warmup(1)
         g.step(1, 3)
     T, ty, _, nch = _sor_shape(g1)
-    assert (T, ty, nch) == tuple(int(x) for x in shape.split(","))
+    want = [int(x) for x in shape.split(",")]
+    assert (T, ty, nch, _sor_rows(g1)) == tuple(want + [1] * (4 - len(want)))
     assert_bitexact(g1.download(ALL), g2.download(ALL), ip, jp, kp, ALL)
     assert g1.metrics()["sor_iters"] == g2.metrics()["sor_iters"]
     g1.close()
@@ -336,6 +339,14 @@ def test_odd_jp_against_oracle(require_gpu, dims):
     per_launch = abi.lib().les_ctx_sor_iters_per_launch(gpu.ctx)
     assert per_launch == (0.5 if jp < 8 else 1.0)
     gpu.close()
+
+
+def _sor_rows(gpu):
+    import ctypes as C
+    from les_halo_b200 import abi
+    r = C.c_int()
+    abi.check(abi.lib().les_ctx_sor_rows(gpu.ctx, C.byref(r)))
+    return r.value
 
 
 def _sor_shape(gpu):
