@@ -568,9 +568,11 @@ void *les_ensemble_stream(les_ensemble *ens);
 /* The ensemble autotuner's record (after the first les_ensemble_step): the
  * candidates' times in ms per four tuning passes of every member (cap
  * entries at most; -1 where not run), their count and the index chosen.
- * Candidate 0: each member's own shape; 1..5: one-iteration passes of
- * (28, 1), (28, 2), (24, 1), (20, 1), (12, 1) tile rows and k chunks where a
- * member can run them.  LES_ENSEMBLE_TUNE=own skips the tuner. */
+ * Candidate 0: each member's own shape; 1..9: one-iteration passes of
+ * (tile rows, k chunks, region rows per warp) (28, 1, 1), (28, 2, 1),
+ * (24, 1, 1), (20, 1, 1), (12, 1, 1), (28, 1, 2), (28, 2, 2), (20, 1, 2),
+ * (12, 1, 2) where a member can run them.  LES_ENSEMBLE_TUNE=own skips the
+ * tuner. */
 les_status les_ensemble_tune_info(les_ensemble *ens, float *ms, int cap, int *ncand, int *chosen);
 /* kernels launched by the ensemble so far (all members) */
 uint64_t les_ensemble_launch_count(les_ensemble *ens);

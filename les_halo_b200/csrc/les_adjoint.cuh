@@ -75,19 +75,36 @@ __global__ void __launch_bounds__(256) k_adj_boundp1(Geo g, float *pb) {
 // One SOR half-sweep of colour nrd transposed: in -> out over p's range;
 // rhsb of the swept cells accumulates.  Cell (i,j,k) is swept when
 // i + j + k + nrd is odd (press.f95:91, i = 1 + mod(k+j+nrd, 2), step 2).
+// FOLDK: the transposed boundp2 of the iteration (planes km+1 and 0 into km
+// and 1, after which both are zero) is applied to the reads: a linear map
+// along k, it commutes with the transposed boundp1, which works within
+// planes, so the boundp1 that runs before this half-sweep may come first.
+// The test is on the plane only, so a warp (one row of one plane) takes one
+// path.
+template <bool FOLDK>
 __global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_sweep(Geo g, const float *in, float *out, float *rhsb,
                                                               const float *cn1, int nrd, float omega) {
     const int i = blockIdx.x * kAdjBX + threadIdx.x, j = blockIdx.y * kAdjBY + threadIdx.y, k = blockIdx.z;
     if (i > g.im + 2 || j > g.jm + 2) return;
     const int im = g.im, jm = g.jm, km = g.km;
     const int c = IX(g, i, j, k);
-    const float v = in[c];
+    // (boundp2 covers i = 0..im+1, j = 0..jm+1; p's last row and column
+    // i = im+2, j = jm+2 pass through)
+    const bool inb = i <= im + 1 && j <= jm + 1;
+    auto ld = [&](int a, int b, int d) {
+        float x = in[IX(g, a, b, d)];
+        if (FOLDK && a <= im + 1 && b <= jm + 1) {
+            if (d == km) x += in[IX(g, a, b, km + 1)];
+            if (d == 1) x += in[IX(g, a, b, 0)];
+        }
+        return x;
+    };
+    const float v = (FOLDK && inb && (k == 0 || k == km + 1)) ? 0.0f : ld(i, j, k);
     const bool ii = i >= 1 && i <= im, jj = j >= 1 && j <= jm, kk = k >= 1 && k <= km;
     // what the forward sweep at swept cell (a,b,d) took from this location
     // through coefficient coef
     auto from = [&](int a, int b, int d, float coef) {
-        const int q = IX(g, a, b, d);
-        return omega * (cn1[q] * coef) * in[q];
+        return omega * (cn1[IX(g, a, b, d)] * coef) * ld(a, b, d);
     };
     auto swept = [&](int a, int b, int d) { return ((a + b + d + nrd) & 1) != 0; };
     float r = v;

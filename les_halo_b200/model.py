@@ -367,10 +367,11 @@ class Ensemble:
     def tune_info(self) -> dict:
         """The ensemble autotuner's candidates (ms per four tuning passes of
         every member) and the one chosen."""
-        ms = (C.c_float * 8)()
+        ms = (C.c_float * 16)()
         n, ch = C.c_int(), C.c_int()
-        abi.check(abi.lib().les_ensemble_tune_info(self.h, ms, 8, C.byref(n), C.byref(ch)))
-        names = ["own", "1,28,1", "1,28,2", "1,24,1", "1,20,1", "1,12,1"]
+        abi.check(abi.lib().les_ensemble_tune_info(self.h, ms, 16, C.byref(n), C.byref(ch)))
+        names = ["own", "1,28,1", "1,28,2", "1,24,1", "1,20,1", "1,12,1", "1,28,1,2", "1,28,2,2", "1,20,1,2",
+                 "1,12,1,2"]
         return {"candidates": {names[i] if i < len(names) else str(i): round(ms[i], 3) for i in range(n.value)},
                 "chosen": names[ch.value] if 0 <= ch.value < len(names) else None}
 

@@ -31,7 +31,7 @@ def test_ensemble_equals_member_steps(require_gpu):
     l1 = ens.launches()
     assert l1 > 0
     ti = ens.tune_info()  # the ensemble autotuner ran once, at the first step
-    assert len(ti["candidates"]) == 6 and ti["chosen"] in ti["candidates"]
+    assert len(ti["candidates"]) == 10 and ti["chosen"] in ti["candidates"]
     assert all(v > 0 for v in ti["candidates"].values())
     for (dims, _, _), a, b in zip(DOMAINS, members, solo):
         assert_bitexact(a.download(ALL), b.download(ALL), *dims, ALL)
