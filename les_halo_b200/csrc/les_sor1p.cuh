@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
     unsigned long long fh = 0, flo = 0;
     int bad = 0;
     float fsum = 0.0f;
+    float bk[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};  // per row: rhs of the colour-1 columns of the last colour-0 plane
     const int tau_end = k1 + 1;  // plane k1 is stored at this step
     const bool edge = ir0 <= 1 || ir0 + kTbRW - 1 >= im;
 
@@ -165,6 +166,11 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
                             fix_add_nonneg(t2, fh, flo, bad);
                     }
                 };
+                // the rhs kept by the previous step's colour 0 (plane tau-1), for
+                // this step's colour 1, before this step's colour 0 replaces it
+                float bkp[2][2];
+#pragma unroll
+                for (int r = 0; r < 2; ++r) bkp[r][0] = bk[r][0], bkp[r][1] = bk[r][1];
                 // One half-sweep of row r on window phase X (plane pl, slot sq),
                 // the k neighbours at phases XU (above) and XL (below); its
                 // in-warp neighbour row's values from the copy o.
@@ -181,7 +187,18 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
                         nn = wrapn[1] ? Sd[(2 * sq + 1) * RW4 + lane] : Pq[RW4];
                         ss = make_float4(o[0], o[1], o[2], o[3]);
                     }
-                    const float4 bb = Bs[sq * RA4 + d0[r]];
+                    // rhs: colour 0 loads the row's plane and keeps the other two
+                    // columns for colour 1 on the same plane at the next step
+                    float4 bb;
+                    if (!stores) {
+                        bb = Bs[sq * RA4 + d0[r]];
+                        bk[r][0] = C0 == 0 ? bb.y : bb.x;
+                        bk[r][1] = C0 == 0 ? bb.w : bb.z;
+                    } else if constexpr (C0 == 0) {
+                        bb = make_float4(bkp[r][0], 0.0f, bkp[r][1], 0.0f);
+                    } else {
+                        bb = make_float4(0.0f, bkp[r][0], 0.0f, bkp[r][1]);
+                    }
                     const float c4l = kq.c4l[pl], c4s = kq.c4s[pl];
                     const float cnq = CN1K ? kq.cnk[pl] : 0.0f, cC = CN1K ? 0.0f : g.cnC[pl];
                     const bool acc = acc_cells[r] && pl >= k0 && pl <= k1;
