@@ -63,7 +63,7 @@ def _compile_all(targets, verbose: bool) -> dict:
     reports = {}
     for out in targets:
         objs = [str(j[1]) for j in jobs if j[0] == out]
-        _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(out), *objs])
+        _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(out), *objs, "-ldl"])
         reports[out] = "".join(log for j, log in zip(jobs, logs) if j[0] == out)
         if verbose:
             sys.stderr.write(reports[out])

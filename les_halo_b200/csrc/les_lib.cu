@@ -29,6 +29,7 @@
 #include "les_refine.cuh"
 #include "les_spectral.cuh"
 #include "les_fft.cuh"
+#include "les_nvtx.h"
 #include "les_step.cuh"
 
 using namespace les;
@@ -869,6 +870,7 @@ les_status les_params_default(les_params *p, int ip, int jp, int kp) {
     p->ip = ip;
     p->jp = jp;
     p->kp = kp;
+    LES_RANGE("les_params_default");
     p->dt = 0.2f;
     p->ro = 1.1763f;
     p->vn = 15.83f * powf(10.0f, -6.0f);
@@ -889,6 +891,7 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     les_status s = check_params(prm);
     if (s != LES_OK) return s;
     int ndev = 0;
+    LES_RANGE("les_ctx_create");
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
         return fail(LES_ERR_CUDA, "no CUDA device");
@@ -1012,6 +1015,7 @@ les_status les_ctx_destroy(les_ctx *c) {
     for (auto &gs : c->graph_src)
         if (gs) cudaGraphDestroy(gs);
     for (auto e : c->tev) cudaEventDestroy(e);
+    LES_RANGE("les_ctx_destroy");
     for (auto x : c->extra) cudaFree(x);
     cudaFree(c->d_fields);
     cudaFree(c->d_tables);
@@ -1048,6 +1052,7 @@ les_status les_ctx_field(les_ctx *c, int field, float **dptr, int *ox, int *si, 
     if (sk) *sk = c->geo.sk;
     return ok();
 }
+    LES_RANGE("les_ctx_field");
 
 static les_status upload_field(les_ctx *c, int f, const float *host) {
     if (!host) return LES_OK;
@@ -1142,6 +1147,7 @@ les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
     if (s != LES_OK) return s;
     s = build_tables(c, hf, true);
     if (s != LES_OK) return s;
+    LES_RANGE("les_ctx_upload");
     const float *src[LES_NFIELDS] = {hf->u,    hf->v,    hf->w,    hf->p,   hf->usum,   hf->vsum,   hf->wsum,
                                      hf->f,    hf->g,    hf->h,    hf->fold, hf->gold,  hf->hold,   hf->rhs,
                                      hf->sm,   hf->amask1, hf->bmask1, hf->cmask1, hf->dmask1};
@@ -1179,6 +1185,7 @@ les_status les_ctx_download(les_ctx *c, les_host_fields *hf) {
     for (int f = 0; f < LES_NFIELDS; ++f) {
         if ((s = download_field(c, f, dst[f])) != LES_OK) return s;
         CK(cudaStreamSynchronize(c->stream));
+    LES_RANGE("les_ctx_download");
     }
     if (hf->delx1) {
         for (int k = 1; k <= c->prm.kp; ++k) {
@@ -1198,6 +1205,7 @@ les_status les_ctx_warmup(les_ctx *c, int n) {
            c->geo, c->F);
     if ((s = enqueue_bondv1(c, n, false)) != LES_OK) return s;
     if ((s = enqueue_boundp(c, false)) != LES_OK) return s;
+    LES_RANGE("les_ctx_warmup");
     if ((s = enqueue_velfg_les(c, false)) != LES_OK) return s;
     CK(cudaStreamSynchronize(c->stream));
     c->p_ghosts_ok = true;  // ifdata.f95:260-262 applied boundp1, boundp2
@@ -1213,6 +1221,7 @@ les_status les_ctx_sor_tile(les_ctx *c, int *T, int *ty) {
 
 les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *nch) {
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
+    LES_RANGE("les_ctx_sor_tile");
     if (T) *T = c->tb.T;
     if (ty) *ty = c->tb.ty;
     if (tx) *tx = c->tb.T ? tb_tx(c->tb.T) : 0;
@@ -1220,6 +1229,7 @@ les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *nch) {
     return ok();
 }
 
+    LES_RANGE("les_ctx_sor_shape");
 les_status les_ctx_sor_rows(les_ctx *c, int *rows) {
     if (!c || !rows) return fail(LES_ERR_BAD_ARG, "NULL argument");
     *rows = c->tb.T ? c->tb.rows : 0;
@@ -1229,6 +1239,7 @@ les_status les_ctx_sor_rows(les_ctx *c, int *rows) {
 float les_ctx_sor_iters_per_launch(les_ctx *c) {
     if (!c) return 0.0f;
     const bool exact = sor_per_colour(c);
+    LES_RANGE("les_ctx_sor_rows");
     return exact ? 0.5f : (float)(c->tb.T ? c->tb.T : 2);
 }
 
@@ -1241,12 +1252,14 @@ les_status les_ctx_set_sor_path(les_ctx *c, int exact) {
 les_status les_bounds_violations(unsigned long long *count, int *first_ijk) {
 #ifdef LES_CHECKED
     LesOob h{};
+    LES_RANGE("les_ctx_set_sor_path");
     CK(cudaDeviceSynchronize());
     CK(cudaMemcpyFromSymbol(&h, g_les_oob, sizeof h));
     if (count) *count = h.count;
     if (first_ijk)
         for (int q = 0; q < 3; ++q) first_ijk[q] = h.claimed ? h.first[q] : 0;
     return ok();
+    LES_RANGE("les_bounds_violations");
 #else
     (void)count;
     (void)first_ijk;
@@ -1263,6 +1276,7 @@ les_status les_ctx_set_reduction_mode(les_ctx *c, int mode) {
         if (cudaMalloc(&c->d_r2, sizeof(float) * c->box_elems) != cudaSuccess) {
             cudaGetLastError();
             return fail(LES_ERR_NOMEM, "reltmp^2 buffer");
+    LES_RANGE("les_ctx_set_reduction_mode");
         }
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -1280,6 +1294,7 @@ les_status les_set_wind_profile(les_ctx *c, const float *wp) {
                        cudaMemcpyHostToDevice, c->stream));
     return ok();
 }
+    LES_RANGE("les_set_wind_profile");
 
 les_status les_step(les_ctx *c, int n0, int nsteps) {
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
@@ -1290,21 +1305,25 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
         const bool exact = sor_per_colour(c);
         const int gi = ((n == 1 && c->prm.ical == 0) ? 1 : 0) + (exact ? 2 : 0);
         if ((!exact || c->ref_outer > 0) && c->tb.T == 0) {  // the refined press uses the passes too
+    LES_RANGE("les_step");
             les_status st = autotune_sor(c);
             if (st != LES_OK) return st;
         }
         if (!c->graph[gi]) {
             // Capture the step once per kind (n==1 broadcast or not); the
+        LES_RANGE("step");
             // kernels only see n through that distinction.
             const uint64_t before = c->launches;
             c->capturing_timed = c->tslots > 0;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            LES_RANGE("sor_autotune");
             les_status st = enqueue_step(c, (gi & 1) ? 1 : 2, exact);
             cudaGraph_t gr = nullptr;
             cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
             c->capturing_timed = false;
             c->graph_kernels[gi] = c->launches - before;
             c->launches = before;  // capturing runs nothing
+            LES_RANGE("step_graph_capture");
             if (st != LES_OK) {
                 if (gr) cudaGraphDestroy(gr);
                 return st;
@@ -1364,6 +1383,7 @@ les_status les_ctx_set_timing(les_ctx *c, int nslots) {
     }
     // graphs are re-captured with (or without) event nodes for the new pool
     for (int gi = 0; gi < 4; ++gi) {
+    LES_RANGE("les_ctx_set_timing");
         if (c->graph[gi]) cudaGraphExecDestroy(c->graph[gi]);
         if (c->graph_src[gi]) cudaGraphDestroy(c->graph_src[gi]);
         c->graph[gi] = nullptr;
@@ -1387,6 +1407,7 @@ les_status les_ctx_phase_times(les_ctx *c, int slot, float *ms, int n) {
     }
     return ok();
 }
+    LES_RANGE("les_ctx_phase_times");
 
 les_status les_ctx_sync(les_ctx *c) {
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
@@ -1398,12 +1419,14 @@ les_status les_last_metrics(les_ctx *c, les_metrics *m) {
     if (!c || !m) return fail(LES_ERR_BAD_ARG, "NULL argument");
     Scal s;
     CK(cudaMemcpyAsync(&s, c->d_scal, sizeof s, cudaMemcpyDeviceToHost, c->stream));
+    LES_RANGE("les_ctx_sync");
     CK(cudaStreamSynchronize(c->stream));
     m->n = s.n;
     m->sor_iters = s.sor_iters;
     m->sor = s.sor;
     m->rhsav = s.rhsav;
     m->pav = s.pav;
+    LES_RANGE("les_last_metrics");
     m->uout = s.uout;
     m->p_centre = s.probe[0];
     m->u_centre = s.probe[1];
@@ -1488,7 +1511,10 @@ static les_status ctx_halo(les_ctx *c, int which, float *buf, int write) {
     CK(cudaStreamSynchronize(c->stream));
     return ok();
 }
-les_status les_ctx_halo_read(les_ctx *c, int which, float *buf) { return ctx_halo(c, which, buf, 0); }
+les_status les_ctx_halo_read(les_ctx *c, int which, float *buf) {
+    LES_RANGE("les_ctx_halo_read");
+    return ctx_halo(c, which, buf, 0);
+}
 les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
     return ctx_halo(c, which, const_cast<float *>(buf), 1);
 }
@@ -1499,5 +1525,6 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 #include "les_stats_io.inc"
 #include "les_ensemble.inc"
 #include "les_refine.inc"
+    LES_RANGE("les_ctx_halo_write");
 #include "les_adjoint.inc"
 #include "les_adjstep.inc"

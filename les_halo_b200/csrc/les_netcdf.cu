@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "les_abi.h"
+#include "les_nvtx.h"
 
 les_status les_internal_fail(les_status s, const char *msg);
 les_status les_internal_ok();
@@ -201,6 +202,7 @@ struct les_netcdf {
 extern "C" {
 
 les_status les_netcdf_open(const char *prefix, int ip, int jp, int kp, int ntimes, les_netcdf **out) {
+    LES_RANGE("les_netcdf_open");
     if (!out) return les_internal_fail(LES_ERR_BAD_ARG, "NULL handle");
     *out = nullptr;
     if (ip < 1 || jp < 1 || kp < 1 || ntimes < 1) return les_internal_fail(LES_ERR_BAD_ARG, "bad grid or time count");
@@ -235,6 +237,7 @@ les_status les_netcdf_open(const char *prefix, int ip, int jp, int kp, int ntime
 
 les_status les_netcdf_write_host(les_netcdf *nc, int t, const float *p, const float *u, const float *v,
                                  const float *w, const float *usum, const float *vsum, const float *wsum) {
+    LES_RANGE("les_netcdf_write_host");
     if (!nc || !p || !u || !v || !w || !usum || !vsum || !wsum)
         return les_internal_fail(LES_ERR_BAD_ARG, "NULL argument");
     if (t < 1 || t > nc->ntimes) {
@@ -254,6 +257,7 @@ les_status les_netcdf_write_host(les_netcdf *nc, int t, const float *p, const fl
 }
 
 les_status les_netcdf_write(les_netcdf *nc, les_ctx *ctx, int t) {
+    LES_RANGE("les_netcdf_write");
     if (!nc || !ctx) return les_internal_fail(LES_ERR_BAD_ARG, "NULL argument");
     const size_t ip = nc->ip, jp = nc->jp, kp = nc->kp;
     std::vector<float> p((ip + 3) * (jp + 3) * (kp + 2)), u((ip + 2) * (jp + 3) * (kp + 2)), v(u.size()),
@@ -273,6 +277,7 @@ les_status les_netcdf_write(les_netcdf *nc, les_ctx *ctx, int t) {
 }
 
 les_status les_netcdf_close(les_netcdf *nc) {
+    LES_RANGE("les_netcdf_close");
     if (!nc) return les_internal_ok();
     les_status s = LES_OK;
     for (NcFile &f : nc->f) {

@@ -14,6 +14,7 @@
 #include "les_halo.cuh"
 #include "les_synth.h"
 #include "les_synth_gen.h"
+#include "les_nvtx.h"
 
 using namespace les;
 
@@ -136,6 +137,7 @@ extern "C" {
 
 les_status les_grid_metrics(int ip, int jp, int kp, float *dx1_, float *dxl_, float *dy1_, float *dyl_, float *z2_,
                             float *dzn_, float *dzs_, float *dxs_, float *dys_) {
+    LES_RANGE("les_grid_metrics");
     if (!dx1_ || !dxl_ || !dy1_ || !dyl_ || !z2_ || !dzn_ || !dzs_ || !dxs_ || !dys_)
         return les_internal_fail(LES_ERR_BAD_ARG, "NULL array");
     auto dx1 = [&](int i) -> float & { return dx1_[i + 1]; };
@@ -167,6 +169,7 @@ les_status les_grid_metrics(int ip, int jp, int kp, float *dx1_, float *dxl_, fl
 les_status les_poisson_coeffs(int ip, int jp, int kp, const float *dxs, const float *dys, const float *dzs,
                               float *cn1, float *cn2l, float *cn2s, float *cn3l, float *cn3s, float *cn4l,
                               float *cn4s) {
+    LES_RANGE("les_poisson_coeffs");
     if (!dxs || !dys || !dzs || !cn1 || !cn2l || !cn2s || !cn3l || !cn3s || !cn4l || !cn4s)
         return les_internal_fail(LES_ERR_BAD_ARG, "NULL array");
     if (ip < 1 || jp < 1 || kp < 1) return les_internal_fail(LES_ERR_DIMS, "bad extents");
@@ -196,6 +199,7 @@ les_status les_poisson_coeffs(int ip, int jp, int kp, const float *dxs, const fl
 
 les_status les_building_masks(int ip, int jp, int kp, const float *zbm, const float *z2, const float *dzn,
                               float *amask1, float *bmask1, float *cmask1, float *dmask1) {
+    LES_RANGE("les_building_masks");
     if (!zbm || !z2 || !dzn || !amask1 || !bmask1 || !cmask1 || !dmask1)
         return les_internal_fail(LES_ERR_BAD_ARG, "NULL array");
     if (ip < 1 || jp < 1 || kp < 1) return les_internal_fail(LES_ERR_DIMS, "bad extents");
@@ -230,10 +234,12 @@ size_t les_halo_buffer_floats(unsigned im, unsigned jm, unsigned km, unsigned hw
 }
 les_status les_halo_pack(const float *a, float *b, unsigned im, unsigned jm, unsigned km, unsigned hw, unsigned vdim,
                          int device, void *stream) {
+    LES_RANGE("les_halo_pack");
     return halo_common(a, b, im, jm, km, hw, vdim, device, stream, 0, 0);
 }
 les_status les_halo_unpack(float *a, const float *b, unsigned im, unsigned jm, unsigned km, unsigned hw, unsigned vdim,
                            int device, void *stream) {
+    LES_RANGE("les_halo_unpack");
     return halo_common(b, a, im, jm, km, hw, vdim, device, stream, 0, 1);
 }
 // One entry per component width, named after the reference's kernels
@@ -263,10 +269,12 @@ LES_HALO_WIDTH(16)
 
 les_status les_halo_pack_inner(const float *a, float *b, unsigned im, unsigned jm, unsigned km, unsigned hw,
                                unsigned vdim, int device, void *stream) {
+    LES_RANGE("les_halo_pack_inner");
     return halo_common(a, b, im, jm, km, hw, vdim, device, stream, 1, 0);
 }
 les_status les_halo_unpack_inner(float *a, const float *b, unsigned im, unsigned jm, unsigned km, unsigned hw,
                                  unsigned vdim, int device, void *stream) {
+    LES_RANGE("les_halo_unpack_inner");
     return halo_common(b, a, im, jm, km, hw, vdim, device, stream, 1, 1);
 }
 
@@ -278,6 +286,7 @@ void les_synth_default(les_synth_cfg *c, int ip, int jp, int kp, uint64_t seed) 
 
 les_status les_synth_grid(const les_synth_cfg *c, float *dx1, float *dxl, float *dy1, float *dyl, float *z2,
                           float *dzn, float *dzs, float *dxs, float *dys) {
+    LES_RANGE("les_synth_grid");
     if (!c || !dx1 || !dy1 || !dzn) return les_internal_fail(LES_ERR_BAD_ARG, "NULL argument");
     les_synth_gen::base_grid(c, dx1, dy1, dzn);
     return les_grid_metrics(c->ip, c->jp, c->kp, dx1, dxl, dy1, dyl, z2, dzn, dzs, dxs, dys);
@@ -286,6 +295,7 @@ les_status les_synth_grid(const les_synth_cfg *c, float *dx1, float *dxl, float 
 float les_synth_terrain(const les_synth_cfg *c, float *zbm) { return les_synth_gen::terrain(c, zbm); }
 
 les_status les_synth_inflow(const les_synth_cfg *c, const float *z2, const float *dzn, float *wp) {
+    LES_RANGE("les_synth_inflow");
     if (!c || !z2 || !dzn || !wp) return les_internal_fail(LES_ERR_BAD_ARG, "NULL argument");
     les_synth_gen::inflow(c, z2, dzn, wp);
     return les_internal_ok();
