@@ -412,6 +412,94 @@ def config2_bench():
             gpu.close()
 
 
+DECOMP = dict(ranks_one_gpu=2, halo=16, sync_every=8, warm=2, steps=5)
+
+
+def decomp_bench(ws=1, rank=0, dist=None):
+    """The x-decomposed step (les_halo_b200/decomp.py) on the workload: on
+    one GPU, DECOMP["ranks_one_gpu"] ranks in this process (device copies
+    between their slabs) against the single domain on the same per-colour
+    SOR path; under torchrun (--decomp), one slab per rank with NCCL
+    send/recv and all-reduce, strong scaling of the one domain.  CUDA events
+    on the ranks' streams, the slowest rank's time."""
+    import torch
+    import les_halo_b200 as lh
+    from les_halo_b200 import abi, decomp as D
+    A = DECOMP
+    case = make_case()
+    cells, nmaxp, ical = case.ip * case.jp * case.kp, case.params.nmaxp, case.params.ical
+    ranks, dd, single_ms = [], None, None
+    try:
+        if ws == 1:
+            dd = D.DecomposedLes(case, A["ranks_one_gpu"], A["halo"], A["sync_every"])
+            ranks, ex = dd.ranks, dd.ex
+        else:
+            slabs = D.split_columns(case.ip, ws, A["halo"])
+            r = D.DDRank(case, slabs[rank])
+            parts = [None] * ws
+            dist.all_gather_object(parts, r.area_part())
+            r.set_owned(None if any(x is None for x in parts) else sum(parts))
+            ranks, ex = [r], D.DistExchange(r, dist, device="cuda")
+        D.run_steps(ranks, ex, 1, A["warm"], nmaxp, ical, A["sync_every"])
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        s0 = ranks[0].stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        for r in ranks[1:]:
+            r.stream().wait_event(e0)
+        D.run_steps(ranks, ex, 1 + A["warm"], A["steps"], nmaxp, ical, A["sync_every"])
+        for r in ranks[1:]:
+            ev = torch.cuda.Event()
+            ev.record(r.stream())
+            s0.wait_event(ev)
+        e1.record(s0)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / A["steps"]
+        if dist:
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t[0])
+        m = ranks[-1].gpu.metrics()
+        H, mid = A["halo"], ranks[0]
+        per_side = (mid.block_floats(D.STATE_MASK, H) + mid.block_floats(D.RHS_MASK, H) +
+                    ((nmaxp - 1) // A["sync_every"]) * mid.block_floats(D.P_MASK, H)) * 4
+        for r in ranks:
+            r.close()
+        ranks = []
+        if dd is not None:
+            dd.ranks = []
+        if ws == 1:
+            g = lh.GpuLes(case)
+            try:
+                abi.check(abi.lib().les_ctx_set_sor_path(g.ctx, 1))
+                st = torch.cuda.ExternalStream(g.stream())
+                g.step(1, A["warm"])
+                g.sync()
+                e0.record(st)
+                g.step(1 + A["warm"], A["steps"])
+                e1.record(st)
+                torch.cuda.synchronize()
+                single_ms = e0.elapsed_time(e1) / A["steps"]
+            finally:
+                g.close()
+        out = {"ranks": A["ranks_one_gpu"] if ws == 1 else ws, "gpus": ws, "halo_columns": H,
+               "p_exchange_every": A["sync_every"], "steps": A["steps"], "ms_per_step": round(ms, 3),
+               "mpts": round(cells / ms / 1e3, 1), "sor_iters": int(m["sor_iters"]),
+               "halo_bytes_per_step_per_neighbour": int(per_side),
+               "sor_path": "per colour (k_sor_colour + boundp), exact all-rank sums",
+               "transport": "device copies, one process" if ws == 1 else "NCCL send/recv + all-reduce"}
+        if single_ms is not None:
+            out.update(single_domain_same_path_ms=round(single_ms, 3), time_vs_single=round(ms / single_ms, 3))
+        return out
+    except Exception as exc:
+        return {"error": f"{type(exc).__name__}: {exc}"[:300]}
+    finally:
+        for r in ranks:
+            r.close()
+
+
 ADJOINT = dict(ip=150, jp=150, kp=90, steps=100, ckpt=10, box=((66, 85), (66, 85), (1, 5)), seed=1)
 
 
@@ -631,6 +719,7 @@ def run_ours(args):
     ens_line = None
     if not args.profile and not args.no_ensemble:
         ens_line = ensemble_bench(args.steps, args.warmup, ws, rank, dist)
+    dd_line = decomp_bench(ws, rank, dist) if (ws > 1 and args.decomp and not args.profile) else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mpts/s", "n_gpus": ws,
@@ -671,10 +760,14 @@ def run_ours(args):
         }
         if ens_line is not None:
             line["ensemble"] = ens_line
+        if dd_line is not None:
+            line["decomposition"] = dd_line
         if not args.profile and not args.no_adjoint and ws == 1:
             line["adjoint"] = adjoint_bench()
         if not args.profile and args.refine and not args.no_config2 and ws == 1:
             line["config2_refined_press"] = config2_bench()
+        if not args.profile and not args.no_decomp and ws == 1:
+            line["decomposition"] = decomp_bench()
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
@@ -699,6 +792,10 @@ def main():
                     help="skip the adjoint (config-3) cost measurement")
     ap.add_argument("--no-config2", action="store_true",
                     help="skip the 1000x1000x150 refined-press measurement")
+    ap.add_argument("--no-decomp", action="store_true",
+                    help="skip the x-decomposed step measurement (one GPU: ranks in one process)")
+    ap.add_argument("--decomp", action="store_true",
+                    help="under torchrun: also time the one domain decomposed over the ranks (NCCL)")
     ap.add_argument("--profile", action="store_true",
                     help="no in-graph timing events (for runs under ncu)")
     ap.add_argument("--grid", default=None,

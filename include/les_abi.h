@@ -625,6 +625,54 @@ les_status les_adj_step_b(les_adj *adj, int n, int slot);
 les_status les_adj_read(les_adj *adj, double *wind_profile_b, double *drag_b, les_host_fields *state_b);
 les_status les_adj_write(les_adj *adj, const les_host_fields *state_b);
 
+/* ---- x-decomposed domain (no reference counterpart: the reference
+ * round-trips its halos through ST_HALO_READ_* / ST_HALO_WRITE_* states,
+ * module_LES_combined_ocl_TEMPL_V2.f95:438-491, on one device).  One context
+ * per rank holds a slab of columns, created and uploaded like any context
+ * from the slab's arrays: columns olo..ohi are its own, the others (at most
+ * H on each side) a copy of its neighbours' own columns.  The host drives
+ * the step as phases and, between them, exchanges the halo columns
+ * (les_dd_pack on the owner, les_dd_unpack on the neighbour) and sums the
+ * limbs of les_dd_sums over the ranks (64-bit integer sums; NCCL all-reduce
+ * or device copies).  Step n, with K = 1 when n == 1 and ical == 0, else 2:
+ *   BEGIN(n); halo(u v w p f g h usum vsum wsum fold gold hold);
+ *   MOMENTUM(K); sum; RHSAV; halo(rhs);
+ *   nmaxp times: [every m-th iteration but the first: halo(p)]
+ *                SOR_ITER; sum; SOR_TEST;
+ *   PAV_SUM; sum; PAV_END.
+ * With halo width H >= 12 and m <= H/2 every own cell equals the single
+ * domain's bit for bit (the per-colour SOR, canonical FP32 sums).
+ * les_dd_area_part: this rank's share (own columns) of the rhsav / pav
+ *   denominator as an exact Q63.64 sum (lo, hi, bad); the ranks add the
+ *   128-bit values and pass the total to les_dd_set_owned.
+ * les_dd_set_owned: make the context a rank: own columns olo..ohi (the
+ *   global sums count only these) and the whole domain's denominator.
+ *   les_step then refuses the context.
+ * les_dd_block_floats: floats of one packed block (fields of mask, width
+ *   columns, every row and plane of the box).
+ * les_dd_pack / les_dd_unpack: columns i0..i0+width-1 of the fields in
+ *   mask (bit LES_F_*) to / from a device buffer, on the context's stream.
+ * les_dd_sums: device address of the context's kLimbs = 6 int64: after a
+ *   phase that ends in "sum" this rank's total, to be replaced by the sum
+ *   over the ranks before the next phase. */
+enum {
+    LES_DD_BEGIN = 0,
+    LES_DD_MOMENTUM = 1,
+    LES_DD_RHSAV = 2,
+    LES_DD_SOR_ITER = 3,
+    LES_DD_SOR_TEST = 4,
+    LES_DD_PAV_SUM = 5,
+    LES_DD_PAV_END = 6
+};
+les_status les_dd_area_part(les_ctx *ctx, int olo, int ohi, unsigned long long *lo, long long *hi, int *bad);
+les_status les_dd_set_owned(les_ctx *ctx, int olo, int ohi, unsigned long long area_lo, long long area_hi,
+                            int area_bad);
+long long les_dd_block_floats(les_ctx *ctx, unsigned mask, int width);
+les_status les_dd_pack(les_ctx *ctx, unsigned mask, int i0, int width, float *buf);
+les_status les_dd_unpack(les_ctx *ctx, unsigned mask, int i0, int width, const float *buf);
+les_status les_dd_sums(les_ctx *ctx, long long **dptr);
+les_status les_dd_phase(les_ctx *ctx, int phase, int arg);
+
 #ifdef __cplusplus
 }
 #endif

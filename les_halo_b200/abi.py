@@ -19,6 +19,8 @@ LES_OK, LES_ERR_BAD_ARG, LES_ERR_DIMS, LES_ERR_CUDA, LES_ERR_TIMEOUT, LES_ERR_NA
 LES_INFLOW_POWER_LAW, LES_INFLOW_EXTERNAL = 0, 1
 # les_ctx_set_reduction_mode bits: sums taken in the reference's serial FP32 order
 LES_RED_CANONICAL, LES_RED_F_RHSAV, LES_RED_F_SOR, LES_RED_F_PAV, LES_RED_FAITHFUL = 0, 1, 2, 4, 7
+(LES_DD_BEGIN, LES_DD_MOMENTUM, LES_DD_RHSAV, LES_DD_SOR_ITER, LES_DD_SOR_TEST, LES_DD_PAV_SUM,
+ LES_DD_PAV_END) = range(7)
 FIELD_IDS = ["u", "v", "w", "p", "usum", "vsum", "wsum", "f", "g", "h", "fold", "gold", "hold",
              "rhs", "sm", "amask1", "bmask1", "cmask1", "dmask1"]
 HALO_IDS = ["p", "uvw", "uvwsum", "fgh", "fgh_old", "rhs", "sm"]
@@ -158,6 +160,13 @@ _SIGS = {
     "les_adj_step_b": (C.c_int, [_P, C.c_int, C.c_int]),
     "les_adj_read": (C.c_int, [_P, _P, _P, C.POINTER(LesHostFields)]),
     "les_adj_write": (C.c_int, [_P, C.POINTER(LesHostFields)]),
+    "les_dd_area_part": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_ulonglong), C.POINTER(C.c_longlong), _I]),
+    "les_dd_set_owned": (C.c_int, [_P, C.c_int, C.c_int, C.c_ulonglong, C.c_longlong, C.c_int]),
+    "les_dd_block_floats": (C.c_longlong, [_P, C.c_uint, C.c_int]),
+    "les_dd_pack": (C.c_int, [_P, C.c_uint, C.c_int, C.c_int, _P]),
+    "les_dd_unpack": (C.c_int, [_P, C.c_uint, C.c_int, C.c_int, _P]),
+    "les_dd_sums": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
+    "les_dd_phase": (C.c_int, [_P, C.c_int, C.c_int]),
 }
 
 # Per-routine entries: every argument is a pointer (Fortran by-reference).

@@ -19,6 +19,10 @@ constexpr int kOX = 31;
 struct Geo {
     int im, jm, km;
     int ox, si, sj, sk;
+    // columns olo..ohi enter the global sums (rhsav, SOR residual, pav):
+    // 1..im, except on a rank of an x-decomposed domain, whose halo columns
+    // belong to its neighbours
+    int olo, ohi;
     // 1-D tables; each pointer is pre-offset so t[i] is the Fortran t(i).
     const float *dx1, *dy1, *dzn, *dzs, *dxs, *dys;
     const float *cn2l, *cn2s, *cn3l, *cn3s, *cn4l, *cn4s;

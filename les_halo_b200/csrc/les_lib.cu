@@ -31,6 +31,7 @@
 #include "les_fft.cuh"
 #include "les_nvtx.h"
 #include "les_step.cuh"
+#include "les_dd.cuh"
 
 using namespace les;
 
@@ -219,6 +220,10 @@ struct les_ctx {
     int red_mode = LES_RED_CANONICAL;
     float *d_r2 = nullptr;                // reltmp^2 per cell (box), LES_RED_F_SOR only
     float *d_drag = nullptr;              // per-column IBM force scale (les_ctx_set_drag)
+    // x-decomposed domain (les_dd.inc): this context is one rank's slab
+    bool dd = false;
+    double dd_area = 0.0;                 // the whole domain's rhsav/pav denominator
+    long long *d_dd = nullptr;            // limbs of a global sum (kDDLimbs)
 };
 
 // Buffers of an SOR pass other than the context's p / second p / rhs / scalars.
@@ -865,12 +870,12 @@ const char *les_last_error_string(void) { return g_err.c_str(); }
 const char *les_version(void) { return "lesb200 0.1 (sm_100a)"; }
 
 les_status les_params_default(les_params *p, int ip, int jp, int kp) {
+    LES_RANGE("les_params_default");
     if (!p) return fail(LES_ERR_BAD_ARG, "params is NULL");
     std::memset(p, 0, sizeof *p);
     p->ip = ip;
     p->jp = jp;
     p->kp = kp;
-    LES_RANGE("les_params_default");
     p->dt = 0.2f;
     p->ro = 1.1763f;
     p->vn = 15.83f * powf(10.0f, -6.0f);
@@ -886,12 +891,12 @@ les_status les_params_default(les_params *p, int ip, int jp, int kp) {
 }
 
 les_status les_ctx_create(const les_params *prm, les_ctx **out) {
+    LES_RANGE("les_ctx_create");
     if (!out) return fail(LES_ERR_BAD_ARG, "out is NULL");
     *out = nullptr;
     les_status s = check_params(prm);
     if (s != LES_OK) return s;
     int ndev = 0;
-    LES_RANGE("les_ctx_create");
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
         return fail(LES_ERR_CUDA, "no CUDA device");
@@ -904,6 +909,8 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
     g.im = ip;
     g.jm = jp;
     g.km = kp;
+    g.olo = 1;
+    g.ohi = ip;
     g.ox = kOX;
     g.si = ((kOX + ip + 3) + 31) / 32 * 32;
     g.sj = jp + 4;
@@ -1008,6 +1015,7 @@ les_status les_ctx_create(const les_params *prm, les_ctx **out) {
 }
 
 les_status les_ctx_destroy(les_ctx *c) {
+    LES_RANGE("les_ctx_destroy");
     if (!c) return ok();
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto &ge : c->graph)
@@ -1015,7 +1023,6 @@ les_status les_ctx_destroy(les_ctx *c) {
     for (auto &gs : c->graph_src)
         if (gs) cudaGraphDestroy(gs);
     for (auto e : c->tev) cudaEventDestroy(e);
-    LES_RANGE("les_ctx_destroy");
     for (auto x : c->extra) cudaFree(x);
     cudaFree(c->d_fields);
     cudaFree(c->d_tables);
@@ -1034,6 +1041,7 @@ les_status les_ctx_destroy(les_ctx *c) {
     cudaFree(c->d_refw);
     cudaFree(c->d_r2);
     cudaFree(c->d_drag);
+    cudaFree(c->d_dd);
     spec_release(c->spec);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1044,6 +1052,7 @@ void *les_ctx_stream(les_ctx *c) { return c ? (void *)c->stream : nullptr; }
 uint64_t les_ctx_launch_count(les_ctx *c) { return c ? c->launches : 0; }
 
 les_status les_ctx_field(les_ctx *c, int field, float **dptr, int *ox, int *si, int *sj, int *sk) {
+    LES_RANGE("les_ctx_field");
     if (!c || field < 0 || field >= LES_NFIELDS) return fail(LES_ERR_BAD_ARG, "bad field");
     if (dptr) *dptr = field_ptr(c, field);
     if (ox) *ox = c->geo.ox;
@@ -1052,7 +1061,6 @@ les_status les_ctx_field(les_ctx *c, int field, float **dptr, int *ox, int *si, 
     if (sk) *sk = c->geo.sk;
     return ok();
 }
-    LES_RANGE("les_ctx_field");
 
 static les_status upload_field(les_ctx *c, int f, const float *host) {
     if (!host) return LES_OK;
@@ -1139,6 +1147,7 @@ static les_status scan_inputs(les_ctx *c, const les_host_fields *hf) {
 }
 
 les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
+    LES_RANGE("les_ctx_upload");
     if (!c || !hf) return fail(LES_ERR_BAD_ARG, "NULL argument");
     if (!hf->dx1 || !hf->dy1 || !hf->dzn || !hf->dzs || !hf->dxs || !hf->dys || !hf->cn2l || !hf->cn2s ||
         !hf->cn3l || !hf->cn3s || !hf->cn4l || !hf->cn4s)
@@ -1147,7 +1156,6 @@ les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
     if (s != LES_OK) return s;
     s = build_tables(c, hf, true);
     if (s != LES_OK) return s;
-    LES_RANGE("les_ctx_upload");
     const float *src[LES_NFIELDS] = {hf->u,    hf->v,    hf->w,    hf->p,   hf->usum,   hf->vsum,   hf->wsum,
                                      hf->f,    hf->g,    hf->h,    hf->fold, hf->gold,  hf->hold,   hf->rhs,
                                      hf->sm,   hf->amask1, hf->bmask1, hf->cmask1, hf->dmask1};
@@ -1177,6 +1185,7 @@ les_status les_ctx_upload(les_ctx *c, const les_host_fields *hf) {
 }
 
 les_status les_ctx_download(les_ctx *c, les_host_fields *hf) {
+    LES_RANGE("les_ctx_download");
     if (!c || !hf) return fail(LES_ERR_BAD_ARG, "NULL argument");
     float *dst[LES_NFIELDS] = {hf->u,  hf->v,  hf->w,    hf->p,    hf->usum, hf->vsum,   hf->wsum,
                                hf->f,  hf->g,  hf->h,    hf->fold, hf->gold, hf->hold,   hf->rhs,
@@ -1185,7 +1194,6 @@ les_status les_ctx_download(les_ctx *c, les_host_fields *hf) {
     for (int f = 0; f < LES_NFIELDS; ++f) {
         if ((s = download_field(c, f, dst[f])) != LES_OK) return s;
         CK(cudaStreamSynchronize(c->stream));
-    LES_RANGE("les_ctx_download");
     }
     if (hf->delx1) {
         for (int k = 1; k <= c->prm.kp; ++k) {
@@ -1197,6 +1205,7 @@ les_status les_ctx_download(les_ctx *c, les_host_fields *hf) {
 }
 
 les_status les_ctx_warmup(les_ctx *c, int n) {
+    LES_RANGE("les_ctx_warmup");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     if (!c->uploaded) return fail(LES_ERR_STATE, "warmup before upload");
     les_status s;
@@ -1205,7 +1214,6 @@ les_status les_ctx_warmup(les_ctx *c, int n) {
            c->geo, c->F);
     if ((s = enqueue_bondv1(c, n, false)) != LES_OK) return s;
     if ((s = enqueue_boundp(c, false)) != LES_OK) return s;
-    LES_RANGE("les_ctx_warmup");
     if ((s = enqueue_velfg_les(c, false)) != LES_OK) return s;
     CK(cudaStreamSynchronize(c->stream));
     c->p_ghosts_ok = true;  // ifdata.f95:260-262 applied boundp1, boundp2
@@ -1213,6 +1221,7 @@ les_status les_ctx_warmup(les_ctx *c, int n) {
 }
 
 les_status les_ctx_sor_tile(les_ctx *c, int *T, int *ty) {
+    LES_RANGE("les_ctx_sor_tile");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     if (T) *T = c->tb.T;
     if (ty) *ty = c->tb.ty;
@@ -1220,8 +1229,8 @@ les_status les_ctx_sor_tile(les_ctx *c, int *T, int *ty) {
 }
 
 les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *nch) {
+    LES_RANGE("les_ctx_sor_shape");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
-    LES_RANGE("les_ctx_sor_tile");
     if (T) *T = c->tb.T;
     if (ty) *ty = c->tb.ty;
     if (tx) *tx = c->tb.T ? tb_tx(c->tb.T) : 0;
@@ -1229,8 +1238,8 @@ les_status les_ctx_sor_shape(les_ctx *c, int *T, int *ty, int *tx, int *nch) {
     return ok();
 }
 
-    LES_RANGE("les_ctx_sor_shape");
 les_status les_ctx_sor_rows(les_ctx *c, int *rows) {
+    LES_RANGE("les_ctx_sor_rows");
     if (!c || !rows) return fail(LES_ERR_BAD_ARG, "NULL argument");
     *rows = c->tb.T ? c->tb.rows : 0;
     return ok();
@@ -1239,27 +1248,26 @@ les_status les_ctx_sor_rows(les_ctx *c, int *rows) {
 float les_ctx_sor_iters_per_launch(les_ctx *c) {
     if (!c) return 0.0f;
     const bool exact = sor_per_colour(c);
-    LES_RANGE("les_ctx_sor_rows");
     return exact ? 0.5f : (float)(c->tb.T ? c->tb.T : 2);
 }
 
 les_status les_ctx_set_sor_path(les_ctx *c, int exact) {
+    LES_RANGE("les_ctx_set_sor_path");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     c->force_exact_sor = exact != 0;
     return ok();
 }
 
 les_status les_bounds_violations(unsigned long long *count, int *first_ijk) {
+    LES_RANGE("les_bounds_violations");
 #ifdef LES_CHECKED
     LesOob h{};
-    LES_RANGE("les_ctx_set_sor_path");
     CK(cudaDeviceSynchronize());
     CK(cudaMemcpyFromSymbol(&h, g_les_oob, sizeof h));
     if (count) *count = h.count;
     if (first_ijk)
         for (int q = 0; q < 3; ++q) first_ijk[q] = h.claimed ? h.first[q] : 0;
     return ok();
-    LES_RANGE("les_bounds_violations");
 #else
     (void)count;
     (void)first_ijk;
@@ -1268,6 +1276,7 @@ les_status les_bounds_violations(unsigned long long *count, int *first_ijk) {
 }
 
 les_status les_ctx_set_reduction_mode(les_ctx *c, int mode) {
+    LES_RANGE("les_ctx_set_reduction_mode");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     if (mode < 0 || mode > LES_RED_FAITHFUL) return fail(LES_ERR_BAD_ARG, "bad reduction mode %d", mode);
     if (mode != LES_RED_CANONICAL && c->ref_outer > 0)
@@ -1276,7 +1285,6 @@ les_status les_ctx_set_reduction_mode(les_ctx *c, int mode) {
         if (cudaMalloc(&c->d_r2, sizeof(float) * c->box_elems) != cudaSuccess) {
             cudaGetLastError();
             return fail(LES_ERR_NOMEM, "reltmp^2 buffer");
-    LES_RANGE("les_ctx_set_reduction_mode");
         }
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -1286,6 +1294,7 @@ les_status les_ctx_set_reduction_mode(les_ctx *c, int mode) {
 }
 
 les_status les_set_wind_profile(les_ctx *c, const float *wp) {
+    LES_RANGE("les_set_wind_profile");
     if (!c || !wp) return fail(LES_ERR_BAD_ARG, "NULL argument");
     if (c->prm.inflow_mode != LES_INFLOW_EXTERNAL) return fail(LES_ERR_STATE, "context uses the power-law inflow");
     const long long bad = first_non_finite(wp, (size_t)c->prm.jp * c->prm.kp);
@@ -1294,36 +1303,36 @@ les_status les_set_wind_profile(les_ctx *c, const float *wp) {
                        cudaMemcpyHostToDevice, c->stream));
     return ok();
 }
-    LES_RANGE("les_set_wind_profile");
 
 les_status les_step(les_ctx *c, int n0, int nsteps) {
+    LES_RANGE("les_step");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     if (!c->uploaded) return fail(LES_ERR_STATE, "step before upload");
     if (nsteps < 0) return fail(LES_ERR_BAD_ARG, "nsteps < 0");
+    if (c->dd) return fail(LES_ERR_STATE, "a rank of a decomposed domain steps by les_dd_phase");
     for (int s = 0; s < nsteps; ++s) {
+        LES_RANGE("step");
         const int n = n0 + s;
         const bool exact = sor_per_colour(c);
         const int gi = ((n == 1 && c->prm.ical == 0) ? 1 : 0) + (exact ? 2 : 0);
         if ((!exact || c->ref_outer > 0) && c->tb.T == 0) {  // the refined press uses the passes too
-    LES_RANGE("les_step");
+            LES_RANGE("sor_autotune");
             les_status st = autotune_sor(c);
             if (st != LES_OK) return st;
         }
         if (!c->graph[gi]) {
             // Capture the step once per kind (n==1 broadcast or not); the
-        LES_RANGE("step");
             // kernels only see n through that distinction.
+            LES_RANGE("step_graph_capture");
             const uint64_t before = c->launches;
             c->capturing_timed = c->tslots > 0;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            LES_RANGE("sor_autotune");
             les_status st = enqueue_step(c, (gi & 1) ? 1 : 2, exact);
             cudaGraph_t gr = nullptr;
             cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
             c->capturing_timed = false;
             c->graph_kernels[gi] = c->launches - before;
             c->launches = before;  // capturing runs nothing
-            LES_RANGE("step_graph_capture");
             if (st != LES_OK) {
                 if (gr) cudaGraphDestroy(gr);
                 return st;
@@ -1374,6 +1383,7 @@ les_status les_step(les_ctx *c, int n0, int nsteps) {
 }
 
 les_status les_ctx_set_timing(les_ctx *c, int nslots) {
+    LES_RANGE("les_ctx_set_timing");
     if (!c || nslots < 0) return fail(LES_ERR_BAD_ARG, "bad argument");
     CK(cudaStreamSynchronize(c->stream));
     if (nslots > 0 && c->tslots > 0 && (size_t)nslots * LES_NTEV <= c->tev.size()) {
@@ -1383,7 +1393,6 @@ les_status les_ctx_set_timing(les_ctx *c, int nslots) {
     }
     // graphs are re-captured with (or without) event nodes for the new pool
     for (int gi = 0; gi < 4; ++gi) {
-    LES_RANGE("les_ctx_set_timing");
         if (c->graph[gi]) cudaGraphExecDestroy(c->graph[gi]);
         if (c->graph_src[gi]) cudaGraphDestroy(c->graph_src[gi]);
         c->graph[gi] = nullptr;
@@ -1398,6 +1407,7 @@ les_status les_ctx_set_timing(les_ctx *c, int nslots) {
 }
 
 les_status les_ctx_phase_times(les_ctx *c, int slot, float *ms, int n) {
+    LES_RANGE("les_ctx_phase_times");
     if (!c || !ms || slot < 0 || slot >= c->tslots) return fail(LES_ERR_BAD_ARG, "bad slot");
     CK(cudaStreamSynchronize(c->stream));
     // ms[0..7]: consecutive phases between the events; ms[8]: whole step
@@ -1407,26 +1417,25 @@ les_status les_ctx_phase_times(les_ctx *c, int slot, float *ms, int n) {
     }
     return ok();
 }
-    LES_RANGE("les_ctx_phase_times");
 
 les_status les_ctx_sync(les_ctx *c) {
+    LES_RANGE("les_ctx_sync");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");
     CK(cudaStreamSynchronize(c->stream));
     return ok();
 }
 
 les_status les_last_metrics(les_ctx *c, les_metrics *m) {
+    LES_RANGE("les_last_metrics");
     if (!c || !m) return fail(LES_ERR_BAD_ARG, "NULL argument");
     Scal s;
     CK(cudaMemcpyAsync(&s, c->d_scal, sizeof s, cudaMemcpyDeviceToHost, c->stream));
-    LES_RANGE("les_ctx_sync");
     CK(cudaStreamSynchronize(c->stream));
     m->n = s.n;
     m->sor_iters = s.sor_iters;
     m->sor = s.sor;
     m->rhsav = s.rhsav;
     m->pav = s.pav;
-    LES_RANGE("les_last_metrics");
     m->uout = s.uout;
     m->p_centre = s.probe[0];
     m->u_centre = s.probe[1];
@@ -1516,6 +1525,7 @@ les_status les_ctx_halo_read(les_ctx *c, int which, float *buf) {
     return ctx_halo(c, which, buf, 0);
 }
 les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
+    LES_RANGE("les_ctx_halo_write");
     return ctx_halo(c, which, const_cast<float *>(buf), 1);
 }
 
@@ -1525,6 +1535,6 @@ les_status les_ctx_halo_write(les_ctx *c, int which, const float *buf) {
 #include "les_stats_io.inc"
 #include "les_ensemble.inc"
 #include "les_refine.inc"
-    LES_RANGE("les_ctx_halo_write");
 #include "les_adjoint.inc"
 #include "les_adjstep.inc"
+#include "les_dd.inc"

@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(kRedNT, 6) k_rhs(Geo g, Fields F, int kchunk, 
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
     const int k0 = 1 + blockIdx.z * kchunk;
     const int k1 = min(g.km, k0 + kchunk - 1);
+    const bool own = i >= g.olo && i <= g.ohi;
     i128 acc = 0;
     int bad = 0;
     if (i <= g.im && j <= g.jm) {
@@ -58,7 +59,7 @@ __global__ void __launch_bounds__(kRedNT, 6) k_rhs(Geo g, Fields F, int kchunk, 
             float r = fdiv(-um + uc, dx1[i], rdx) + fdiv(-vm + vc, dy1[j], rdy) + kdiv(-wm + wc, dz, rdz);
             r = fdiv(fc - fm, dx1[i], rdx) + fdiv(gc - gm, dy1[j], rdy) + kdiv(hc - hm, dz, rdz) + kdiv(r, g.dt, rdt);
             F.rhs[c] = r;
-            acc += fix_term(dx1[i] * dy1[j] * dzn[k] * r, bad);
+            if (own) acc += fix_term(dx1[i] * dy1[j] * dzn[k] * r, bad);
         }
     }
     block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
@@ -157,6 +158,7 @@ __global__ void __launch_bounds__(kRedNT) k_sor_colour(Geo g, float *__restrict_
     const int k0 = 1 + blockIdx.z * kchunk;
     const int k1 = min(g.km, k0 + kchunk - 1);
     const float rhsav = s->rhsav;
+    const bool own = i >= g.olo && i <= g.ohi;
     i128 acc = 0;
     int bad = 0;
     if (i <= g.im && j <= g.jm) {
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(kRedNT) k_sor_colour(Geo g, float *__restrict_
                                   (rhs[c] - rhsav)) -
                            pc);
             p[c] = pc + reltmp;
-            acc += fix_term(reltmp * reltmp, bad);
+            if (own) acc += fix_term(reltmp * reltmp, bad);
             if (r2) r2[c] = reltmp * reltmp;
         }
     }
@@ -247,6 +249,7 @@ __global__ void __launch_bounds__(kRedNT) k_pav_reduce(Geo g, const float *p0, c
     const int j = 1 + blockIdx.y * kRedBY + threadIdx.y;
     const int k0 = 1 + blockIdx.z * kchunk;
     const int k1 = min(g.km, k0 + kchunk - 1);
+    const bool own = i >= g.olo && i <= g.ohi;
     i128 acc = 0;
     int bad = 0;
     if (i <= g.im && j <= g.jm) {
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(kRedNT) k_pav_reduce(Geo g, const float *p0, c
         for (int q = 0; q < kRedKMax; ++q) pv[q] = (k0 + q <= k1) ? p[IX(g, i, j, k0 + q)] : 0.0f;
 #pragma unroll
         for (int q = 0; q < kRedKMax; ++q)
-            if (k0 + q <= k1) acc += fix_term(pv[q] * g.dx1[i] * g.dy1[j] * g.dzn[k0 + q], bad);
+            if (own && k0 + q <= k1) acc += fix_term(pv[q] * g.dx1[i] * g.dy1[j] * g.dzn[k0 + q], bad);
     }
     block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)]);
 }
