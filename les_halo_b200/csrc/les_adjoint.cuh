@@ -79,33 +79,40 @@ __global__ void __launch_bounds__(256) k_adj_boundp1(Geo g, float *pb) {
 // and 1, after which both are zero) is applied to the reads: a linear map
 // along k, it commutes with the transposed boundp1, which works within
 // planes, so the boundp1 that runs before this half-sweep may come first.
-// The test is on the plane only, so a warp (one row of one plane) takes one
-// path.
-template <bool FOLDK>
-__global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_sweep(Geo g, const float *in, float *out, float *rhsb,
-                                                              const float *cn1, int nrd, float omega) {
-    const int i = blockIdx.x * kAdjBX + threadIdx.x, j = blockIdx.y * kAdjBY + threadIdx.y, k = blockIdx.z;
-    if (i > g.im + 2 || j > g.jm + 2) return;
+// Only planes k <= 2 and k >= km-1 read plane 1 or km (their own or a
+// neighbour's), so only their blocks take the folding body (the plane is
+// the block's z, one path per block); neighbours are addressed by offsets
+// from the cell's index.
+template <bool FOLD>
+__device__ __forceinline__ void adj_sweep_cell(const Geo &g, const float *__restrict__ in, float *__restrict__ out,
+                                               float *__restrict__ rhsb, const float *__restrict__ cn1, int nrd,
+                                               float omega, int i, int j, int k) {
     const int im = g.im, jm = g.jm, km = g.km;
     const int c = IX(g, i, j, k);
+    const int sy = g.si, sz = g.si * g.sj;
+#ifdef LES_CHECKED
+    auto nb = [&](int di, int dj, int dk) { return IX(g, i + di, j + dj, k + dk); };
+#else
+    auto nb = [&](int di, int dj, int dk) { return c + di + sy * dj + sz * dk; };
+#endif
+    // in at box index x of plane d, with the fold of planes km+1 and 0
+    // (every location read here lies in boundp2's range i <= im+1, j <= jm+1)
+    auto ldx = [&](int x, int d) {
+        float v = in[x];
+        if (FOLD) {
+            if (d == km) v += in[x + sz];
+            if (d == 1) v += in[x - sz];
+        }
+        return v;
+    };
     // (boundp2 covers i = 0..im+1, j = 0..jm+1; p's last row and column
     // i = im+2, j = jm+2 pass through)
     const bool inb = i <= im + 1 && j <= jm + 1;
-    auto ld = [&](int a, int b, int d) {
-        float x = in[IX(g, a, b, d)];
-        if (FOLDK && a <= im + 1 && b <= jm + 1) {
-            if (d == km) x += in[IX(g, a, b, km + 1)];
-            if (d == 1) x += in[IX(g, a, b, 0)];
-        }
-        return x;
-    };
-    const float v = (FOLDK && inb && (k == 0 || k == km + 1)) ? 0.0f : ld(i, j, k);
+    const float v = (FOLD && inb) ? ((k == 0 || k == km + 1) ? 0.0f : ldx(c, k)) : in[c];
     const bool ii = i >= 1 && i <= im, jj = j >= 1 && j <= jm, kk = k >= 1 && k <= km;
-    // what the forward sweep at swept cell (a,b,d) took from this location
-    // through coefficient coef
-    auto from = [&](int a, int b, int d, float coef) {
-        return omega * (cn1[IX(g, a, b, d)] * coef) * ld(a, b, d);
-    };
+    // what the forward sweep at swept cell x (plane d) took from this
+    // location through coefficient coef
+    auto from = [&](int x, int d, float coef) { return omega * (cn1[x] * coef) * ldx(x, d); };
     auto swept = [&](int a, int b, int d) { return ((a + b + d + nrd) & 1) != 0; };
     float r = v;
     if (ii && jj && kk) {
@@ -113,27 +120,38 @@ __global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_sweep(Geo g, const float
             rhsb[c] -= (omega * cn1[c]) * v;
             r = (1.0f - omega) * v;
         } else {  // every interior neighbour was swept
-            if (i > 1) r += from(i - 1, j, k, g.cn2l[i - 1]);
-            if (i < im) r += from(i + 1, j, k, g.cn2s[i + 1]);
-            if (j > 1) r += from(i, j - 1, k, g.cn3l[j - 1]);
-            if (j < jm) r += from(i, j + 1, k, g.cn3s[j + 1]);
-            if (k > 1) r += from(i, j, k - 1, g.cn4l[k - 1]);
-            if (k < km) r += from(i, j, k + 1, g.cn4s[k + 1]);
+            if (i > 1) r += from(nb(-1, 0, 0), k, g.cn2l[i - 1]);
+            if (i < im) r += from(nb(1, 0, 0), k, g.cn2s[i + 1]);
+            if (j > 1) r += from(nb(0, -1, 0), k, g.cn3l[j - 1]);
+            if (j < jm) r += from(nb(0, 1, 0), k, g.cn3s[j + 1]);
+            if (k > 1) r += from(nb(0, 0, -1), k - 1, g.cn4l[k - 1]);
+            if (k < km) r += from(nb(0, 0, 1), k + 1, g.cn4s[k + 1]);
         }
     } else if (jj && kk && i == 0) {
-        if (swept(1, j, k)) r += from(1, j, k, g.cn2s[1]);
+        if (swept(1, j, k)) r += from(nb(1, 0, 0), k, g.cn2s[1]);
     } else if (jj && kk && i == im + 1) {
-        if (swept(im, j, k)) r += from(im, j, k, g.cn2l[im]);
+        if (swept(im, j, k)) r += from(nb(-1, 0, 0), k, g.cn2l[im]);
     } else if (ii && kk && j == 0) {
-        if (swept(i, 1, k)) r += from(i, 1, k, g.cn3s[1]);
+        if (swept(i, 1, k)) r += from(nb(0, 1, 0), k, g.cn3s[1]);
     } else if (ii && kk && j == jm + 1) {
-        if (swept(i, jm, k)) r += from(i, jm, k, g.cn3l[jm]);
+        if (swept(i, jm, k)) r += from(nb(0, -1, 0), k, g.cn3l[jm]);
     } else if (ii && jj && k == 0) {
-        if (swept(i, j, 1)) r += from(i, j, 1, g.cn4s[1]);
+        if (swept(i, j, 1)) r += from(nb(0, 0, 1), 1, g.cn4s[1]);
     } else if (ii && jj && k == km + 1) {
-        if (swept(i, j, km)) r += from(i, j, km, g.cn4l[km]);
+        if (swept(i, j, km)) r += from(nb(0, 0, -1), km, g.cn4l[km]);
     }
     out[c] = r;
+}
+
+template <bool FOLDK>
+__global__ void __launch_bounds__(kAdjBX *kAdjBY) k_adj_sweep(Geo g, const float *in, float *out, float *rhsb,
+                                                              const float *cn1, int nrd, float omega) {
+    const int i = blockIdx.x * kAdjBX + threadIdx.x, j = blockIdx.y * kAdjBY + threadIdx.y, k = blockIdx.z;
+    if (i > g.im + 2 || j > g.jm + 2) return;
+    if (FOLDK && (k <= 2 || k >= g.km - 1))
+        adj_sweep_cell<true>(g, in, out, rhsb, cn1, nrd, omega, i, j, k);
+    else
+        adj_sweep_cell<false>(g, in, out, rhsb, cn1, nrd, omega, i, j, k);
 }
 
 // Interior sum of x in FP64: one partial per 32 x 8 tile of a plane (fixed
