@@ -333,7 +333,8 @@ def ensemble_bench(steps, warmup, ws=1, rank=0, dist=None):
         for g in members:
             g.close()
     ens_ms, cells_all, failed = ensemble_job(ens_ms if err is None else float("inf"), cells, err is not None,
-                                             dist, "cuda" if dist is not None else "cpu")
+                                             dist, "cuda" if dist is not None and dist.get_backend() == "nccl"
+                                             else "cpu")
     if failed:
         return {"error": err or "failed on another rank"}
     out = {"members": E["members"], "cells": cells_all, "kp": E["kp"], "steps": steps, "ranks": ws,

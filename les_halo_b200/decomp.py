@@ -253,7 +253,9 @@ class LocalExchange:
 class DistExchange:
     """One rank per process over torch.distributed (NCCL for the product,
     gloo with CPU tensors in the host tests).  Each exchange is one batch of
-    send/recv pairs with the two neighbours; the sums are one all-reduce."""
+    send/recv pairs with the two neighbours; the sums are one all-reduce.
+    device="cpu" with a GPU rank stages the blocks and the sums through host
+    memory (gloo between processes that share a GPU)."""
 
     def __init__(self, rank, dist, device=None):
         import torch
@@ -262,16 +264,17 @@ class DistExchange:
         self.dist = dist
         self.halo = rank.slab.halo
         self.device = device
+        self.stage = device == "cpu" and rank.stream() is not None
         self.bufs = {}
 
     def _ctx(self):
         s = self.rank.stream()
         return self.torch.cuda.stream(s) if s is not None else contextlib.nullcontext()
 
-    def _buf(self, key, n):
+    def _buf(self, key, n, device=None):
         b = self.bufs.get(key)
         if b is None or b.numel() < n:
-            b = self.torch.empty(n, dtype=self.torch.float32, device=self.device)
+            b = self.torch.empty(n, dtype=self.torch.float32, device=device or self.device)
             self.bufs[key] = b
         return b
 
@@ -286,17 +289,31 @@ class DistExchange:
                 if nb is None:
                     continue
                 sb, rb = self._buf(("s", side, mask), n), self._buf(("r", side, mask), n)
-                self.rank.pack(mask, si0, H, sb)
+                if self.stage:
+                    db = self._buf(("d", side, mask), n, "cuda")
+                    self.rank.pack(mask, si0, H, db)
+                    sb[:n].copy_(db[:n])  # device to host, ordered after the pack
+                else:
+                    self.rank.pack(mask, si0, H, sb)
                 ops += [dist.P2POp(dist.isend, sb[:n], nb), dist.P2POp(dist.irecv, rb[:n], nb)]
-                recvs.append((di0, rb))
+                recvs.append((side, di0, rb))
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
-            for di0, rb in recvs:
+            for side, di0, rb in recvs:
+                if self.stage:
+                    db = self._buf(("d", side, mask), n, "cuda")
+                    db[:n].copy_(rb[:n])
+                    rb = db
                 self.rank.unpack(mask, di0, H, rb)
 
     def allreduce(self):
         with self._ctx():
-            self.dist.all_reduce(self.rank.sums())
+            if self.stage:
+                t = self.rank.sums().cpu()
+                self.dist.all_reduce(t)
+                self.rank.sums().copy_(t)
+            else:
+                self.dist.all_reduce(self.rank.sums())
 
 
 def run_steps(ranks, ex, n0: int, nsteps: int, nmaxp: int, ical: int = 0, sync_every: int = DEFAULT_SYNC):
