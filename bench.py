@@ -419,8 +419,9 @@ DECOMP = dict(ranks_one_gpu=2, halo=16, sync_every=8, warm=2, steps=5)
 def decomp_bench(ws=1, rank=0, dist=None):
     """The x-decomposed step (les_halo_b200/decomp.py) on the workload: on
     one GPU, DECOMP["ranks_one_gpu"] ranks in this process (device copies
-    between their slabs) against the single domain on the same per-colour
-    SOR path; under torchrun (--decomp), one slab per rank with NCCL
+    between their slabs) against the single domain on the same SOR path
+    (one-iteration passes; per colour with LES_DD_SOR=colour); under
+    torchrun (--decomp), one slab per rank with NCCL
     send/recv and all-reduce, strong scaling of the one domain.  CUDA events
     on the ranks' streams, the slowest rank's time."""
     import torch
@@ -474,7 +475,8 @@ def decomp_bench(ws=1, rank=0, dist=None):
         if ws == 1:
             g = lh.GpuLes(case)
             try:
-                abi.check(abi.lib().les_ctx_set_sor_path(g.ctx, 1))
+                if os.environ.get("LES_DD_SOR") == "colour":
+                    abi.check(abi.lib().les_ctx_set_sor_path(g.ctx, 1))
                 st = torch.cuda.ExternalStream(g.stream())
                 g.step(1, A["warm"])
                 g.sync()
@@ -489,7 +491,8 @@ def decomp_bench(ws=1, rank=0, dist=None):
                "p_exchange_every": A["sync_every"], "steps": A["steps"], "ms_per_step": round(ms, 3),
                "mpts": round(cells / ms / 1e3, 1), "sor_iters": int(m["sor_iters"]),
                "halo_bytes_per_step_per_neighbour": int(per_side),
-               "sor_path": "per colour (k_sor_colour + boundp), exact all-rank sums",
+               "sor_path": "one-iteration passes, exact all-rank sums"
+                           if os.environ.get("LES_DD_SOR") != "colour" else "per colour, exact all-rank sums",
                "transport": "device copies, one process" if ws == 1 else "NCCL send/recv + all-reduce"}
         if single_ms is not None:
             out.update(single_domain_same_path_ms=round(single_ms, 3), time_vs_single=round(ms / single_ms, 3))

@@ -641,7 +641,8 @@ les_status les_adj_write(les_adj *adj, const les_host_fields *state_b);
  *                SOR_ITER; sum; SOR_TEST;
  *   PAV_SUM; sum; PAV_END.
  * With halo width H >= 12 and m <= H/2 every own cell equals the single
- * domain's bit for bit (the per-colour SOR, canonical FP32 sums).
+ * domain's bit for bit (canonical FP32 sums; the SOR on the one-iteration
+ * pass kernels, or per colour with LES_DD_SOR=colour).
  * les_dd_area_part: this rank's share (own columns) of the rhsav / pav
  *   denominator as an exact Q63.64 sum (lo, hi, bad); the ranks add the
  *   128-bit values and pass the total to les_dd_set_owned.

@@ -20,6 +20,9 @@ constexpr int kDDLimbs = 6;  // 4 limbs of the total, the bad flag, spare
 struct DDFields {
     float *f[kDDMaxFields];
     int n;
+    int pidx;           // index of p in f (-1: none): p is the second buffer palt when sc->pbuf
+    float *palt;
+    const Scal *sc;
 };
 
 namespace {
@@ -35,7 +38,8 @@ __global__ void __launch_bounds__(256) k_dd_pack(Geo g, DDFields fs, int i0, int
         const long long row = r / w;
         const int c = (int)(r - row * w);
         const int j = (int)(row % g.sj) - 1, k = (int)(row / g.sj) - 1;
-        buf[t] = fs.f[f][IX(g, i0 + c, j, k)];
+        const float *src = (f == fs.pidx && fs.sc->pbuf) ? fs.palt : fs.f[f];
+        buf[t] = src[IX(g, i0 + c, j, k)];
     }
 }
 
@@ -49,18 +53,19 @@ __global__ void __launch_bounds__(256) k_dd_unpack(Geo g, DDFields fs, int i0, i
         const long long row = r / w;
         const int c = (int)(r - row * w);
         const int j = (int)(row % g.sj) - 1, k = (int)(row / g.sj) - 1;
-        fs.f[f][IX(g, i0 + c, j, k)] = buf[t];
+        float *dst = (f == fs.pidx && fs.sc->pbuf) ? fs.palt : fs.f[f];
+        dst[IX(g, i0 + c, j, k)] = buf[t];
     }
 }
 
-// The total of n partial sums as limbs: out[0..2] the low three 32-bit
-// limbs (0..2^32-1), out[3] the top limb (signed), out[4] the bad flag.
-// Summing the limbs of several totals as 64-bit integers is exact for up to
-// 2^31 ranks, and k_dd_unlimbs folds the sums back into 128 bits.
-__global__ void __launch_bounds__(1024) k_dd_limbs(const FixPart *part, int n, long long *out) {
+// The total of n partial sums part[b * stride] as limbs: out[0..2] the low
+// three 32-bit limbs (0..2^32-1), out[3] the top limb (signed), out[4] the
+// bad flag.  Summing the limbs of several totals as 64-bit integers is exact
+// for up to 2^31 ranks, and the sums fold back into 128 bits (dd_total).
+__global__ void __launch_bounds__(1024) k_dd_limbs(const FixPart *part, int n, int stride, long long *out) {
     i128 tot;
     int bad;
-    final_fix(part, n, tot, bad);
+    final_fix_strided(part, n, stride, 0, tot, bad);
     if (threadIdx.x == 0) {
         const unsigned __int128 u = (unsigned __int128)tot;
         out[0] = (long long)(unsigned long long)(u & 0xffffffffu);
@@ -72,11 +77,27 @@ __global__ void __launch_bounds__(1024) k_dd_limbs(const FixPart *part, int n, l
     }
 }
 
-__global__ void k_dd_unlimbs(const long long *in, FixPart *part) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ i128 dd_total(const long long *in) {
     const unsigned __int128 u = (unsigned __int128)(i128)in[0] + ((unsigned __int128)(i128)in[1] << 32) +
                                 ((unsigned __int128)(i128)in[2] << 64) + ((unsigned __int128)(i128)in[3] << 96);
-    part[0] = fix_to_part((i128)u, in[4] != 0);
+    return (i128)u;
+}
+
+__global__ void k_dd_unlimbs(const long long *in, FixPart *part) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    part[0] = fix_to_part(dd_total(in), in[4] != 0);
+}
+
+// The stop test of a one-iteration SOR pass (tb_finish_pass with nit = 1)
+// on the all-rank residual: the pass wrote the other p buffer, which
+// becomes current; a pass after the stop did nothing.
+__global__ void k_dd_sor_finish(const long long *in, float pjuge, Scal *s) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || s->converged) return;
+    const float sor = (float)fix_finish(dd_total(in), in[4] != 0);
+    s->sor = sor;
+    s->sor_iters += 1;
+    if (sor < pjuge) s->converged = 1;
+    s->pbuf ^= 1;
 }
 
 }  // namespace

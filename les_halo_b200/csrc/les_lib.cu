@@ -222,6 +222,7 @@ struct les_ctx {
     float *d_drag = nullptr;              // per-column IBM force scale (les_ctx_set_drag)
     // x-decomposed domain (les_dd.inc): this context is one rank's slab
     bool dd = false;
+    bool dd_passes = false;               // its SOR on one-iteration passes (else per colour)
     double dd_area = 0.0;                 // the whole domain's rhsav/pav denominator
     long long *d_dd = nullptr;            // limbs of a global sum (kDDLimbs)
 };
@@ -611,7 +612,7 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     a.niter = niter;
     a.mode = mode;
     a.itmax = itmax;
-    a.fast = tb_fast_ok(c, sh) ? 1 : 0;
+    a.fast = (!c->dd && tb_fast_ok(c, sh)) ? 1 : 0;
     a.pjuge = pjuge;
     a.part = c->d_part;
     a.sc = c->d_scal;
@@ -623,34 +624,32 @@ les_status launch_sor_tb(les_ctx *c, const TbShape &sh, int niter, int mode, flo
     }
     const Geo &g = c->geo;
 #define TBL(TT, KT) LAUNCH_SMEM(c, (k_sor_tb<TT, KT>), grid, block, sm, g, a, c->kq)
+    // one-iteration passes: CN1K, odd jp, and DD (a rank of an x-decomposed
+    // domain: own-column sums, finished by the host) as template arguments
+    const int v1 = (c->cn1_by_k ? 1 : 0) + (c->prm.jp % 2 ? 2 : 0) + (c->dd ? 4 : 0);
+#define S1L(K, KT, JO, DDV) LAUNCH_SMEM(c, (K<KT, JO, DDV>), grid, block, s1_smem(sh.ty), g, a, c->kq)
+#define S1SW(K)                                         \
+    switch (v1) {                                      \
+        case 0: S1L(K, false, false, false); break;    \
+        case 1: S1L(K, true, false, false); break;     \
+        case 2: S1L(K, false, true, false); break;     \
+        case 3: S1L(K, true, true, false); break;      \
+        case 4: S1L(K, false, false, true); break;     \
+        case 5: S1L(K, true, false, true); break;      \
+        case 6: S1L(K, false, true, true); break;      \
+        default: S1L(K, true, true, true); break;      \
+    }
     if (sh.rows == 2) {  // T = 1 (tb_shape_ok)
-        const size_t smp = s1_smem(sh.ty);
-        if (c->prm.jp % 2) {
-            if (c->cn1_by_k)
-                LAUNCH_SMEM(c, (k_sor1p<true, true>), grid, block, smp, g, a, c->kq);
-            else
-                LAUNCH_SMEM(c, (k_sor1p<false, true>), grid, block, smp, g, a, c->kq);
-        } else {
-            if (c->cn1_by_k)
-                LAUNCH_SMEM(c, (k_sor1p<true, false>), grid, block, smp, g, a, c->kq);
-            else
-                LAUNCH_SMEM(c, (k_sor1p<false, false>), grid, block, smp, g, a, c->kq);
-        }
+        S1SW(k_sor1p);
         return LES_OK;
     }
+    if (sh.T == 1) {
+        S1SW(k_sor1);
+        return LES_OK;
+    }
+#undef S1SW
+#undef S1L
     switch (sh.T * 2 + (c->cn1_by_k ? 1 : 0)) {
-        case 2:
-            if (c->prm.jp % 2)
-                LAUNCH_SMEM(c, (k_sor1<false, true>), grid, block, s1_smem(sh.ty), g, a, c->kq);
-            else
-                LAUNCH_SMEM(c, (k_sor1<false, false>), grid, block, s1_smem(sh.ty), g, a, c->kq);
-            break;
-        case 3:
-            if (c->prm.jp % 2)
-                LAUNCH_SMEM(c, (k_sor1<true, true>), grid, block, s1_smem(sh.ty), g, a, c->kq);
-            else
-                LAUNCH_SMEM(c, (k_sor1<true, false>), grid, block, s1_smem(sh.ty), g, a, c->kq);
-            break;
         case 4: LAUNCH_SMEM(c, k_sor2<false>, grid, block, s2_smem(sh.ty), g, a, c->kq); break;
         case 5: LAUNCH_SMEM(c, k_sor2<true>, grid, block, s2_smem(sh.ty), g, a, c->kq); break;
         case 6: TBL(3, false); break;
@@ -679,25 +678,27 @@ les_status set_tb_smem_attrs() {
     }
     TBA(3, false) TBA(3, true)
 #undef TBA
-#define S1A(KT, JO)                                                                                \
-    {                                                                                              \
-        cudaFuncAttributes fa;                                                                     \
-        CK(cudaFuncGetAttributes(&fa, k_sor1<KT, JO>));                                            \
-        const int mx = optin - (int)fa.sharedSizeBytes;                                            \
-        CK(cudaFuncSetAttribute(k_sor1<KT, JO>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+#define S1A(KT, JO, DDV)                                                                                \
+    {                                                                                                   \
+        cudaFuncAttributes fa;                                                                          \
+        CK(cudaFuncGetAttributes(&fa, k_sor1<KT, JO, DDV>));                                            \
+        const int mx = optin - (int)fa.sharedSizeBytes;                                                 \
+        CK(cudaFuncSetAttribute(k_sor1<KT, JO, DDV>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
         lim = std::min(lim, mx);                                                                   \
     }
-    S1A(false, false) S1A(true, false) S1A(false, true) S1A(true, true)
+    S1A(false, false, false) S1A(true, false, false) S1A(false, true, false) S1A(true, true, false)
+    S1A(false, false, true) S1A(true, false, true) S1A(false, true, true) S1A(true, true, true)
 #undef S1A
-#define S1PA(KT, JO)                                                                                \
-    {                                                                                               \
-        cudaFuncAttributes fa;                                                                      \
-        CK(cudaFuncGetAttributes(&fa, k_sor1p<KT, JO>));                                            \
-        const int mx = optin - (int)fa.sharedSizeBytes;                                             \
-        CK(cudaFuncSetAttribute(k_sor1p<KT, JO>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
+#define S1PA(KT, JO, DDV)                                                                                \
+    {                                                                                                    \
+        cudaFuncAttributes fa;                                                                           \
+        CK(cudaFuncGetAttributes(&fa, k_sor1p<KT, JO, DDV>));                                            \
+        const int mx = optin - (int)fa.sharedSizeBytes;                                                  \
+        CK(cudaFuncSetAttribute(k_sor1p<KT, JO, DDV>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)); \
         lim = std::min(lim, mx);                                                                    \
     }
-    S1PA(false, false) S1PA(true, false) S1PA(false, true) S1PA(true, true)
+    S1PA(false, false, false) S1PA(true, false, false) S1PA(false, true, false) S1PA(true, true, false)
+    S1PA(false, false, true) S1PA(true, false, true) S1PA(false, true, true) S1PA(true, true, true)
 #undef S1PA
 #define S2A(KT)                                                                                \
     {                                                                                          \

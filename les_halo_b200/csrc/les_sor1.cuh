@@ -51,7 +51,7 @@ using IC = std::integral_constant<int, V>;
 // two rows also copy their input rows into a side pair of rows per plane
 // slot, and read each other there (the region holds each real row once:
 // ty + 4 <= jm).
-template <bool CN1K, bool JODD>
+template <bool CN1K, bool JODD, bool DD>
 __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_constant__ TbKCoef kq) {
     extern __shared__ float4 smem4[];
     Scal *sc = a.sc;
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
     const bool ytile = (y >= 2 && y < 2 + ty && jr0 + y <= jm);
     const bool row0 = (y >= 1 && y < RH - 1), row1 = (y >= 2 && y < RH - 2);  // rows each colour sweeps
     float c2l[kTbCW], c2s[kTbCW], cA[kTbCW];
-    int fl[kTbCW];  // bit 0: 1 <= i <= im, 1: i == 1, 2: i == im
+    int fl[kTbCW];  // bit 0: 1 <= i <= im, 1: i == 1, 2: i == im, 3 (DD): summed (olo <= i <= ohi)
 #pragma unroll
     for (int c = 0; c < kTbCW; ++c) {
         const int i = ir0 + kTbCW * lane + c;
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
         c2l[c] = ok ? g.cn2l[i] : 0.0f;
         c2s[c] = ok ? g.cn2s[i] : 0.0f;
         cA[c] = (!CN1K && ok) ? g.cnA[i] : 0.0f;
-        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0);
+        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0) | ((DD && ok && i >= g.olo && i <= g.ohi) ? 8 : 0);
     }
     const int x0 = kTbCW * lane;
     const bool lane_tile = (x0 >= RX && x0 < RX + TX);
@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
     int bad = 0;
     float fsum = 0.0f;
     const int tau_end = k1 + 1;  // plane k1 is stored at this step
-    const bool edge = ir0 <= 1 || ir0 + kTbRW - 1 >= im;
+    // (DD: and tiles with columns outside the summed ones olo..ohi, whose sums test fl bit 3)
+    const bool edge = ir0 <= 1 || ir0 + kTbRW - 1 >= im || (DD && (ir0 + RX < g.olo || ir0 + RX + TX - 1 > g.ohi));
 
     // Steps kb .. tau_end, four per group.  PAR: colour-0 x parity at the
     // group's first step; FAST: FP32 residual; EDGE: i ghosts by select.
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
                                                          c4l * pu + c4s * pd - (b - rhsav)) -
                                                   pc);
                     pc_ref = pc + reltmp;
-                    if (acc && (!EDGE || (fl[C] & 1))) {
+                    if (acc && (!EDGE || (fl[C] & (DD ? 8 : 1)))) {
                         const float t2 = reltmp * reltmp;
                         if constexpr (FAST)
                             fsum += t2;
@@ -276,6 +277,7 @@ __global__ void __launch_bounds__(1024, 1) k_sor1(Geo g, TbArgs a, const __grid_
         const i128 v = (i128)(((unsigned __int128)fh << 64) | (unsigned __int128)flo);
         block_fix_sum_any(v, bad, &a.part[b * kTbTMax]);
     }
+    if (DD) return;  // a rank of an x-decomposed domain: the host sums the partials over the ranks
     __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -21,7 +21,7 @@
 namespace les {
 namespace {
 
-template <bool CN1K, bool JODD>
+template <bool CN1K, bool JODD, bool DD>
 __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_constant__ TbKCoef kq) {
     extern __shared__ float4 smem4[];
     Scal *sc = a.sc;
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
         d0[r] = y * RW4 + lane;
     }
     float c2l[kTbCW], c2s[kTbCW], cA[kTbCW];
-    int fl[kTbCW];  // bit 0: 1 <= i <= im, 1: i == 1, 2: i == im
+    int fl[kTbCW];  // bit 0: 1 <= i <= im, 1: i == 1, 2: i == im, 3 (DD): summed (olo <= i <= ohi)
 #pragma unroll
     for (int c = 0; c < kTbCW; ++c) {
         const int i = ir0 + kTbCW * lane + c;
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
         c2l[c] = ok ? g.cn2l[i] : 0.0f;
         c2s[c] = ok ? g.cn2s[i] : 0.0f;
         cA[c] = (!CN1K && ok) ? g.cnA[i] : 0.0f;
-        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0);
+        fl[c] = (ok ? 1 : 0) | (i == 1 ? 2 : 0) | (i == im ? 4 : 0) | ((DD && ok && i >= g.olo && i <= g.ohi) ? 8 : 0);
     }
     // x parity of the colour-0 columns of each row at the first step
     const int par0 = (jw[0] + 1 - ir0 + kb) & 1, par1 = (jw[1] + 1 - ir0 + kb) & 1;
@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
     float fsum = 0.0f;
     float bk[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};  // per row: rhs of the colour-1 columns of the last colour-0 plane
     const int tau_end = k1 + 1;  // plane k1 is stored at this step
-    const bool edge = ir0 <= 1 || ir0 + kTbRW - 1 >= im;
+    // (DD: and tiles with columns outside the summed ones olo..ohi, whose sums test fl bit 3)
+    const bool edge = ir0 <= 1 || ir0 + kTbRW - 1 >= im || (DD && (ir0 + RX < g.olo || ir0 + RX + TX - 1 > g.ohi));
 
     // Steps kb .. tau_end, four per group.  PAR: row 0's colour-0 x parity
     // at the group's first step; DIFF: row 1's parity differs from row 0's
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
                                                          c4l * pu + c4s * pd - (b - rhsav)) -
                                                   pc);
                     pc_ref = pc + reltmp;
-                    if (acc && (!EDGE || (fl[C] & 1))) {
+                    if (acc && (!EDGE || (fl[C] & (DD ? 8 : 1)))) {
                         const float t2 = reltmp * reltmp;
                         if constexpr (FAST)
                             fsum += t2;
@@ -300,6 +301,7 @@ __global__ void __launch_bounds__(512, 1) k_sor1p(Geo g, TbArgs a, const __grid_
         const i128 v = (i128)(((unsigned __int128)fh << 64) | (unsigned __int128)flo);
         block_fix_sum_any(v, bad, &a.part[b * kTbTMax]);
     }
+    if (DD) return;  // a rank of an x-decomposed domain: the host sums the partials over the ranks
     __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0) {
