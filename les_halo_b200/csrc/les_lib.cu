@@ -1515,9 +1515,23 @@ static les_status ctx_halo(les_ctx *c, int which, float *buf, int write) {
     // p2 = (p, p): both components read p; on write the second is ignored,
     // so one value lands on each p point
     if (write && which == LES_H_P) cv.comp[1] = nullptr;
-    if (write) CK(cudaMemcpyAsync(c->d_stage, buf, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
-    LAUNCH(c, k_ctx_halo, dim3(cdiv((long long)n, 256)), dim3(256), c->geo, cv, c->d_stage, d, write);
-    if (!write) CK(cudaMemcpyAsync(buf, c->d_stage, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    // page-locked host memory (cudaHostAlloc / cudaHostRegister) is mapped
+    // into the device's address space: the kernel reads or writes the
+    // caller's buffer across the host link itself, with no staging copy
+    cudaPointerAttributes pa{};
+    float *mapped = nullptr;
+    if (cudaPointerGetAttributes(&pa, buf) == cudaSuccess) {
+        if (pa.type == cudaMemoryTypeHost && pa.devicePointer) mapped = static_cast<float *>(pa.devicePointer);
+    } else {
+        cudaGetLastError();
+    }
+    if (mapped) {
+        LAUNCH(c, k_ctx_halo, dim3(cdiv((long long)n, 256)), dim3(256), c->geo, cv, mapped, d, write);
+    } else {
+        if (write) CK(cudaMemcpyAsync(c->d_stage, buf, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+        LAUNCH(c, k_ctx_halo, dim3(cdiv((long long)n, 256)), dim3(256), c->geo, cv, c->d_stage, d, write);
+        if (!write) CK(cudaMemcpyAsync(buf, c->d_stage, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+    }
     CK(cudaStreamSynchronize(c->stream));
     return ok();
 }

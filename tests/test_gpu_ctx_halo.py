@@ -76,8 +76,24 @@ def _ref_sizes(ip, jp, kp):
             "sm": 2 * (ip + jp + 4) * (kp + 2)}
 
 
+_KEEP = []
+
+
+def _host(n, pinned, fill=0.0):
+    """A float32 host buffer: pageable numpy memory (staged through the
+    device by the library), or page-locked memory (torch pin_memory), which
+    the library's kernel reads and writes in place."""
+    if not pinned:
+        return np.full(n, fill, np.float32)
+    import torch
+    t = torch.full((n,), fill, dtype=torch.float32).pin_memory()
+    _KEEP.append(t)
+    return t.numpy()
+
+
+@pytest.mark.parametrize("pinned", [False, True])
 @pytest.mark.parametrize("dims", [(24, 20, 16), (33, 19, 12)])
-def test_ctx_halo_read_write_vs_oracle(require_gpu, dims):
+def test_ctx_halo_read_write_vs_oracle(require_gpu, dims, pinned):
     ip, jp, kp = dims
     L = abi.lib()
     case = synthetic_case(ip, jp, kp, seed=ip + jp, masks_and_poisson=oracle.masks_and_poisson)
@@ -94,13 +110,14 @@ def test_ctx_halo_read_write_vs_oracle(require_gpu, dims):
         # read: the ring of the combined array, N|S|W|E, component-major
         want = np.zeros(n, np.float32)
         oracle.halo_pack(np.ascontiguousarray(comb.ravel(order="F")), want, im, jm, km, 1, vd)
-        got = np.full(n, np.nan, np.float32)
+        got = _host(n, pinned, np.nan)
         abi.check(L.les_ctx_halo_read(gpu.ctx, h, got.ctypes.data))
         np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32), err_msg=which)
         # write: random ring values land where halo_exchange.cl's write puts them
-        buf = rng.standard_normal(n).astype(np.float32)
+        buf = _host(n, pinned)
+        buf[:] = rng.standard_normal(n).astype(np.float32)
         flat = np.ascontiguousarray(comb.ravel(order="F"))
-        oracle.halo_unpack(flat, buf, im, jm, km, 1, vd)
+        oracle.halo_unpack(flat, np.ascontiguousarray(buf), im, jm, km, 1, vd)
         after = flat.reshape(comb.shape, order="F")
         expect = _fields_from(which, after, F)
         abi.check(L.les_ctx_halo_write(gpu.ctx, h, buf.ctypes.data))
@@ -110,7 +127,7 @@ def test_ctx_halo_read_write_vs_oracle(require_gpu, dims):
                                           err_msg=f"{which}: {nm}")
         # round trip: reading the ring back gives what a read of the new
         # state must give, and writing it again changes nothing
-        back = np.zeros(n, np.float32)
+        back = _host(n, pinned)
         abi.check(L.les_ctx_halo_read(gpu.ctx, h, back.ctypes.data))
         _, _, comb2 = _combined(which, now, ip, jp, kp)
         want2 = np.zeros(n, np.float32)
