@@ -737,7 +737,9 @@ def run_ours(args):
                                     "rows_per_warp": rw.value},
                        "l2": "inputs larger than L2 (19 state fields, 3.5 GB)"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_sor_tb" if ipl >= 1 else "k_sor_colour",
+            "roofline": {"bound": "hbm",
+                         "kernel": ("k_sor_colour" if ipl < 1 else "k_sor1p" if rw.value == 2 else
+                                    {1: "k_sor1", 2: "k_sor2"}.get(tT, "k_sor_tb")),
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": peak_kind,
