@@ -173,3 +173,17 @@ def _x(slab, mask):
     if slab.west is not None:
         out.append(("unpack", mask, slab.olo - slab.halo))
     return out
+
+
+def test_dd_entries_validate_without_a_gpu():
+    import ctypes as C
+    L = abi.lib()
+    lo, hi, bad = C.c_ulonglong(), C.c_longlong(), C.c_int()
+    assert L.les_dd_area_part(None, 1, 2, C.byref(lo), C.byref(hi), C.byref(bad)) == abi.LES_ERR_BAD_ARG
+    assert L.les_dd_set_owned(None, 1, 2, 0, 0, 0) == abi.LES_ERR_BAD_ARG
+    assert L.les_dd_phase(None, abi.LES_DD_BEGIN, 1) == abi.LES_ERR_BAD_ARG
+    assert L.les_dd_pack(None, D.P_MASK, 1, 4, None) == abi.LES_ERR_BAD_ARG
+    assert L.les_dd_unpack(None, D.P_MASK, 1, 4, None) == abi.LES_ERR_BAD_ARG
+    assert L.les_dd_block_floats(None, D.P_MASK, 4) == -1
+    d = C.c_void_p()
+    assert L.les_dd_sums(None, C.byref(d)) == abi.LES_ERR_BAD_ARG
