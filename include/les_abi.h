@@ -655,7 +655,10 @@ les_status les_adj_write(les_adj *adj, const les_host_fields *state_b);
  *   mask (bit LES_F_*) to / from a device buffer, on the context's stream.
  * les_dd_sums: device address of the context's kLimbs = 6 int64: after a
  *   phase that ends in "sum" this rank's total, to be replaced by the sum
- *   over the ranks before the next phase. */
+ *   over the ranks before the next phase.
+ * les_dd_local_sum: that replacement for n ranks of this process on one
+ *   device (one kernel on ranks[0]'s stream, ordered by events against
+ *   every rank's stream). */
 enum {
     LES_DD_BEGIN = 0,
     LES_DD_MOMENTUM = 1,
@@ -672,6 +675,7 @@ long long les_dd_block_floats(les_ctx *ctx, unsigned mask, int width);
 les_status les_dd_pack(les_ctx *ctx, unsigned mask, int i0, int width, float *buf);
 les_status les_dd_unpack(les_ctx *ctx, unsigned mask, int i0, int width, const float *buf);
 les_status les_dd_sums(les_ctx *ctx, long long **dptr);
+les_status les_dd_local_sum(int n, les_ctx *const *ranks);
 les_status les_dd_phase(les_ctx *ctx, int phase, int arg);
 
 #ifdef __cplusplus

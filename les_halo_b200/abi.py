@@ -167,6 +167,7 @@ _SIGS = {
     "les_dd_unpack": (C.c_int, [_P, C.c_uint, C.c_int, C.c_int, _P]),
     "les_dd_sums": (C.c_int, [_P, C.POINTER(C.c_void_p)]),
     "les_dd_phase": (C.c_int, [_P, C.c_int, C.c_int]),
+    "les_dd_local_sum": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
 }
 
 # Per-routine entries: every argument is a pointer (Fortran by-reference).

@@ -100,5 +100,20 @@ __global__ void k_dd_sor_finish(const long long *in, float pjuge, Scal *s) {
     s->pbuf ^= 1;
 }
 
+// The limbs of every rank of one process on one device: their sums
+// (64-bit integers, as an all-reduce forms them) written back to each.
+constexpr int kDDMaxLocal = 64;
+struct DDLocal {
+    long long *s[kDDMaxLocal];
+    int n;
+};
+__global__ void k_dd_local_sum(DDLocal r) {
+    const int t = threadIdx.x;
+    if (blockIdx.x != 0 || t >= kDDLimbs) return;
+    long long v = 0;
+    for (int q = 0; q < r.n; ++q) v += r.s[q][t];
+    for (int q = 0; q < r.n; ++q) r.s[q][t] = v;
+}
+
 }  // namespace
 }  // namespace les

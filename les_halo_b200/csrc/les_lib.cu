@@ -225,6 +225,7 @@ struct les_ctx {
     bool dd_passes = false;               // its SOR on one-iteration passes (else per colour)
     double dd_area = 0.0;                 // the whole domain's rhsav/pav denominator
     long long *d_dd = nullptr;            // limbs of a global sum (kDDLimbs)
+    cudaEvent_t dd_ev = nullptr;          // orders les_dd_local_sum against this context's stream
 };
 
 // Buffers of an SOR pass other than the context's p / second p / rhs / scalars.
@@ -1043,6 +1044,7 @@ les_status les_ctx_destroy(les_ctx *c) {
     cudaFree(c->d_r2);
     cudaFree(c->d_drag);
     cudaFree(c->d_dd);
+    if (c->dd_ev) cudaEventDestroy(c->dd_ev);
     spec_release(c->spec);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

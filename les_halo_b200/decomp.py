@@ -11,9 +11,9 @@ phase schedule is in include/les_abi.h beside les_dd_phase).  The global
 sums travel as the limbs of their exact Q63.64 totals, so every own cell
 stays the single domain's bit for bit.
 
-Transports: ``LocalExchange`` (every rank in this process, device copies
-ordered by CUDA events: the ranks of one GPU, or of several GPUs driven by
-one process) and ``DistExchange`` (one rank per process, NCCL send/recv and
+Transports: ``LocalExchange`` (every rank in this process on one GPU, halo
+blocks ordered by CUDA events between the ranks' streams, the sums added by
+one kernel) and ``DistExchange`` (one rank per process, NCCL send/recv and
 all-reduce through torch.distributed; with gloo and CPU tensors the same
 code exercises the host logic).
 """
@@ -194,7 +194,7 @@ def _transfers(slabs, halo):
 class LocalExchange:
     """Every rank in this process: a halo block is packed on the owner's
     stream, unpacked on the neighbour's after a CUDA event, and the sums are
-    added on rank 0's stream and copied back."""
+    added by one kernel on rank 0's stream (les_dd_local_sum)."""
 
     def __init__(self, ranks):
         import torch
@@ -203,6 +203,7 @@ class LocalExchange:
         self.halo = ranks[0].slab.halo
         self.xfers = _transfers([r.slab for r in ranks], self.halo)
         self.bufs = {}
+        self._ctxs = (C.c_void_p * len(ranks))(*[r.ctx.value for r in ranks])
 
     def _buf(self, key, n, device):
         b = self.bufs.get(key)
@@ -230,24 +231,8 @@ class LocalExchange:
             b[1].record(dst.stream())
 
     def allreduce(self):
-        torch = self.torch
-        if len(self.ranks) == 1:
-            return
-        s0 = self.ranks[0].stream()
-        for r in self.ranks[1:]:
-            ev = torch.cuda.Event()
-            ev.record(r.stream())
-            s0.wait_event(ev)
-        with torch.cuda.stream(s0):
-            tot = self.ranks[0].sums().clone()
-            for r in self.ranks[1:]:
-                tot += r.sums()
-            for r in self.ranks:
-                r.sums().copy_(tot)
-        ev = torch.cuda.Event()
-        ev.record(s0)
-        for r in self.ranks[1:]:
-            r.stream().wait_event(ev)
+        if len(self.ranks) > 1:
+            abi.check(abi.lib().les_dd_local_sum(len(self.ranks), self._ctxs))
 
 
 class DistExchange:
