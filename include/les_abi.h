@@ -129,6 +129,12 @@ les_status les_step(les_ctx *ctx, int n0, int nsteps);
 les_status les_set_wind_profile(les_ctx *ctx, const float *wind_profile);
 les_status les_ctx_sync(les_ctx *ctx);
 les_status les_last_metrics(les_ctx *ctx, les_metrics *m);
+/* The WV_DEBUG sums (velnw.f95:61-68, feedbf.f95:30-36,68-83, the sum(x)
+ * of every state array): sums[f] = the sum of field f (LES_F_*) over its
+ * Fortran bounds, rhs as les_ctx_download returns it, each an exact Q63.64
+ * sum of the FP32 values rounded to FP64 (independent of the order and of
+ * the device).  LES_NFIELDS doubles; synchronous. */
+les_status les_ctx_field_sums(les_ctx *ctx, double *sums);
 /* CUDA stream (cudaStream_t) the context launches on. */
 void *les_ctx_stream(les_ctx *ctx);
 /* Number of kernels the library launched on this context so far. */

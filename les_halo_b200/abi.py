@@ -101,6 +101,7 @@ _SIGS = {
     "les_ctx_sync": (C.c_int, [_P]),
     "les_last_metrics": (C.c_int, [_P, C.POINTER(LesMetrics)]),
     "les_ctx_stream": (C.c_void_p, [_P]),
+    "les_ctx_field_sums": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "les_ctx_launch_count": (C.c_uint64, [_P]),
     "les_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "les_ctx_set_sor_path": (C.c_int, [_P, C.c_int]),

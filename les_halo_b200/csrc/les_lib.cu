@@ -1207,6 +1207,23 @@ les_status les_ctx_download(les_ctx *c, les_host_fields *hf) {
     return ok();
 }
 
+les_status les_ctx_field_sums(les_ctx *c, double *sums) {
+    LES_RANGE("les_ctx_field_sums");
+    if (!c || !sums) return fail(LES_ERR_BAD_ARG, "NULL argument");
+    double *d_out = reinterpret_cast<double *>(c->d_stage);  // LES_NFIELDS doubles
+    for (int f = 0; f < LES_NFIELDS; ++f) {
+        const FBounds b = field_bounds(f, c->prm.ip, c->prm.jp, c->prm.kp);
+        const bool sub = (f == LES_F_RHS) && c->rhs_raw;
+        const int nb = (int)std::min<long long>(cdiv((long long)b.n(), kRedNT * 8LL), (long long)c->npart);
+        LAUNCH(c, k_field_sum, dim3(nb), dim3(kRedNT), c->geo, field_ptr(c, f), b.li, b.lj, b.lk, b.ni(), b.nj(),
+               b.nk(), c->d_scal, sub ? 1 : 0, c->d_part);
+        LAUNCH(c, k_field_sum_final, dim3(1), dim3(1024), c->d_part, nb, d_out + f);
+    }
+    CK(cudaMemcpyAsync(sums, d_out, sizeof(double) * LES_NFIELDS, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return ok();
+}
+
 les_status les_ctx_warmup(les_ctx *c, int n) {
     LES_RANGE("les_ctx_warmup");
     if (!c) return fail(LES_ERR_BAD_ARG, "NULL ctx");

@@ -133,6 +133,33 @@ __device__ __forceinline__ void final_fix(const FixPart *part, int n, i128 &tot,
     }
 }
 
+// Exact sum (Q63.64 terms, les_fix.h) of a field over its Fortran bounds,
+// one partial per block (kRedNT threads); rhs as the caller sees it
+// (rhs - rhsav on the interior when sub_interior).
+__global__ void __launch_bounds__(kRedNT) k_field_sum(Geo g, const float *__restrict__ box, int li, int lj, int lk,
+                                                      int ni, int nj, int nk, const Scal *s, int sub_interior,
+                                                      FixPart *part) {
+    const size_t n = (size_t)ni * nj * nk;
+    const float sub = sub_interior ? s->rhsav : 0.0f;
+    i128 acc = 0;
+    int bad = 0;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+        const int i = li + (int)(t % ni), r = (int)(t / ni);
+        const int j = lj + r % nj, k = lk + r / nj;
+        float x = box[IX(g, i, j, k)];
+        if (sub_interior && i >= 1 && i <= g.im && j >= 1 && j <= g.jm && k >= 1 && k <= g.km) x = x - sub;
+        acc += fix_term(x, bad);
+    }
+    block_fix_sum<kRedNT>(acc, bad, &part[blockIdx.x]);
+}
+
+__global__ void __launch_bounds__(1024) k_field_sum_final(const FixPart *part, int n, double *out) {
+    i128 tot;
+    int bad;
+    final_fix(part, n, tot, bad);
+    if (threadIdx.x == 0) *out = fix_finish(tot, bad);
+}
+
 // rhsav = num/area (press.f95:138), area given (grid-only, finished on the host).
 __global__ void __launch_bounds__(1024) k_final_rhsav(const FixPart *part, int n, double area, Scal *s) {
     i128 tot;

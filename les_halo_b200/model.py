@@ -138,6 +138,13 @@ class GpuLes:
         abi.check(abi.lib().les_last_metrics(self.ctx, C.byref(m)))
         return {n: getattr(m, n) for n, _ in m._fields_}
 
+    def field_sums(self) -> dict:
+        """The reference's WV_DEBUG sums (sum(u), sum(v), ... over each array's
+        bounds, velnw.f95:61-68): exact on the device, rounded to FP64."""
+        out = (C.c_double * len(abi.FIELD_IDS))()
+        abi.check(abi.lib().les_ctx_field_sums(self.ctx, out))
+        return {n: out[i] for i, n in enumerate(abi.FIELD_IDS)}
+
     def download(self, names=None) -> dict:
         """Fortran-layout copies of the state arrays."""
         names = names or FL.STATE + FL.MASKS
